@@ -1,0 +1,188 @@
+"""GPU parity of the pass-1 / accumulation / pass-2 kernels, called through the C ABI (libxpgi.so), on the shoebox
+chunks stored in the golden fixtures: against the oracle (same arithmetic contract: integers and per-pixel terms
+bit-exact, sums to float64-rounding) and against the reference's own outputs (tolerance.py)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import golden_io as G
+import tolerance as T
+from oracle import kernels as OK
+
+pytestmark = pytest.mark.gpu
+
+CASES = G.CASES
+
+
+def _rows_from_chunk(d, rc, nb, device):
+    from xpg_b200 import device as D
+    m, Dz, Dy, Dx = d["sb"].shape
+    pxs = rc["pxs"].astype(np.int32) if "pxs" in rc else np.ones(m, np.int32)
+    return D.RowSet(S=rc["S"], phi=rc["phi"], ix0=rc["ix0"], iy0=rc["iy0"], iz0=rc["iz0"], fb=rc["fb"],
+                    region=rc["region"], has_p=rc["has_p"], pS=rc["pS"], pphi=rc["pphi"], pxs=pxs,
+                    Dz=np.full(m, Dz), bx=np.full(m, Dx), nb=nb, device=device, sb_bias=0.0)
+
+
+def _block(d, prefix=""):
+    from xpg_b200 import native as N
+    b = N.XiBlock()
+    b.frames_phi0 = float(d["frames_phi0"])
+    b.osc = float(d["osc"])
+    b.sd = float(d[prefix + "sd"])
+    b.sm = float(d[prefix + "sm"])
+    b.gain = float(d[prefix + "gain"])
+    rcw = torch.as_tensor(np.asarray(d[prefix + "rcw"], np.float32)).cuda()
+    b.rcw = N.ptr(rcw)
+    for c in range(3):
+        b.s0[c] = float(d["s0"][c])
+        b.axis[c] = float(d["axis"][c])
+    return b, rcw
+
+
+def _run_case(case):
+    from xpg_b200 import device as D
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    g = spec.geometry()
+    det = D.DeviceDetector(g, tmpl)
+    odet = OK.detector_consts(g, tmpl)
+    results = []
+    for i in G.chunks(case):
+        d, rc, nb, o1, o2 = G.chunk(case, i)
+        rows = _rows_from_chunk(d, rc, nb, "cuda")
+        arena = torch.as_tensor(d["sb"].reshape(-1)).cuda()
+        blk, keep = _block(d)
+        p1 = D.Pass1Buffers(rows)
+        D.pass1(det, rows, blk, arena, p1)
+        D.status()
+        h1 = {k: v.cpu().numpy() for k, v in p1.t.items()}
+        res = dict(chunk=i, d=d, rc=rc, nb=nb, o1=o1, o2=o2, rows=rows, h1=h1, odet=odet)
+        if o2:
+            prof = torch.as_tensor(d["prof"]).cuda()
+            blk2, keep2 = _block(d, "p2_")
+            p2 = D.Pass2Buffers(rows)
+            D.pass2(det, rows, blk2, arena, prof, p1, p2)
+            D.status()
+            res["h2"] = {k: v.cpu().numpy() for k, v in p2.t.items()}
+        results.append(res)
+    return results
+
+
+def _row_out(h1, rows, j):
+    """Row j's pass-1 outputs in the oracle's shapes."""
+    Dz, bx = int(rows.Dz[j]), int(rows.bx[j])
+    po, fo = rows.pix_off[j], rows.frm_off[j]
+    o = {k: h1[k][j] for k in h1 if h1[k].shape[0] == rows.n}
+    for k in ("img2", "J", "u1", "u2", "all_valid2"):
+        o[k] = h1[k][po:po + bx * bx].reshape(bx, bx)
+    o["all_valid2"] = o["all_valid2"].astype(bool)
+    o["fz"] = h1["fz"][fo:fo + Dz]
+    return o
+
+
+@pytest.fixture(scope="module", params=CASES)
+def case_results(request):
+    return request.param, _run_case(request.param)
+
+
+EXACT = ("n_over", "n_fg_masked", "n_fg_nb", "nfg", "bg", "nbg", "zeta", "seff", "all_valid2", "J", "u1", "u2")
+
+
+def test_pass1_matches_oracle(case_results):
+    """Integer counts, masks, the background and every per-pixel geometric term are bit-exact with the oracle;
+    the float64-accumulated sums agree to their float32 rounding."""
+    case, results = case_results
+    for r in results:
+        d, rc, nb = r["d"], r["rc"], r["nb"]
+        for j in range(r["rows"].n):
+            mine = _row_out(r["h1"], r["rows"], j)
+            ref = OK.pass1(d["sb"][j], G.row_dict(rc, j), G.nb_row(nb, j), r["odet"], d["s0"], d["axis"],
+                           d["frames_phi0"], d["osc"], d["sd"], d["sm"], d["gain"], d["rcw"])
+            for k in EXACT:
+                a, b = np.asarray(mine[k]), np.asarray(ref[k])
+                assert np.array_equal(a.astype(np.float64), b.astype(np.float64)), (case, r["chunk"], j, k)
+            for k in ("isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "img2", "fz"):
+                ok, worst = T.within(k, mine[k], ref[k], ref, rel=2e-6)
+                assert ok, (case, r["chunk"], j, k, worst)
+
+
+def test_pass1_matches_reference(case_results):
+    """Against XPG's own pass 1: integers exact, floats within tolerance.py."""
+    case, results = case_results
+    for r in results:
+        o1 = r["o1"]
+        for j in range(r["rows"].n):
+            mine = _row_out(r["h1"], r["rows"], j)
+            ctx = {k: o1[k][j] for k in o1}
+            for k in ("n_over", "n_fg_masked", "n_fg_nb", "nfg"):
+                assert int(mine[k]) == int(o1[k][j]), (case, r["chunk"], j, k)
+            assert np.array_equal(mine["all_valid2"], o1["all_valid2"][j]), (case, r["chunk"], j)
+            for k in ("bg", "nbg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "zeta",
+                      "seff", "J", "u1", "u2", "img2", "fz"):
+                ok, worst = T.within(k, mine[k], o1[k][j], ctx)
+                assert ok, (case, r["chunk"], j, k, worst)
+
+
+def test_pass2_matches_oracle_and_reference(case_results):
+    case, results = case_results
+    n = 0
+    for r in results:
+        if "h2" not in r:
+            continue
+        d, rc, nb, o1, o2 = r["d"], r["rc"], r["nb"], r["o1"], r["o2"]
+        for j in range(r["rows"].n):
+            m1 = _row_out(r["h1"], r["rows"], j)
+            pix = dict(zeta=m1["zeta"], J=m1["J"], u1=m1["u1"], u2=m1["u2"], seff=m1["seff"])
+            ref = OK.pass2(d["sb"][j], G.row_dict(rc, j), G.nb_row(nb, j), r["odet"], d["s0"], d["axis"],
+                           d["frames_phi0"], d["osc"], d["p2_sd"], d["p2_sm"], d["p2_gain"], d["prof"], m1["bg"],
+                           m1["nbg"], d["p2_rcw"], pix)
+            mine = {k: r["h2"][k][j] for k in r["h2"]}
+            ctx_o = dict(ref, vsum=m1["vsum"])
+            for k in ref:
+                ok, worst = T.within(k, mine[k], ref[k], ctx_o, rel=2e-6)
+                assert ok, ("oracle", case, r["chunk"], j, k, worst, mine[k], ref[k])
+            ctx = {k: o2[k][j] for k in o2}
+            for k in ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "ipartner", "rho", "p_fg"):
+                ok, worst = T.within(k, mine[k], o2[k][j], ctx)
+                assert ok, ("reference", case, r["chunk"], j, k, worst, mine[k], o2[k][j])
+            n += 1
+    assert n > 0 or case == "sigmas"
+
+
+def test_accumulate_and_finalize_match_oracle():
+    """Profile accumulation of every stored pass-1 chunk's strong rows (float64 grids) and the finalised
+    profiles."""
+    from xpg_b200 import device as D
+    case = "adaptive"
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    g = spec.geometry()
+    det = D.DeviceDetector(g, tmpl)
+    nreg = spec.n_regions_xy ** 2
+    num_o = np.zeros((nreg, 41, 41))
+    den_o = np.zeros((nreg, 41, 41))
+    num = torch.zeros((nreg, 41, 41), dtype=torch.float64, device="cuda")
+    den = torch.zeros_like(num)
+    n_strong = 0
+    for i in G.chunks(case):
+        d, rc, nb, o1, o2 = G.chunk(case, i)
+        rows = _rows_from_chunk(d, rc, nb, "cuda")
+        arena = torch.as_tensor(d["sb"].reshape(-1)).cuda()
+        blk, keep = _block(d)
+        p1 = D.Pass1Buffers(rows)
+        D.pass1(det, rows, blk, arena, p1)
+        D.accumulate(rows, p1, nreg, num, den)
+        h1 = {k: v.cpu().numpy() for k, v in p1.t.items()}
+        for j in range(rows.n):
+            o = _row_out(h1, rows, j)
+            if OK.is_strong_for_profiles(o):
+                OK.accumulate(num_o, den_o, o, int(rc["region"][j]))
+                n_strong += 1
+    assert n_strong > 10
+    np.testing.assert_allclose(num.cpu().numpy(), num_o, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(den.cpu().numpy(), den_o, rtol=1e-12, atol=1e-12)
+    prof = torch.empty((nreg, 41, 41), dtype=torch.float32, device="cuda")
+    D.finalize_profiles(num, den, prof)
+    want = OK.finalize_profiles(num_o, den_o)
+    got = prof.cpu().numpy()
+    assert np.max(np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), 1e-30)) < 2.5e-7

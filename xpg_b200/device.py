@@ -1,0 +1,287 @@
+"""Device-side objects of the integration path: detector constants, packed per-reflection rows, the shoebox arena
+and the pass outputs, each with the C struct that the kernels read (include/xpgi.h).
+
+Every buffer is a torch CUDA tensor (torch is the allocator and the stream); the arithmetic runs in libxpgi.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import native as N
+
+F32 = torch.float32
+
+
+def _dev(a, dtype, device):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(device, non_blocking=False)
+
+
+class DeviceDetector:
+    """XPG's `_detector_consts` (`xpg/integrate_kernels.py:48-65`) on the device."""
+
+    def __init__(self, g, bkg_template=None, device="cuda"):
+        P0, Bx, By = g.panels()
+        U1, U2 = Bx / g.qx, By / g.qy
+        UN = np.cross(U1, U2)
+        f = lambda a: _dev(np.asarray(a, np.float32).reshape(-1, 3), F32, device)
+        self.t = dict(P0=f(P0), Bx=f(Bx), By=f(By), U1=f(U1), U2=f(U2), UN=f(UN))
+        seg = g.segmap() if getattr(g, "segmented", False) else None
+        geo = getattr(g, "geo_corr", None)
+        self.t["segmap"] = None if seg is None else _dev(seg.astype(np.int16), torch.int16, device)
+        self.t["gx"] = None if geo is None else _dev(np.asarray(geo[0], np.float32), F32, device)
+        self.t["gy"] = None if geo is None else _dev(np.asarray(geo[1], np.float32), F32, device)
+        self.t["bkg"] = None if bkg_template is None else _dev(np.asarray(bkg_template, np.float32), F32, device)
+        d = N.XiDetector()
+        d.n_panels = int(np.asarray(P0).reshape(-1, 3).shape[0])
+        for k in ("P0", "Bx", "By", "U1", "U2", "UN", "segmap", "gx", "gy", "bkg"):
+            setattr(d, k, N.ptr(self.t[k]))
+        if seg is not None:
+            d.seg_ny, d.seg_nx = seg.shape
+        if geo is not None:
+            d.geo_ny, d.geo_nx = np.asarray(geo[0]).shape
+        if bkg_template is not None:
+            d.bkg_ny, d.bkg_nx = np.asarray(bkg_template).shape
+        d.orgx, d.orgy = float(g.orgx), float(g.orgy)
+        d.qx, d.qy, d.wl = float(g.qx), float(g.qy), float(g.wavelength)
+        tsens = float(max(g.sensor_thickness, 1e-6))
+        mu = float(max(g.mu, 1e-6))
+        d.tsens, d.mu, d.inv_mu = tsens, mu, 1.0 / mu
+        d.parallax = 1 if g.has_parallax else 0
+        self.s = d
+
+
+def block_consts(g, sd, sm, gain, rcw, device="cuda"):
+    """XiBlock of a phi block (`xpg/integrate.py:466-475`): returns (struct, keep-alive tensors)."""
+    b = N.XiBlock()
+    b.frames_phi0 = float(np.float32(np.radians(g.z_to_phi(0.0))))
+    b.osc = float(np.float32(np.radians(g.osc)))
+    b.sd, b.sm, b.gain = float(np.float32(sd)), float(np.float32(sm)), float(np.float32(gain))
+    rc = _dev(np.asarray(rcw, np.float32), F32, device)
+    b.rcw = N.ptr(rc)
+    s0 = np.asarray(g.s0, np.float32)
+    ax = np.asarray(g.axis, np.float32)
+    for c in range(3):
+        b.s0[c] = float(s0[c])
+        b.axis[c] = float(ax[c])
+    return b, rc
+
+
+class RowSet:
+    """Per-reflection inputs of a set of rows (any mix of shoebox shapes), packed on the device with their arena
+    offsets: `sb_off` (shoebox voxels), `pix_off` (per-pixel outputs), `frm_off` (per-frame outputs)."""
+
+    def __init__(self, S, phi, ix0, iy0, iz0, fb, region, has_p, pS, pphi, pxs, Dz, bx, nb, device="cuda",
+                 sb_bias=3.0):
+        n = len(phi)
+        self.n = n
+        self.Dz = np.asarray(Dz, np.int64)
+        self.bx = np.asarray(bx, np.int64)
+        V = self.Dz * self.bx * self.bx
+        self.vox = V
+        self.sb_off = np.concatenate([[0], np.cumsum(V)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        P = self.bx * self.bx
+        self.pix_off = np.concatenate([[0], np.cumsum(P)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        self.frm_off = np.concatenate([[0], np.cumsum(self.Dz)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        self.n_vox = int(V.sum())
+        self.n_pix = int(P.sum())
+        self.n_frm = int(self.Dz.sum())
+        K = int(np.asarray(nb["x"]).shape[1]) if n else 0
+        if K > N.XI_MAX_K:
+            raise ValueError(f"{K} neighbour columns > {N.XI_MAX_K}")
+        d = device
+        self.t = dict(
+            S=_dev(np.asarray(S, np.float32).reshape(n, 3), F32, d), phi=_dev(phi, F32, d),
+            ix0=_dev(ix0, torch.int32, d), iy0=_dev(iy0, torch.int32, d), iz0=_dev(iz0, torch.int32, d),
+            fb=_dev(np.asarray(fb, np.float32), F32, d), region=_dev(region, torch.int32, d),
+            has_p=_dev(np.asarray(has_p, np.float32), F32, d), pS=_dev(np.asarray(pS, np.float32).reshape(n, 3), F32, d),
+            pphi=_dev(pphi, F32, d), pxs=_dev(pxs, torch.int32, d), Dz=_dev(self.Dz, torch.int32, d),
+            bx=_dev(self.bx, torch.int32, d), sb_off=_dev(self.sb_off, torch.int64, d),
+            pix_off=_dev(self.pix_off, torch.int64, d), frm_off=_dev(self.frm_off, torch.int64, d))
+        for k in ("x", "y", "z", "sx", "sz"):
+            self.t["nb" + k] = _dev(np.asarray(nb[k], np.float32).reshape(n, K), F32, d)
+        r = N.XiRows()
+        r.n = n
+        for k in ("S", "phi", "ix0", "iy0", "iz0", "fb", "region", "has_p", "pS", "pphi", "pxs", "Dz", "bx",
+                  "sb_off", "pix_off", "frm_off", "nbx", "nby", "nbz", "nbsx", "nbsz"):
+            setattr(r, k, N.ptr(self.t[k]))
+        r.K = K
+        r.order = None
+        r.n_order = 0
+        r.max_bx = int(self.bx.max()) if n else 3
+        r.max_dz = int(self.Dz.max()) if n else 1
+        r.sb_bias = float(sb_bias)
+        self.s = r
+        self.device = device
+
+    def groups(self):
+        """Launch groups: rows of one box side, each with its own row order (deepest first)."""
+        out = []
+        for b in np.unique(self.bx):
+            rows = np.flatnonzero(self.bx == b)
+            rows = rows[np.argsort(-self.Dz[rows], kind="stable")]
+            out.append((int(b), int(self.Dz[rows].max()), rows.astype(np.int32)))
+        return out
+
+    def view(self, order=None, max_bx=None, max_dz=None):
+        """A copy of the struct restricted to `order` (device int32 tensor) with its shape maxima."""
+        r = N.XiRows.from_buffer_copy(self.s)
+        if order is not None:
+            r.order = N.ptr(order)
+            r.n_order = int(order.numel())
+        if max_bx is not None:
+            r.max_bx = int(max_bx)
+        if max_dz is not None:
+            r.max_dz = int(max_dz)
+        return r
+
+
+class Pass1Buffers:
+    """Pass-1 outputs of a RowSet (`xpg/integrate_kernels.py:362-365`)."""
+
+    SCALARS = ("bg", "nbg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "nfg", "zeta",
+               "seff")
+    COUNTS = ("n_over", "n_fg_masked", "n_fg_nb")
+
+    def __init__(self, rows: RowSet):
+        d = rows.device
+        n = rows.n
+        self.t = {k: torch.empty(n, dtype=F32, device=d) for k in self.SCALARS}
+        self.t.update({k: torch.empty(n, dtype=torch.int64, device=d) for k in self.COUNTS})
+        self.t["fz"] = torch.empty(rows.n_frm, dtype=F32, device=d)
+        for k in ("img2", "J", "u1", "u2"):
+            self.t[k] = torch.empty(rows.n_pix, dtype=F32, device=d)
+        self.t["all_valid2"] = torch.empty(rows.n_pix, dtype=torch.uint8, device=d)
+        o = N.XiPass1Out()
+        for k, v in self.t.items():
+            setattr(o, k, N.ptr(v))
+        self.s = o
+
+    def pass2_in(self):
+        i = N.XiPass2In()
+        for k in ("zeta", "seff", "J", "u1", "u2", "bg", "nbg"):
+            setattr(i, k, N.ptr(self.t[k]))
+        return i
+
+
+class Pass2Buffers:
+    KEYS = ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "ipartner", "rho", "p_fg")
+
+    def __init__(self, rows: RowSet):
+        self.t = {k: torch.empty(rows.n, dtype=F32, device=rows.device) for k in self.KEYS}
+        o = N.XiPass2Out()
+        for k, v in self.t.items():
+            setattr(o, k, N.ptr(v))
+        self.s = o
+
+
+def _stream(stream):
+    return N.stream_handle(stream)
+
+
+def pass1(det: DeviceDetector, rows: RowSet, blk, arena, out: Pass1Buffers, stream=None, groups=None):
+    """Pass 1 of every row, one launch per box side."""
+    lib = N.load()
+    for bxg, dzg, order in (groups if groups is not None else _device_groups(rows)):
+        r = rows.view(order, bxg, dzg)
+        N.check(lib.xi_pass1(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), C.byref(out.s),
+                             _stream(stream)), "xi_pass1")
+
+
+def pass2(det: DeviceDetector, rows: RowSet, blk, arena, prof, p1: Pass1Buffers, out: Pass2Buffers, stream=None,
+          groups=None):
+    lib = N.load()
+    i2 = p1.pass2_in()
+    for bxg, dzg, order in (groups if groups is not None else _device_groups(rows)):
+        r = rows.view(order, bxg, dzg)
+        N.check(lib.xi_pass2(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), N.ptr(prof), C.byref(i2),
+                             C.byref(out.s), _stream(stream)), "xi_pass2")
+
+
+def accumulate(rows: RowSet, p1: Pass1Buffers, n_regions, num, den, sel=None, strong_test=True, order=None,
+               stream=None):
+    lib = N.load()
+    r = rows.view(order)
+    N.check(lib.xi_accumulate(C.byref(r), C.byref(p1.s), N.ptr(sel), 1 if strong_test else 0, int(n_regions),
+                              N.ptr(num), N.ptr(den), _stream(stream)), "xi_accumulate")
+
+
+def finalize_profiles(num, den, prof, stream=None):
+    lib = N.load()
+    N.check(lib.xi_finalize_profiles(N.ptr(num), N.ptr(den), int(num.shape[0]), N.ptr(prof), _stream(stream)),
+            "xi_finalize_profiles")
+
+
+def status(stream=None):
+    N.check(N.load().xi_status(_stream(stream)), "kernel status")
+
+
+def _device_groups(rows: RowSet):
+    cache = getattr(rows, "_groups", None)
+    if cache is None:
+        cache = [(b, dz, torch.as_tensor(o).to(rows.device)) for b, dz, o in rows.groups()]
+        rows._groups = cache
+    return cache
+
+
+class GatherRows:
+    """Boxes of a block's rows for the frame gather (`xpg/integrate.py:372-398`), with bin counters for binned
+    rows."""
+
+    def __init__(self, rows: RowSet, ix0, iy0, iz0, fb, pxs, device="cuda"):
+        n = rows.n
+        fb = np.asarray(fb, np.int64)
+        binned = fb > 1
+        cnt_len = np.where(binned, rows.Dz, 0)
+        cnt_off = np.where(binned, np.concatenate([[0], np.cumsum(cnt_len)[:-1]]) if n else 0, -1).astype(np.int64)
+        self.n_cnt = int(cnt_len.sum())
+        self.any_binned = bool(binned.any())
+        d = device
+        self.t = dict(ix0=_dev(ix0, torch.int32, d), iy0=_dev(iy0, torch.int32, d), iz0=_dev(iz0, torch.int32, d),
+                      fb=_dev(fb, torch.int32, d), Dz=rows.t["Dz"], bx=rows.t["bx"], pxs=_dev(pxs, torch.int32, d),
+                      sb_off=rows.t["sb_off"], cnt_off=_dev(cnt_off, torch.int64, d))
+        g = N.XiGatherRows()
+        g.n = n
+        for k, v in self.t.items():
+            setattr(g, k, N.ptr(v))
+        g.order = None
+        g.n_order = 0
+        self.s = g
+        self.iz0 = np.asarray(iz0, np.int64)
+        self.span = rows.Dz * fb
+        self.binned = binned
+
+    def view(self, order):
+        g = N.XiGatherRows.from_buffer_copy(self.s)
+        g.order = N.ptr(order)
+        g.n_order = int(order.numel())
+        return g
+
+
+def frames_struct(data, first_fi, overload, min_valid=0, mask=None, frame_ok=None):
+    """XiFrames of a device wedge (n_frames, ny, nx) of uint32 raw counts or float32 prepared frames."""
+    f = N.XiFrames()
+    f.data = N.ptr(data)
+    f.is_float = 1 if data.dtype == torch.float32 else 0
+    if data.dtype not in (torch.float32, torch.int32, torch.uint32):
+        raise TypeError("frames must be uint32 (raw) or float32 (prepared)")
+    f.n_frames, f.ny, f.nx = (int(v) for v in data.shape)
+    f.first_fi = int(first_fi)
+    f.frame_ok = N.ptr(frame_ok)
+    f.overload = int(min(int(overload), 0xFFFFFFFF)) if overload is not None else 0xFFFFFFFF
+    f.min_valid = int(min_valid)
+    f.mask = N.ptr(mask)
+    return f
+
+
+def gather(frames_s, grows: GatherRows, order, arena, cnt, stream=None):
+    lib = N.load()
+    g = grows.view(order)
+    N.check(lib.xi_gather(C.byref(frames_s), C.byref(g), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_gather")
+
+
+def decode_bins(grows: GatherRows, arena, cnt, stream=None):
+    lib = N.load()
+    N.check(lib.xi_decode_bins(C.byref(grows.s), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")
