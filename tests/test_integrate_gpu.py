@@ -1,0 +1,123 @@
+"""End-to-end GPU parity of the drop-in `integrate()` / `estimate_sigmas()` against the reference's own results on
+the golden sweeps (frames re-rendered from the fixture's seed and checked by crc)."""
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+import golden_io as G
+import tolerance as T
+
+pytestmark = pytest.mark.gpu
+
+EXACT_INT = ("n_over", "n_fg_masked", "iz0", "dz", "fb", "region", "ix0", "iy0", "overlap", "hkl", "block", "lattice")
+CHECK_F = ("bg", "isum", "vsum", "vsum0", "iprf", "vprf", "vprf0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m",
+           "corr", "p_valid", "p_total", "rho", "p_fg")
+
+
+def _run(case, images=None, **over):
+    from xpg_b200 import frames as FR
+    from xpg_b200.integrate import integrate
+    from xpg_b200.plan import IntegrationModel
+    z = G.load(case)
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    exp = spec.experiment()
+    edges = z["edges"]
+    if images is None:
+        images = FR.U32Frames(G.frames_of(case), first=1, overload=spec.overload)
+    model = IntegrationModel(sigma_d=spec.sigma_d, sigma_m=spec.sigma_m, gain=1.0)
+    kw = dict(frames=(1, spec.nframes), mask=mask, minimum_zeta=0.05, verbose=False,
+              n_regions_xy=spec.n_regions_xy, exclude_frames=excl, bkg_template=tmpl)
+    kw.update(over)
+    return integrate(images, [exp] * (len(edges) - 1), edges, model, float(z["dmin"]), **kw)
+
+
+def _compare(case, res):
+    z = G.load(case)
+    out = {k[4:]: v for k, v in z.items() if k.startswith("out_")}
+    r = res.refl
+    assert len(r["x"]) == len(out["x"])
+    for k in EXACT_INT:
+        assert np.array_equal(np.asarray(r[k]), np.asarray(out[k])), (case, k)
+    worst = {}
+    for k in CHECK_F:
+        mine, ref = np.asarray(r[k], np.float64), np.asarray(out[k], np.float64)
+        bad = []
+        for j in range(len(ref)):
+            ctx = {kk: out[kk][j] for kk in ("isum", "vsum", "vprf", "p_valid", "p_total", "m_m")}
+            ctx["seff"] = 1e-3
+            ok, w = T.within(k, mine[j], ref[j], ctx)
+            worst[k] = max(worst.get(k, 0.0), w)
+            if not ok:
+                bad.append((j, mine[j], ref[j]))
+        assert not bad, (case, k, len(bad), bad[:3])
+    return worst
+
+
+@pytest.mark.parametrize("case", G.CASES)
+def test_integrate_matches_reference(case):
+    res = _run(case)
+    z = G.load(case)
+    # per-block adapted widths (they feed pass 2)
+    bp = json.loads(str(z["bp_json"]))
+    for b, v in bp.items():
+        mine = res.block_params[int(b)]
+        assert mine["n"] == v["n"], (b, mine, v)
+        assert abs(mine["sigma_m"] - v["sigma_m"]) <= 1e-6 * v["sigma_m"], (b, mine, v)
+        assert abs(mine["sigma_d"] - v["sigma_d"]) <= 1e-6 * v["sigma_d"], (b, mine, v)
+        assert np.allclose(mine["rcw"], v["rcw"], atol=1.5e-3), (b, mine, v)
+    # learnt profiles of every block
+    for k in z:
+        if k.startswith("prof_"):
+            b = int(k[5:])
+            for reg in range(z[k].shape[0]):
+                peak = float(np.abs(z[k][reg]).max())
+                np.testing.assert_allclose(res.profiles[b][reg], z[k][reg], rtol=1e-5, atol=1e-5 * peak)
+    worst = _compare(case, res)
+    assert worst["iprf"] < T.REL
+
+
+def test_imageset_float_path_identical():
+    """Frames handed over as an XPG-style float32 ImageSet give bit-identical results to the raw uint32 path."""
+    from xpg_b200 import frames as FR
+    from xpg_b200.synth import encode_frame
+    case = "binned"
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    raw = G.frames_of(case)
+
+    class Images:
+        first, last, nx, ny = 1, spec.nframes, spec.nx, spec.ny
+
+        def get(self, f):
+            return encode_frame(raw[f - 1], spec.overload)
+    a = _run(case).refl
+    b = _run(case, images=FR.ImageSetFrames(Images())).refl
+    for k in CHECK_F + ("n_over", "n_fg_masked"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
+
+
+def test_results_independent_of_wedge_size():
+    """Wedge size (frames per upload and gather launch) changes nothing."""
+    a = _run("binned", wedge_frames=7).refl
+    b = _run("binned", wedge_frames=64).refl
+    for k in CHECK_F:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
+
+
+def test_estimate_sigmas_matches_reference():
+    from xpg_b200 import frames as FR
+    from xpg_b200.integrate import estimate_sigmas
+    from xpg_b200.plan import IntegrationModel
+    case = "sigmas"
+    z = G.load(case)
+    spec = G.spec_of(case)
+    images = FR.U32Frames(G.frames_of(case), first=1, overload=spec.overload)
+    model = estimate_sigmas(images, spec.experiment(), IntegrationModel(spec.sigma_d, spec.sigma_m),
+                            max(float(z["dmin"]), 2.0), (1, spec.nframes), verbose=False)
+    np.testing.assert_allclose([model.sigma_d, model.sigma_m], z["model"], rtol=1e-6)
+    hist = np.array(model.history)
+    assert hist.shape == z["history"].shape
+    np.testing.assert_allclose(hist[:, :2], z["history"][:, :2], rtol=1e-6)
+    assert np.array_equal(hist[:, 2], z["history"][:, 2])

@@ -43,8 +43,25 @@ def scale(key, ref, row_ctx):
 MAIN = {"bg", "nbg", "isum", "vsum", "vsum0", "iprf", "vprf", "vprf0"}
 
 
+def meaningful(key, row_ctx):
+    """The second moments of a spot are ratios of sums that cancel for reflections that are not significant:
+    m_d / m_m are compared only where I/sigma >= 3 (XPG uses them only for strong spots, I/sigma > 10)."""
+    if key in ("m_d", "m_m") and "isum" in row_ctx and "vsum" in row_ctx:
+        return float(row_ctx["isum"]) >= 3.0 * np.sqrt(max(float(row_ctx["vsum"]), 1e-6))
+    # profile-fit results of a reflection with under 1% of its profile on valid pixels are extrapolations from a
+    # handful of pixels (XPG's PEAK is then < 1% and the reflection is rejected downstream)
+    if key in PASS2 and "p_valid" in row_ctx and "p_total" in row_ctx:
+        return float(row_ctx["p_valid"]) >= 0.01 * float(row_ctx["p_total"])
+    return True
+
+
+PASS2 = {"iprf", "vprf", "vprf0", "corr", "rho", "ipartner"}
+
+
 def within(key, mine, ref, row_ctx, rel=None):
     """(ok, worst relative-to-scale error) of mine against ref."""
+    if not meaningful(key, row_ctx):
+        return True, 0.0
     mine = np.asarray(mine, np.float64)
     ref = np.asarray(ref, np.float64)
     r = rel if rel is not None else (REL if key in MAIN else REL_AUX)

@@ -575,8 +575,11 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
     }
     // ---- IRLS: Poisson-weighted 2x2 normal equations, float64 sums, N_IRLS iterations ----------------------
     double a11 = 0.0, a12 = 0.0, a22 = 1.0, b1 = 0.0, b2 = 0.0, det2 = 1.0;
+    float Iw = 0.0f, Ipw = 0.0f;        // intensities of the last iteration's weights (the variance tail uses them)
     for (int it = 0; it < kIrls; ++it) {
         const float I = s_I, Ip = s_Ip;
+        Iw = I;
+        Ipw = Ip;
         const float Ipos = fmaxf(I, 0.0f), Ippos = fmaxf(Ip, 0.0f);
         double s11 = 0.0, s1 = 0.0, s12 = 0.0, s22 = 0.0, s2 = 0.0;
         for (int p = threadIdx.x; p < P; p += NT) {
@@ -626,7 +629,8 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
         __syncthreads();
     }
     const float I = s_I, Ip = s_Ip;
-    const float Ipos = fmaxf(I, 0.0f), Ippos = fmaxf(Ip, 0.0f);
+    const float Ippos = fmaxf(Ip, 0.0f);
+    const float Iwpos = fmaxf(Iw, 0.0f), Ipwpos = fmaxf(Ipw, 0.0f);
     // ---- tail pass 1: C, a110, C0 (last iteration's weights), use counts, sums for pm / nm, p_valid, p_total, p_fg
     {
         Mask65 fgz;
@@ -652,8 +656,8 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
                 if (fg2 && fgz.get(z)) acc[7] += (double)pv;                // p_fg numerator
                 if (!valid || nbz || !(pv > pthr || ppv > ppthr)) continue;
                 const float net = v - bpix;
-                float mu = bpix + Ipos * pv;
-                if (has_p) mu = mu + Ippos * ppv;
+                float mu = bpix + Iwpos * pv;
+                if (has_p) mu = mu + Ipwpos * ppv;
                 const float iv = 1.0f / (gain * fmaxf(mu, kVarFloor));
                 const float wb = pv * bref;
                 acc[0] += (double)(wb * iv);                                // C

@@ -1,0 +1,107 @@
+"""Frame sources of the integration: how detector frames reach the device.
+
+* `U32Frames`: raw uint32 frames (Eiger-style: 0xFFFFFFFF flagged, counts >= overload overloaded) in host memory
+  (numpy, ideally pinned) or already on the device (torch). The kernels encode them (`xpg/io/images.py:72-102`).
+* `ImageSetFrames`: any XPG-style image set (`first`, `last`, `nx`, `ny`, `get(frame)` -> float32 frame with -1
+  masked / -2 overloaded, `xpg/io/images.py:59-102`); frames are stacked per wedge on the host and uploaded as
+  float32.
+
+A wedge is a run of consecutive frame numbers; `wedge(f_a, f_b, ok)` returns the device tensor (n, ny, nx) of frames
+f_a..f_b (1-based, inclusive) and the XiFrames encoding parameters. Frames whose `ok` flag is False (excluded) are
+neither read nor uploaded.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+class _PinnedRing:
+    """Two pinned staging buffers used alternately; a buffer is refilled only after its last upload finished."""
+
+    def __init__(self, dtype):
+        self.dtype = dtype
+        self.bufs = [None, None]
+        self.events = [None, None]
+        self.k = 0
+
+    def take(self, n):
+        k = self.k
+        self.k ^= 1
+        if self.events[k] is not None:
+            self.events[k].synchronize()
+            self.events[k] = None
+        if self.bufs[k] is None or self.bufs[k].numel() < n:
+            self.bufs[k] = torch.empty(n, dtype=self.dtype, pin_memory=True)
+        return k, self.bufs[k][:n]
+
+    def upload(self, k, h, device):
+        d = h.to(device, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self.events[k] = ev
+        return d
+
+
+class U32Frames:
+    def __init__(self, data, first=1, overload=1 << 20, min_valid=0, device="cuda"):
+        self.data = data
+        self.first = int(first)
+        n = int(data.shape[0])
+        self.last = self.first + n - 1
+        self.ny, self.nx = int(data.shape[1]), int(data.shape[2])
+        self.overload = int(overload) if overload is not None else None
+        self.min_valid = int(min_valid)
+        self.device = device
+        self.on_device = torch.is_tensor(data) and data.is_cuda
+        self._ring = _PinnedRing(torch.int32)
+
+    def _host_slice(self, a, b):
+        return self.data[a - self.first:b - self.first + 1]
+
+    def wedge(self, f_a, f_b, ok=None, stream=None):
+        if self.on_device:
+            t = self.data[f_a - self.first:f_b - self.first + 1]
+            return (t if t.dtype in (torch.int32, torch.float32) else t.view(torch.int32)), False
+        src = self._host_slice(f_a, f_b)
+        if torch.is_tensor(src):
+            h = src if src.dtype == torch.int32 else src.view(torch.int32)
+            return h.to(self.device, non_blocking=True), False
+        n = src.shape[0]
+        k, buf = self._ring.take(n * self.ny * self.nx)
+        h = buf.view(n, self.ny, self.nx)
+        np.copyto(h.numpy(), np.ascontiguousarray(src).view(np.int32))
+        return self._ring.upload(k, h, self.device), False
+
+
+class ImageSetFrames:
+    """Adapter of an XPG ImageSet: frames arrive already encoded as float32."""
+
+    def __init__(self, images, device="cuda"):
+        self.images = images
+        self.first, self.last = int(images.first), int(images.last)
+        self.ny, self.nx = int(images.ny), int(images.nx)
+        self.overload = None
+        self.min_valid = 0
+        self.device = device
+        self._ring = _PinnedRing(torch.float32)
+
+    def wedge(self, f_a, f_b, ok=None, stream=None):
+        n = f_b - f_a + 1
+        k, buf = self._ring.take(n * self.ny * self.nx)
+        h = buf.view(n, self.ny, self.nx)
+        hn = h.numpy()
+        for w in range(n):
+            if ok is not None and not ok[w]:
+                hn[w] = -1.0
+                continue
+            hn[w] = self.images.get(f_a + w)
+        return self._ring.upload(k, h, self.device), True
+
+
+def as_frame_source(images, device="cuda"):
+    if isinstance(images, (U32Frames, ImageSetFrames)):
+        return images
+    if hasattr(images, "get") and hasattr(images, "first"):
+        return ImageSetFrames(images, device)
+    raise TypeError("images: a U32Frames, ImageSetFrames or an XPG-style ImageSet (first, last, nx, ny, get)")

@@ -1,0 +1,279 @@
+"""Drop-in for XPG's integration stage (`xpg/integrate.py`): `integrate`, `estimate_sigmas`, `IntegrationModel`,
+`IntegrationResult` with the reference's signatures (`:197-215`, `:1002-1003`), computed on one B200.
+
+Data flow of a sweep:
+  host   predictions and the shoebox plan (xpg_b200.plan), block by block;
+  device frames arrive in wedges of consecutive frames (uploaded from host memory, or already resident); one
+         launch per (open block, wedge) gathers every box window into the block's shoebox arena (value + 3,
+         binned rows as IEEE-encoded sums);
+  device when a block's last frame has arrived: bin decode, pass 1, strong-row profile accumulation (float64
+         grids), profile finalisation, pass 2; the host adapts sigma_M / rocking curve / sigma_D in between
+         (float64, xpg_b200.adapt) from the block's strong rows.
+Blocks are processed in the order they complete, so the adaptive widths carry over exactly as in the reference.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import adapt as A
+from . import device as D
+from . import native as N
+from .frames import as_frame_source
+from .geometry import centring_allowed
+from .plan import DZ_BUCKETS, IntegrationModel, plan_integration
+
+PROFILE_GRID = 41
+MAX_DZ = max(DZ_BUCKETS)
+WEDGE_FRAMES = 32                     # frames per upload / gather launch
+OUT_F64 = ("bg", "isum", "vsum", "vsum0", "iprf", "vprf", "vprf0", "corr", "xo", "yo", "zo", "p_valid", "p_total",
+           "frac_rec", "rho", "m_d", "m_m", "p_fg")
+
+
+@dataclass
+class IntegrationResult:
+    refl: dict
+    model: IntegrationModel
+    profiles: dict = field(default_factory=dict)
+    timing: dict = field(default_factory=dict)
+
+
+def _reference_row_order(rows, bucket, bxs, pxs, has_partner):
+    """The block's rows in XPG's kernel-call order (`xpg/integrate.py:375-381`): depth bucket, then box side, then
+    super-pixel side (both ascending), partners first within a group."""
+    out = []
+    for B in DZ_BUCKETS:
+        for bx in np.unique(bxs[rows]):
+            for sp in np.unique(pxs[rows]):
+                sel = rows[(bucket[rows] == B) & (bxs[rows] == bx) & (pxs[rows] == sp)]
+                sel = sel[np.argsort(~has_partner[sel], kind="stable")]
+                out.append(sel)
+    return np.concatenate(out) if out else np.zeros(0, int)
+
+
+class _Block:
+    """Device state of one open phi block."""
+
+    def __init__(self, b, rows, plan, device):
+        self.b = b
+        self.rows = rows                                  # global row indices, reference kernel-call order
+        p = plan
+        refl = p.refl
+        pj = p.partner[rows]
+        self.rowset = D.RowSet(
+            S=refl["S"][rows].astype(np.float32), phi=np.radians(refl["phi"][rows]).astype(np.float32),
+            ix0=p.ix0[rows], iy0=p.iy0[rows], iz0=p.iz0[rows], fb=p.fb[rows], region=p.region[rows],
+            has_p=p.has_partner[rows], pS=refl["S"][pj].astype(np.float32),
+            pphi=np.radians(refl["phi"][pj]).astype(np.float32), pxs=p.pxs[rows], Dz=p.Dz[rows], bx=p.bx[rows],
+            nb={k: v[rows] for k, v in p.nb.items()}, device=device, sb_bias=3.0)
+        self.grows = D.GatherRows(self.rowset, p.ix0[rows], p.iy0[rows], p.iz0[rows], p.fb[rows], p.pxs[rows],
+                                  device)
+        self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
+        self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
+        self.z_lo = p.iz0[rows].astype(np.int64)
+        self.z_hi = self.z_lo + self.grows.span - 1      # last frame index a row's box can take
+
+    def rows_in(self, fi_a, fi_b):
+        """Local rows whose box frame range meets [fi_a, fi_b]."""
+        return np.flatnonzero((self.z_lo <= fi_b) & (self.z_hi >= fi_a)).astype(np.int32)
+
+
+def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dmax=1e9, frames=None, mask=None,
+              minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
+              adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
+              n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed):
+    """Integrate a sweep (`xpg/integrate.py:209-999`). `exp_blocks`: one experiment per phi block, `block_edges` in
+    frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id)."""
+    N.require_cuda()
+    t0 = time.time()
+    lattice_of = [0] * len(exp_blocks)
+    if extra_lattices:
+        exp_blocks = list(exp_blocks)
+        for li, lat in enumerate(extra_lattices, start=1):
+            exp_blocks += list(lat)
+            lattice_of += [li] * len(lat)
+    src = as_frame_source(images, device)
+    if frames is None:
+        frames = (src.first, src.last)
+    f_first, f_last = int(frames[0]), int(frames[1])
+    plan = plan_integration(exp_blocks, block_edges, model, dmin, dmax, (f_first, f_last), minimum_zeta,
+                            n_regions_xy, adaptive, deconvolve_overlaps, lattice_of, foreign_spots, n_foreign, allowed)
+    refl = plan.refl
+    n = plan.n
+    if verbose:
+        log(f"  INTEGRATE: {plan.info['n_predicted']} predicted reflections, box {plan.box}x{plan.box} px, sigma_D "
+            f"{model.sigma_d:.4f} sigma_M {model.sigma_m:.4f} deg; {plan.info['n_wide']} wide in phi (> {MAX_DZ} "
+            f"frames): integrated in bins, {plan.info['n_trunc']} of them still truncated")
+    out = {k: np.full(n, np.nan, np.float64) for k in OUT_F64}
+    out["n_over"] = np.zeros(n, np.int32)
+    out["n_fg_masked"] = np.zeros(n, np.int32)
+    keep_fz = not learn_profiles
+    fz_out = np.zeros((n, MAX_DZ), np.float32) if keep_fz else None
+    nreg = plan.nreg
+    sd = np.radians(model.sigma_d)
+    sm = np.radians(model.sigma_m)
+    state = dict(sd=sd, sm=sm, rcw=A.rc_default_weights())
+    block_params, prof_by_block = {}, {}
+    t_dev = 0.0
+    nblocks = len(exp_blocks)
+    blocks_rows = [_reference_row_order(r, plan.Dz, plan.bx, plan.pxs, plan.has_partner) if r.size else r
+                   for r in plan.blocks_refl]
+    excl = set(int(f) for f in exclude_frames)
+    read = [f for f in range(f_first, f_last + 1) if f not in excl]
+    read_fi = np.array([f - 1 for f in read], np.int64)
+    # a block takes every frame read up to the first frame read at or after its last needed frame
+    # (`xpg/integrate.py:789-793`: completion is checked after the frame's gather)
+    eff_hi = {}
+    for b in range(nblocks):
+        if plan.blocks_refl[b].size:
+            k = np.searchsorted(read_fi, plan.need_hi[b], "left")
+            eff_hi[b] = int(read_fi[min(k, len(read_fi) - 1)]) if len(read_fi) else -1
+    pending = sorted((b for b in range(nblocks) if plan.blocks_refl[b].size), key=lambda b: plan.need_lo[b])
+    opened, open_order = {}, []
+    det_cache = {}
+    mask_t = None
+    if mask is not None and not np.asarray(mask).all():
+        mask_t = torch.as_tensor(np.asarray(mask, np.uint8)).to(device)
+
+    def process(b, blk: _Block):
+        nonlocal t_dev
+        tg = time.time()
+        sd_b = state["sd"] if adaptive else sd
+        sm_b, rcw_b = (state["sm"], state["rcw"]) if adaptive else (sm, A.rc_default_weights())
+        g = exp_blocks[b].geom
+        key = (id(g), id(bkg_template))
+        if key not in det_cache:
+            det_cache.clear()
+            det_cache[key] = D.DeviceDetector(g, bkg_template, device)
+        det = det_cache[key]
+        rs = blk.rowset
+        if blk.grows.any_binned:
+            D.decode_bins(blk.grows, blk.arena, blk.cnt)
+        c1, k1 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
+        p1 = D.Pass1Buffers(rs)
+        D.pass1(det, rs, c1, blk.arena, p1)
+        num = torch.zeros((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float64, device=device)
+        den = torch.zeros_like(num)
+        if learn_profiles:
+            D.accumulate(rs, p1, nreg, num, den)
+        h1 = _host_pass1(p1, rs)
+        rows = blk.rows
+        if adaptive:
+            st = _adapt_rows(h1, plan, rows)
+            sets = []
+            if st.any():
+                F = _fz_padded(h1, rs, st)
+                sets.append((F, refl["phi"][rows][st], refl["zeta_k"][rows][st], plan.iz0[rows][st],
+                             h1["m_d"][st], refl["x"][rows][st], refl["y"][rows][st]))
+            sm_b, rcw_b, sd_next, params = A.adapt_block(g, sets, sd, sm, sd_b, sm_b, rcw_b)
+            if sd_next is not None:
+                state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
+            block_params[b] = params
+        prof = torch.empty((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
+        D.finalize_profiles(num, den, prof)
+        h2 = None
+        if not moments_only:
+            c2, k2 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
+            p2 = D.Pass2Buffers(rs)
+            D.pass2(det, rs, c2, blk.arena, prof, p1, p2)
+            h2 = {k: v.double().cpu().numpy() for k, v in p2.t.items()}
+        D.status()
+        prof_by_block[b] = prof.cpu().numpy()
+        for k in ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m"):
+            out[k][rows] = h1[k]
+        out["n_over"][rows] = h1["n_over"]
+        out["n_fg_masked"][rows] = h1["n_fg_masked"]
+        if fz_out is not None:
+            fz_out[rows] = _fz_padded(h1, rs, np.ones(rs.n, bool))
+        if h2 is not None:
+            for k in ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "rho", "p_fg"):
+                out[k][rows] = h2[k]
+        t_dev += time.time() - tg
+
+    # ---- frame loop: wedges of consecutive frame numbers --------------------------------------------------------
+    W = max(int(wedge_frames), 1)
+    f = f_first
+    while f <= f_last:
+        f_b = min(f + W - 1, f_last)
+        fi_a, fi_b = f - 1, f_b - 1
+        while pending and plan.need_lo[pending[0]] <= fi_b:
+            b = pending.pop(0)
+            opened[b] = _Block(b, blocks_rows[b], plan, device)
+            open_order.append(b)
+        ok = np.array([(g_ not in excl) for g_ in range(f, f_b + 1)], bool)
+        if ok.any() and opened:
+            data, is_f = src.wedge(f, f_b, ok)
+            ok_t = torch.as_tensor(ok.astype(np.uint8)).to(device) if not ok.all() else None
+            for b in open_order:
+                blk = opened.get(b)
+                if blk is None or eff_hi[b] < fi_a:
+                    continue
+                nf = min(fi_b, eff_hi[b]) - fi_a + 1
+                loc = blk.rows_in(fi_a, fi_a + nf - 1)
+                if loc.size == 0:
+                    continue
+                fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
+                                     mask_t, ok_t[:nf] if ok_t is not None else None)
+                D.gather(fs, blk.grows, torch.as_tensor(loc).to(device), blk.arena, blk.cnt)
+        done = sorted((b for b in open_order if b in opened and eff_hi[b] <= fi_b),
+                      key=lambda b: (eff_hi[b], open_order.index(b)))
+        for b in done:
+            process(b, opened.pop(b))
+        f = f_b + 1
+    for b in open_order:
+        if b in opened:
+            process(b, opened.pop(b))
+
+    refl.update(out)
+    refl["overlap"] = plan.overlap
+    if fz_out is not None:
+        refl["fz"] = fz_out
+    refl["iz0"], refl["dz"], refl["fb"] = plan.iz0, plan.dz, plan.fb
+    refl["region"] = plan.region
+    refl["ix0"], refl["iy0"] = plan.ix0 * plan.pxs, plan.iy0 * plan.pxs
+    if (plan.pxs > 1).any():
+        refl["pxs"] = plan.pxs
+    if verbose:
+        okk = np.isfinite(refl["iprf"])
+        log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - t0:.1f}s (device {t_dev:.1f}s)")
+    res = IntegrationResult(refl, model, prof_by_block, dict(total=time.time() - t0, gpu=t_dev))
+    res.block_params = block_params
+    return res
+
+
+def _host_pass1(p1: D.Pass1Buffers, rs: D.RowSet):
+    """Per-row pass-1 outputs on the host (one stacked float64 copy, `xpg/integrate_kernels.py:169-183`), plus the
+    per-frame fz array."""
+    keys = D.Pass1Buffers.SCALARS + D.Pass1Buffers.COUNTS
+    st = torch.stack([p1.t[k].double() for k in keys]).cpu().numpy()
+    h = {k: st[i].astype(np.float32 if k in D.Pass1Buffers.SCALARS else np.int64) for i, k in enumerate(keys)}
+    h["fz"] = p1.t["fz"].cpu().numpy()
+    return h
+
+
+def _fz_padded(h1, rs: D.RowSet, sel):
+    """fz of the selected rows, padded to the deepest box (zeros)."""
+    rows = np.flatnonzero(sel)
+    F = np.zeros((rows.size, MAX_DZ), np.float32)
+    for k, j in enumerate(rows):
+        o, dz = rs.frm_off[j], rs.Dz[j]
+        F[k, :dz] = h1["fz"][o:o + dz]
+    return F.astype(np.float64) if rows.size else F
+
+
+def _adapt_rows(h1, plan, rows):
+    """Strong rows of the per-block adaptation (`xpg/integrate.py:411-414`), float64 on the float32 outputs."""
+    isum = h1["isum"].astype(np.float64)
+    vs = h1["vsum"].astype(np.float64)
+    return (isum > 0) & (isum / np.sqrt(np.maximum(vs, 1e-6)) > 15) & (h1["n_over"] == 0) & \
+        (h1["frac_rec"].astype(np.float64) > 0.98) & (plan.fb[rows] == 1)
+
+
+def estimate_sigmas(images, exp, model0: IntegrationModel, dmin, frames, n_sample_frames=30, verbose=True, log=print,
+                    extra_exps=(), bkg_template=None, foreign_spots=None, max_iter=None, guard=None):
+    """sigma_D / sigma_M from strong spots (`xpg/integrate.py:1002-1092`), on moments-only device integrations."""
+    return A.estimate_sigmas(integrate, images, exp, model0, dmin, frames, n_sample_frames, verbose, log, extra_exps,
+                             bkg_template, foreign_spots, max_iter, guard)
