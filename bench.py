@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 shoebox integration (drop-in for XPG's INTEGRATE stage).
+
+Workload (default `config2-block`): one 360-frame phi block of the 16M-pixel sweep (4148 x 4362 px of 75 um at
+120 mm, lambda 0.98 A, 0.1 deg frames, P 21 21 21 60/85/120 A, sigma_M 0.15 deg, sigma_D 0.03 deg, background 0.2,
+5 x 5 profile regions). A step is one full `integrate()` call of the drop-in API on that block: predictions and shoebox
+plan, frame gather, pass 1, profile learning, adaptive widths, pass 2, results back on the host. The block's frames
+(every frame its boxes reach) are synthetic, seeded and rendered on the device before timing (`data`); the frame
+stack (~34 GB) is far larger than L2, so no flush is needed between steps.
+
+  value  reflections integrated per second with the frames resident in HBM (device-timed, CUDA events, max over
+         ranks), whole job over all ranks;
+  e2e    the same with the frames in pinned host memory, uploaded inside every step;
+  roofline  of the dominant kernel (largest share of device time): algorithmic bytes per launch / live CUDA-event
+         launch duration, against the measured HBM copy bandwidth;
+  cpu_baseline  the oracle (numpy restatement of the reference's CPU path) on a bounded sample of the same block.
+
+With --gpus N (torchrun, one rank per GPU) every rank integrates a block of its own sweep (replicas: sweeps are
+independent; weak scaling). `--impl reference` times the CPU restatement of the reference on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "integrated reflections/s (one 360-frame phi block of the 16M-pixel sweep per step)"
+UNIT = "refl/s"
+
+
+def _env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.gpu = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait(5)
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "0x1", "1"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class Block:
+    """One phi block of a synthetic sweep, planned and rendered on the device."""
+
+    def __init__(self, name, seed_offset=0, device="cuda"):
+        from xpg_b200 import synth
+        from xpg_b200.plan import IntegrationModel, plan_integration
+        if name == "config2-block":
+            self.spec = synth.config2(seed=2 + seed_offset)
+            self.edges = np.array([0.0, 360.0])
+        elif name == "config1":
+            self.spec = synth.config1(seed=1 + seed_offset)
+            self.edges = np.array([0.0, 100.0])
+        else:
+            raise ValueError(name)
+        s = self.spec
+        self.exp = s.experiment()
+        self.dmin = s.resolution_limit()
+        self.model = IntegrationModel(sigma_d=s.sigma_d, sigma_m=s.sigma_m)
+        # frames the block's boxes reach
+        probe = plan_integration([self.exp], self.edges, self.model, self.dmin, 1e9, (1, s.nframes), 0.05,
+                                 s.n_regions_xy, True, True)
+        self.n_frames = int(min(max(probe.need_hi) + 1, s.nframes))
+        self.plan = plan_integration([self.exp], self.edges, self.model, self.dmin, 1e9, (1, self.n_frames), 0.05,
+                                     s.n_regions_xy, True, True)
+        self.n_refl = self.plan.n
+        _, self.table = synth.reflection_table(s, z_range=(-5.0, self.n_frames + 5.0))
+        self.frames = synth.device_frames(s, self.table, 1, self.n_frames, device=device)
+        self.device = device
+
+    def integrate(self, frames):
+        from xpg_b200.integrate import integrate
+        return integrate(frames, [self.exp], self.edges, self.model, self.dmin, frames=(1, self.n_frames),
+                         verbose=False, n_regions_xy=self.spec.n_regions_xy)
+
+    def source(self, host=None):
+        from xpg_b200.frames import U32Frames
+        return U32Frames(self.frames if host is None else host, first=1, overload=self.spec.overload,
+                         device=self.device)
+
+    def bytes_per_kernel(self):
+        """Algorithmic bytes of every kernel over one step ("Roofline accounting")."""
+        p = self.plan
+        V = (p.Dz * p.bx * p.bx).astype(np.float64)
+        P = (p.bx * p.bx).astype(np.float64)
+        raw = (np.minimum(p.Dz * p.fb, np.maximum(self.n_frames - p.iz0, 0)) * (p.bx * p.pxs) ** 2).astype(np.float64)
+        return {"pass1": float((4 * V + 17 * P + 4 * p.Dz + 92).sum()),
+                "pass2": float((4 * V + 12 * P + 52).sum()),
+                "gather": float((4 * raw + 4 * V).sum()),
+                "decode_bins": float((8 * V * (p.fb > 1)).sum())}
+
+
+SAMPLE = dict(a=100, wz=24, crop=1024)     # frame window and detector crop of the CPU sample
+
+
+def _sample_rows(p, nx, ny):
+    """Rows of the CPU sample: boxes inside frames [a, a + wz) and inside a crop x crop detector patch."""
+    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
+    x0, y0 = nx // 2 + 300, ny // 2 + 300
+    x0, y0 = min(x0, nx - c), min(y0, ny - c)
+    inside = (p.iz0 >= a) & (p.iz0 + p.Dz * p.fb <= a + wz) & (p.pxs == 1) & \
+        (p.ix0 >= x0) & (p.ix0 + p.bx <= x0 + c) & (p.iy0 >= y0) & (p.iy0 + p.bx <= y0 + c)
+    return np.flatnonzero(inside), (y0, x0)
+
+
+def _frame_prep_seconds(raw_full, overload):
+    """Host time to prepare one full frame (encoding and mask ceiling, as XPG's frame loop does for every frame)."""
+    from oracle import gather as OG
+    ts = []
+    for f in raw_full:
+        t0 = time.perf_counter()
+        OG.prepare_frame(f, overload, 0, None)
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts))
+
+
+def _cpu_baseline(blk, budget_s=20.0, max_rows=400):
+    """The oracle restatement of the reference's CPU path on a bounded sample of the block, 1 core: gather, pass 1
+    and pass 2 of sample rows timed directly, plus each reflection's share of the full-frame preparation (one frame
+    timed, charged as frames / reflections of the block)."""
+    from oracle import kernels as OK
+    from oracle import pipeline as OP
+    p = blk.plan
+    s = blk.spec
+    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
+    rows, (y0, x0) = _sample_rows(p, s.nx, s.ny)
+    rows = rows[:max_rows]
+    full = blk.frames[a:a + 3].cpu().numpy().view(np.uint32)
+    t_prep = _frame_prep_seconds(full, s.overload)
+    raw = blk.frames[a:a + wz, y0:y0 + c, x0:x0 + c].cpu().numpy().view(np.uint32)
+    prep = OP.prepared_frames(raw, a, s.overload, [1])
+    g = blk.exp.geom
+    det = OK.detector_consts(g, None)
+    prof = np.repeat(OK.gaussian_profile()[None], p.nreg, 0)
+    prof = prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2)
+    t0 = time.perf_counter()
+    done = 0
+    for k in range(0, rows.size, 20):
+        OP.integrate_rows(prep, list(range(a, a + wz)), OP.row_payload(p, rows[k:k + 20]), det,
+                          g.s0.astype(np.float32), g.axis.astype(np.float32), np.float32(np.radians(g.z_to_phi(0.0))),
+                          np.float32(np.radians(g.osc)), np.radians(s.sigma_d), np.radians(s.sigma_m), 1.0,
+                          OK.rc_default_weights(), prof, origin=(y0, x0))
+        done = k + min(20, rows.size - k)
+        if time.perf_counter() - t0 > budget_s:
+            break
+    t_rows = time.perf_counter() - t0
+    per_refl = t_rows / max(done, 1) + t_prep * blk.n_frames / blk.n_refl
+    return {"value": round(1.0 / per_refl, 2), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{done} reflections of the block (boxes inside frames {a + 1}-{a + wz}): gather, pass 1 and "
+                      f"pass 2 by the numpy oracle in {t_rows:.1f} s, plus the block's full-frame preparation "
+                      f"({t_prep * 1e3:.0f} ms per frame x {blk.n_frames} frames) shared over its {blk.n_refl} "
+                      f"reflections"}
+
+
+def run(args):
+    import torch
+    rank, world, local = _env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from xpg_b200 import device as D
+    from xpg_b200.csrc import build
+    if build.stale():
+        build.build()
+    blk = Block(args.workload, seed_offset=rank)
+    src = blk.source()
+    for _ in range(args.warmup):
+        blk.integrate(src)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    D.TIMER.reset()
+    D.TIMER.enabled = True
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    n_ok = 0
+    for _ in range(args.steps):
+        res = blk.integrate(src)
+        n_ok += int(np.isfinite(res.refl["iprf"]).sum())
+    e1.record()
+    torch.cuda.synchronize()
+    D.TIMER.enabled = False
+    clk = clocks.stop()
+    t = e0.elapsed_time(e1) * 1e-3
+    ksum = D.TIMER.summary()
+    launches = D.TIMER.launches
+    t_max = t
+    n_total = blk.n_refl * args.steps
+    if dist is not None:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        nn = torch.tensor([n_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(nn)
+        n_total = int(nn.item())
+    value = n_total / t_max
+    # roofline of the dominant kernel
+    peak, peak_kind = _peaks()
+    bpk = blk.bytes_per_kernel()
+    dom = max(ksum, key=lambda k: ksum[k][1]) if ksum else None
+    roof = None
+    if dom is not None:
+        n_l, t_k = ksum[dom]
+        per_launch = bpk.get(dom, 0.0) * args.steps / max(n_l, 1)
+        achieved = per_launch / (t_k / n_l) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "launches": n_l, "ms_per_launch": round(t_k / n_l * 1e3, 4),
+                "share": {k: round(v[1] / max(sum(x[1] for x in ksum.values()), 1e-12), 4) for k, v in ksum.items()}}
+    # end to end: frames from pinned host memory, uploaded inside every step; results read back by the API
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(blk.frames.shape, dtype=torch.int32, pin_memory=True)
+        host.copy_(blk.frames)
+        hsrc = blk.source(host)
+        blk.integrate(hsrc)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        k2 = max(1, min(args.steps, args.e2e_steps))
+        f0.record()
+        for _ in range(k2):
+            res = blk.integrate(hsrc)
+        f1.record()
+        torch.cuda.synchronize()
+        te = f0.elapsed_time(f1) * 1e-3
+        if dist is not None:
+            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        n_out = sum(v.nbytes for v in res.refl.values() if isinstance(v, np.ndarray))
+        e2e = {"value": round(blk.n_refl * world * k2 / te, 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(host.numel() * 4), "d2h_bytes_per_step": int(n_out), "steps": k2}
+        del host
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = _cpu_baseline(blk)
+    if dist is not None:
+        dist.barrier()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulation)",
+                "data": "synthetic: seeded 16M-pixel frames rendered on the device (spec in xpg_b200/synth.py)",
+                "config": {"workload": args.workload, "reflections_per_step": blk.n_refl,
+                           "frames_per_step": blk.n_frames, "detector": [blk.spec.nx, blk.spec.ny],
+                           "voxels_per_step": int((blk.plan.Dz * blk.plan.bx ** 2).sum()),
+                           "l2": "inputs larger than L2 (frame stack ~{:.0f} GB)".format(blk.frames.numel() * 4 / 1e9),
+                           "parallelism": f"replicas x{world} (one block per rank)"},
+                "integrated_per_step": n_ok // max(args.steps, 1),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _ref_worker(args_tuple):
+    """Oracle work of one chunk of rows (spawned process): gather, pass 1, pass 2 from prepared frame crops."""
+    (prep, a, wz, payload, spec_d, nreg, origin) = args_tuple
+    from oracle import kernels as OK
+    from oracle import pipeline as OP
+    from xpg_b200 import synth
+    spec = synth.SweepSpec(**spec_d)
+    g = spec.geometry()
+    det = OK.detector_consts(g, None)
+    prof = np.repeat(OK.gaussian_profile()[None], nreg, 0)
+    prof = prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2)
+    OP.integrate_rows(prep, list(range(a, a + wz)), payload, det, g.s0.astype(np.float32), g.axis.astype(np.float32),
+                      np.float32(np.radians(g.z_to_phi(0.0))), np.float32(np.radians(g.osc)),
+                      np.radians(spec.sigma_d), np.radians(spec.sigma_m), 1.0, OK.rc_default_weights(), prof,
+                      origin=origin)
+    return len(payload)
+
+
+def reference_arm(args):
+    """The reference's CPU path (its numpy restatement in oracle/) on all host cores: per step a bounded sample of
+    the block's reflections (gather, pass 1, pass 2 spread over spawned processes) plus their share of the block's
+    full-frame preparation (one frame timed per step, frames spread over the cores as XPG's decode pool does)."""
+    rank, world, local = _env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from dataclasses import asdict
+
+    import torch
+    from oracle import pipeline as OP
+    from xpg_b200 import synth
+    from xpg_b200.plan import IntegrationModel, plan_integration
+    cores = len(os.sched_getaffinity(0))
+    spec = synth.config2() if args.workload == "config2-block" else synth.config1()
+    edges = np.array([0.0, 360.0]) if args.workload == "config2-block" else np.array([0.0, 100.0])
+    exp = spec.experiment()
+    model = IntegrationModel(spec.sigma_d, spec.sigma_m)
+    dmin = spec.resolution_limit()
+    probe = plan_integration([exp], edges, model, dmin, 1e9, (1, spec.nframes), 0.05, spec.n_regions_xy, True, True)
+    n_frames = int(min(max(probe.need_hi) + 1, spec.nframes))
+    p = plan_integration([exp], edges, model, dmin, 1e9, (1, n_frames), 0.05, spec.n_regions_xy, True, True)
+    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
+    rows_all, (y0, x0) = _sample_rows(p, spec.nx, spec.ny)
+    _, table = synth.reflection_table(spec, z_range=(a - 40.0, a + wz + 40.0))
+    if torch.cuda.is_available():
+        raw = synth.device_frames(spec, table, a + 1, wz).cpu().numpy().view(np.uint32)
+    else:
+        raw = synth.render_frames(spec, range(a + 1, a + wz + 1), table)
+    prep = OP.prepared_frames(raw[:, y0:y0 + c, x0:x0 + c], a, spec.overload, [1])
+    per_step = max(cores * 4, 16)
+    sd = asdict(spec)
+    sd.pop("U", None)
+    ctx = mp.get_context("spawn")
+    n_done, t_all = 0, 0.0
+    with ctx.Pool(cores) as pool:
+        def step(k):
+            lo = (k * per_step) % max(rows_all.size - per_step, 1)
+            rows = rows_all[lo:lo + per_step]
+            chunks = [OP.row_payload(p, rows[i::cores]) for i in range(cores)]
+            t0 = time.perf_counter()
+            n = sum(pool.map(_ref_worker, [(prep, a, wz, ch, sd, p.nreg, (y0, x0)) for ch in chunks if ch]))
+            t_rows = time.perf_counter() - t0
+            t_prep = _frame_prep_seconds(raw[:1], spec.overload)
+            return n, t_rows + t_prep * n_frames / p.n * n / cores
+        for k in range(args.warmup):
+            step(k)
+        for k in range(args.steps):
+            n, t = step(args.warmup + k)
+            n_done += n
+            t_all += t
+    value = n_done / t_all
+    line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_all / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulation)", "impl": "reference",
+            "data": "synthetic: seeded 16M-pixel frames (spec in xpg_b200/synth.py)",
+            "config": {"workload": args.workload, "reflections_per_step": per_step},
+            "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{per_step} reflections per step of the block (boxes inside frames "
+                                       f"{a + 1}-{a + wz}, a {c} px detector patch): gather + pass 1 + pass 2 by the "
+                                       f"numpy restatement over {cores} spawned processes, plus their share of the "
+                                       f"block's full-frame preparation"},
+            "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--workload", default="config2-block", choices=("config2-block", "config1"))
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        run(args)
+
+
+if __name__ == "__main__":
+    main()

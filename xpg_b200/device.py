@@ -15,6 +15,53 @@ from . import native as N
 F32 = torch.float32
 
 
+class KernelTimer:
+    """Optional per-kernel CUDA-event timing of the library calls (pairs of events on the launching stream around
+    each call) and a count of kernel launches. Off unless `TIMER.enabled`; read after a synchronize."""
+
+    def __init__(self):
+        self.enabled = False
+        self.reset()
+
+    def reset(self):
+        self.events = []                 # (name, start, end)
+        self.launches = 0
+
+    def span(self, name, n_launches=1):
+        return _Span(self, name, n_launches)
+
+    def summary(self):
+        out = {}
+        for name, a, b in self.events:
+            t = a.elapsed_time(b) * 1e-3
+            d = out.setdefault(name, [0, 0.0])
+            d[0] += 1
+            d[1] += t
+        return out
+
+
+class _Span:
+    def __init__(self, timer, name, n):
+        self.t, self.name, self.n = timer, name, n
+
+    def __enter__(self):
+        self.t.launches += self.n
+        if self.t.enabled:
+            self.a = torch.cuda.Event(enable_timing=True)
+            self.a.record()
+        return self
+
+    def __exit__(self, *exc):
+        if self.t.enabled:
+            b = torch.cuda.Event(enable_timing=True)
+            b.record()
+            self.t.events.append((self.name, self.a, b))
+        return False
+
+
+TIMER = KernelTimer()
+
+
 def _dev(a, dtype, device):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(device, non_blocking=False)
 
@@ -186,8 +233,9 @@ def pass1(det: DeviceDetector, rows: RowSet, blk, arena, out: Pass1Buffers, stre
     lib = N.load()
     for bxg, dzg, order in (groups if groups is not None else _device_groups(rows)):
         r = rows.view(order, bxg, dzg)
-        N.check(lib.xi_pass1(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), C.byref(out.s),
-                             _stream(stream)), "xi_pass1")
+        with TIMER.span("pass1"):
+            N.check(lib.xi_pass1(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), C.byref(out.s),
+                                 _stream(stream)), "xi_pass1")
 
 
 def pass2(det: DeviceDetector, rows: RowSet, blk, arena, prof, p1: Pass1Buffers, out: Pass2Buffers, stream=None,
@@ -196,22 +244,25 @@ def pass2(det: DeviceDetector, rows: RowSet, blk, arena, prof, p1: Pass1Buffers,
     i2 = p1.pass2_in()
     for bxg, dzg, order in (groups if groups is not None else _device_groups(rows)):
         r = rows.view(order, bxg, dzg)
-        N.check(lib.xi_pass2(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), N.ptr(prof), C.byref(i2),
-                             C.byref(out.s), _stream(stream)), "xi_pass2")
+        with TIMER.span("pass2"):
+            N.check(lib.xi_pass2(C.byref(det.s), C.byref(r), C.byref(blk), N.ptr(arena), N.ptr(prof), C.byref(i2),
+                                 C.byref(out.s), _stream(stream)), "xi_pass2")
 
 
 def accumulate(rows: RowSet, p1: Pass1Buffers, n_regions, num, den, sel=None, strong_test=True, order=None,
                stream=None):
     lib = N.load()
     r = rows.view(order)
-    N.check(lib.xi_accumulate(C.byref(r), C.byref(p1.s), N.ptr(sel), 1 if strong_test else 0, int(n_regions),
-                              N.ptr(num), N.ptr(den), _stream(stream)), "xi_accumulate")
+    with TIMER.span("accumulate"):
+        N.check(lib.xi_accumulate(C.byref(r), C.byref(p1.s), N.ptr(sel), 1 if strong_test else 0, int(n_regions),
+                                  N.ptr(num), N.ptr(den), _stream(stream)), "xi_accumulate")
 
 
 def finalize_profiles(num, den, prof, stream=None):
     lib = N.load()
-    N.check(lib.xi_finalize_profiles(N.ptr(num), N.ptr(den), int(num.shape[0]), N.ptr(prof), _stream(stream)),
-            "xi_finalize_profiles")
+    with TIMER.span("finalize"):
+        N.check(lib.xi_finalize_profiles(N.ptr(num), N.ptr(den), int(num.shape[0]), N.ptr(prof), _stream(stream)),
+                "xi_finalize_profiles")
 
 
 def status(stream=None):
@@ -279,9 +330,12 @@ def frames_struct(data, first_fi, overload, min_valid=0, mask=None, frame_ok=Non
 def gather(frames_s, grows: GatherRows, order, arena, cnt, stream=None):
     lib = N.load()
     g = grows.view(order)
-    N.check(lib.xi_gather(C.byref(frames_s), C.byref(g), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_gather")
+    with TIMER.span("gather"):
+        N.check(lib.xi_gather(C.byref(frames_s), C.byref(g), N.ptr(arena), N.ptr(cnt), _stream(stream)),
+                "xi_gather")
 
 
 def decode_bins(grows: GatherRows, arena, cnt, stream=None):
     lib = N.load()
-    N.check(lib.xi_decode_bins(C.byref(grows.s), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")
+    with TIMER.span("decode_bins"):
+        N.check(lib.xi_decode_bins(C.byref(grows.s), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")

@@ -66,6 +66,16 @@ class XiFrames(C.Structure):
                 ("mask", _fp)]
 
 
+class XiSynthSpots(C.Structure):
+    _fields_ = [("n", C.c_int), ("x", _fp), ("y", _fp), ("z", _fp), ("counts", _fp), ("sig_t", _fp),
+                ("sig_r", _fp), ("sig_z", _fp), ("orgx", C.c_double), ("orgy", C.c_double)]
+
+
+class XiSynthBackground(C.Structure):
+    _fields_ = [("level", C.c_double), ("ramp", C.c_double), ("orgx", C.c_double), ("orgy", C.c_double),
+                ("rmax", C.c_double)]
+
+
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_gather", "xi_decode_bins", "xi_pass1", "xi_accumulate",
            "xi_finalize_profiles", "xi_pass2")
 
@@ -95,6 +105,10 @@ def load(path=None):
     lib.xi_finalize_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.xi_pass2.argtypes = [C.POINTER(XiDetector), C.POINTER(XiRows), C.POINTER(XiBlock), C.c_void_p, C.c_void_p,
                              C.POINTER(XiPass2In), C.POINTER(XiPass2Out), C.c_void_p]
+    lib.xi_synth_frames.restype = C.c_int
+    lib.xi_synth_frames.argtypes = [C.POINTER(XiSynthSpots), C.POINTER(XiSynthBackground), C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p]
+    lib.xi_synth_last_error.restype = C.c_char_p
     if path is None:
         _LIB = lib
     return lib

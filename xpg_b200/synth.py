@@ -143,9 +143,9 @@ def _hash_unit(keys, salt):
     return ((x >> np.uint64(11)).astype(np.float64) + 0.5) / float(2 ** 53)
 
 
-def reflection_table(spec: SweepSpec, z_margin=5.0):
-    """Predicted reflections of the sweep (z in [-margin, nframes + margin)) with their true photon counts and the
-    spot widths used to render them."""
+def reflection_table(spec: SweepSpec, z_margin=5.0, z_range=None):
+    """Predicted reflections of the sweep (z in [-margin, nframes + margin), or in z_range) with their true photon
+    counts and the spot widths used to render them."""
     exp = spec.experiment()
     g = exp.geom
     A = exp.crystal.Astar
@@ -153,7 +153,8 @@ def reflection_table(spec: SweepSpec, z_margin=5.0):
     from .geometry import generate_hkl
     hkl = generate_hkl(A, dmin)
     hkl = hkl[centring_allowed(hkl, spec.space_group)]
-    pr = predict_reflections(g, A, dmin, z_range=(-z_margin, spec.nframes + z_margin), hkl=hkl)
+    zr = (-z_margin, spec.nframes + z_margin) if z_range is None else z_range
+    pr = predict_reflections(g, A, dmin, z_range=zr, hkl=hkl)
     key = ((pr["hkl"][:, 0].astype(np.int64) + 1024) << 22) + ((pr["hkl"][:, 1].astype(np.int64) + 1024) << 11) \
         + (pr["hkl"][:, 2].astype(np.int64) + 1024)
     d = 1.0 / np.linalg.norm(pr["S"] - g.s0, axis=1)
@@ -284,3 +285,36 @@ def encode_frame(raw, overload, min_valid=0, mask=None):
 
 def replace_spec(spec, **kw):
     return replace(spec, **kw)
+
+
+def device_frames(spec: SweepSpec, table, first_frame, n_frames, out=None, device="cuda", stream=None):
+    """Frames first_frame .. first_frame + n_frames - 1 rendered on the device (int32 view of uint32 counts),
+    shape (n_frames, ny, nx). Same model as `render_frames`, with a device counter-based Poisson draw (so the pixel
+    values differ from the host generator's)."""
+    import ctypes as C
+
+    import torch
+
+    from . import native as N
+    N.require_cuda()
+    if out is None:
+        out = torch.empty((n_frames, spec.ny, spec.nx), dtype=torch.int32, device=device)
+    g = spec.geometry()
+    keep = (table["z"] + 5 * table["sig_z"] > first_frame - 1) & (table["z"] - 5 * table["sig_z"] < first_frame - 1 + n_frames)
+    t = {k: torch.as_tensor(np.ascontiguousarray(table[k][keep], np.float64)).to(device)
+         for k in ("x", "y", "z", "counts", "sig_t", "sig_r", "sig_z")}
+    sp = N.XiSynthSpots()
+    sp.n = int(keep.sum())
+    for k, v in t.items():
+        setattr(sp, k, N.ptr(v))
+    sp.orgx, sp.orgy = float(g.orgx), float(g.orgy)
+    bg = N.XiSynthBackground()
+    bg.level, bg.ramp, bg.orgx, bg.orgy = spec.background, spec.ramp, float(g.orgx), float(g.orgy)
+    cx = np.array([1.0, spec.nx, 1.0, spec.nx])
+    cy = np.array([1.0, 1.0, spec.ny, spec.ny])
+    bg.rmax = float(max(np.hypot(cx - g.orgx, cy - g.orgy).max(), 1.0))
+    rc = N.load().xi_synth_frames(C.byref(sp), C.byref(bg), int(first_frame), int(n_frames), spec.ny, spec.nx,
+                                  int(spec.seed), 1 if spec.gaps else 0, N.ptr(out), N.stream_handle(stream))
+    if rc != 0:
+        raise RuntimeError("xi_synth_frames: " + N.load().xi_synth_last_error().decode())
+    return out
