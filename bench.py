@@ -104,6 +104,9 @@ class Block:
         if name == "config2-block":
             self.spec = synth.config2(seed=2 + seed_offset)
             self.edges = np.array([0.0, 360.0])
+        elif name == "config2-small":          # a 20-frame block of the same sweep (profiling captures)
+            self.spec = synth.config2(seed=2 + seed_offset)
+            self.edges = np.array([0.0, 20.0])
         elif name == "config1":
             self.spec = synth.config1(seed=1 + seed_offset)
             self.edges = np.array([0.0, 100.0])
@@ -411,7 +414,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--workload", default="config2-block", choices=("config2-block", "config1"))
+    ap.add_argument("--workload", default="config2-block", choices=("config2-block", "config2-small", "config1"))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

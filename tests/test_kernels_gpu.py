@@ -90,8 +90,9 @@ EXACT = ("n_over", "n_fg_masked", "n_fg_nb", "nfg", "bg", "nbg", "zeta", "seff",
 
 
 def test_pass1_matches_oracle(case_results):
-    """Integer counts, masks, the background and every per-pixel geometric term are bit-exact with the oracle;
-    the float64-accumulated sums agree to their float32 rounding."""
+    """Integer counts, masks, the background and every per-pixel geometric term are bit-exact with the oracle; the
+    accumulated sums (float32 within a pixel column, float64 across columns on the device; float64 throughout in
+    the oracle) agree within 1e-5 of their scale."""
     case, results = case_results
     for r in results:
         d, rc, nb = r["d"], r["rc"], r["nb"]
@@ -103,7 +104,7 @@ def test_pass1_matches_oracle(case_results):
                 a, b = np.asarray(mine[k]), np.asarray(ref[k])
                 assert np.array_equal(a.astype(np.float64), b.astype(np.float64)), (case, r["chunk"], j, k)
             for k in ("isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "img2", "fz"):
-                ok, worst = T.within(k, mine[k], ref[k], ref, rel=2e-6)
+                ok, worst = T.within(k, mine[k], ref[k], ref, rel=1e-5)
                 assert ok, (case, r["chunk"], j, k, worst)
 
 

@@ -38,6 +38,7 @@ constexpr float kSbOff = 3.0f;     // shoeboxes are stored as value + 3 (0 = unr
 struct NbShared {
     int nact;
     int act[XI_MAX_K];
+    int zmin[XI_MAX_K];             // frame of the smallest dz^2 of each active neighbour
     float dx2[XI_MAX_K][XI_MAX_BX];
     float dy2[XI_MAX_K][XI_MAX_BX];
     float dz2[XI_MAX_K][XI_MAX_DZ];
@@ -80,16 +81,47 @@ __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const 
         }
     }
     __syncthreads();
+    for (int a = threadIdx.x; a < nb.nact; a += blockDim.x) {
+        int zm = 0;
+        for (int z = 1; z < Dz; ++z)
+            if (nb.dz2[a][z] < nb.dz2[a][zm]) zm = z;
+        nb.zmin[a] = zm;
+    }
+    __syncthreads();
 }
 
-// frames of pixel (i, j) inside any active neighbour's ellipsoid: ((dx^2 + dy^2) + dz^2 < 1)
+// Frames of pixel (i, j) inside any active neighbour's ellipsoid: ((dx^2 + dy^2) + dz^2 < 1). dz^2 over the frames
+// is unimodal (the bin centres increase, float subtraction, division and squaring are monotone), so for a given
+// dx^2 + dy^2 the frames that pass form one interval around the minimum: found by two binary searches on the same
+// float comparisons as a full scan.
 __device__ __forceinline__ Mask65 neighbour_frames(const NbShared& nb, int i, int j, int Dz) {
     Mask65 m;
     m.clear();
     for (int a = 0; a < nb.nact; ++a) {
-        float dxy = nb.dx2[a][i] + nb.dy2[a][j];
-        for (int z = 0; z < Dz; ++z)
-            if (dxy + nb.dz2[a][z] < 1.0f) m.set(z);
+        const float dxy = nb.dx2[a][i] + nb.dy2[a][j];
+        const float* d2 = nb.dz2[a];
+        const int zm = nb.zmin[a];
+        if (!(dxy + d2[zm] < 1.0f)) continue;
+        int lo = 0, hi = zm;                 // first z in [0, zm] that passes
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (dxy + d2[mid] < 1.0f) hi = mid; else lo = mid + 1;
+        }
+        const int z0 = lo;
+        lo = zm;
+        hi = Dz - 1;                         // last z in [zm, Dz - 1] that passes
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (dxy + d2[mid] < 1.0f) lo = mid; else hi = mid - 1;
+        }
+        const int z1 = lo;
+        // bits z0..z1
+        if (z0 < 64) {
+            const int e = min(z1, 63);
+            const unsigned long long upto = (e == 63) ? ~0ull : ((1ull << (e + 1)) - 1ull);
+            m.lo |= upto & ~((1ull << z0) - 1ull);
+        }
+        if (z1 >= 64) m.hi |= 1u;            // Dz <= 65: bit 64 only
     }
     return m;
 }
@@ -152,15 +184,114 @@ __device__ void box_geometry(const XiDetector& det, const float S[3], const floa
 }
 
 // ==================================================================================================================
+// shared per-CTA helpers
+// ==================================================================================================================
+
+// Rocking-curve fractions of all Dz bins: the Dz x 21 mixture terms are spread over the CTA, then each bin sums its
+// terms in component order in float64 (same value as rocking_fraction, computed 21x wider).
+__device__ void rocking_curve_cta(int Dz, int iz0, float fb, const XiBlock& B, const float* rcw, float phi,
+                                  float zeta, float* terms, float* R) {
+    const float s = B.sm / fmaxf(fabsf(zeta), 1e-3f);
+    const float sw = (s * 0.25f) * kSqrt2;
+    for (int q = threadIdx.x; q < Dz * XI_RC_K; q += blockDim.x) {
+        const int z = q / XI_RC_K, k = q % XI_RC_K;
+        float lo, hi;
+        bin_limits(iz0, fb, z, B.frames_phi0, B.osc, &lo, &hi);
+        const float c = (k == XI_RC_K - 1) ? 3.5f : (float)((double)k * 0.35 + (-3.5));
+        const float cs = c * s;
+        const float a = ((hi - phi) - cs) / sw;
+        const float b = ((lo - phi) - cs) / sw;
+        terms[q] = (rcw[k] * 0.5f) * (erf32(a) - erf32(b));
+    }
+    __syncthreads();
+    for (int z = threadIdx.x; z < Dz; z += blockDim.x) {
+        double acc = 0.0;
+        for (int k = 0; k < XI_RC_K; ++k) acc += (double)terms[z * XI_RC_K + k];
+        R[z] = (float)acc;
+    }
+    __syncthreads();
+}
+
+// Per-pixel neighbour frame masks and background template of a box, computed once (shared memory).
+__device__ void pixel_tables(const XiDetector& det, const NbShared& nb, int bx, int Dz, const float* xs,
+                             const float* ys, unsigned long long* nblo, unsigned* nbhi, float* brefs) {
+    const int P = bx * bx;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const int i = p % bx, j = p / bx;
+        const Mask65 m = neighbour_frames(nb, i, j, Dz);
+        nblo[p] = m.lo;
+        nbhi[p] = m.hi;
+        brefs[p] = bkg_ref(det, xs[i], ys[j]);
+    }
+    __syncthreads();
+}
+
+// Per-CTA shared copies of the small tables every pixel reads: the panel maps (up to 16 panels) and the rocking-curve
+// weights. Returns the detector description with its panel pointers redirected to the shared copies.
+constexpr int kSmemPanels = 16;
+struct CtaTables {
+    float pan[6][3 * kSmemPanels];
+    float rcw[XI_RC_K];
+};
+
+__device__ XiDetector cta_tables(const XiDetector& det, const XiBlock& B, CtaTables& T) {
+    XiDetector d = det;
+    const int np = det.n_panels;
+    if (np <= kSmemPanels) {
+        for (int r = threadIdx.x; r < 3 * np; r += blockDim.x) {
+            T.pan[0][r] = det.P0[r];
+            T.pan[1][r] = det.Bx[r];
+            T.pan[2][r] = det.By[r];
+            T.pan[3][r] = det.U1[r];
+            T.pan[4][r] = det.U2[r];
+            T.pan[5][r] = det.UN[r];
+        }
+        d.P0 = T.pan[0];
+        d.Bx = T.pan[1];
+        d.By = T.pan[2];
+        d.U1 = T.pan[3];
+        d.U2 = T.pan[4];
+        d.UN = T.pan[5];
+    }
+    for (int k = threadIdx.x; k < XI_RC_K; k += blockDim.x) T.rcw[k] = B.rcw[k];
+    return d;
+}
+
+// Completes the staging of a shoebox in shared memory: waits for the bulk copy (bounded; on a timeout the status
+// word gets bit 2 and the values are copied with plain loads), or copies with plain loads when the row's arena
+// offset is not 16-byte aligned. Ends with a barrier.
+__device__ void stage_wait(bool tma, unsigned long long* bar, float* stage, const float* sb, int V, int* status) {
+    bool ok = true;
+    if (tma) ok = mbar_wait(bar, 0, 1ll << 24);
+    if (!tma || !ok) {
+        if (!ok && threadIdx.x == 0) atomicOr(status, 2);
+        __syncthreads();
+        for (int v = threadIdx.x; v < V; v += blockDim.x) stage[v] = sb[v];
+    } else {
+        // the bulk copy moved whole 16-byte units; the last 0..3 values come with plain loads (no read past the row)
+        for (int v = (V & ~3) + threadIdx.x; v < V; v += blockDim.x) stage[v] = sb[v];
+    }
+    __syncthreads();
+}
+
+// ==================================================================================================================
 // pass 1
 // ==================================================================================================================
-template <int NT>
-__global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock B, const float* __restrict__ arena,
+constexpr int kClipCand = 2048;     // background voxels above the lowest clip threshold kept per CTA
+
+// Dynamic shared memory: nblo (8P) | geometry scratch e1s/e2s (8P), then brefs (4P) + nbhi (4P) | flags (P, padded
+// to 16) | staged shoebox (4V, when STAGED).
+__host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)17 * P + 15) / 16 * 16; }
+
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
                                               XiPass1Out O, const int32_t* __restrict__ order, int max_bx,
                                               int max_dz, int* status) {
-    extern __shared__ float dyn[];
+    extern __shared__ __align__(16) unsigned char dyn1[];
+    __shared__ CtaTables T;
     __shared__ float xs[XI_MAX_BX], ys[XI_MAX_BX];
     __shared__ float fR[XI_MAX_DZ], fzz[XI_MAX_DZ], fe3[XI_MAX_DZ];
+    __shared__ float terms[XI_MAX_DZ * XI_RC_K];
     __shared__ NbShared nb;
     __shared__ float s_e1[3], s_e2[3], s_S[3], s_zeta, s_seff, s_b;
     __shared__ unsigned long long s_fgz_lo, s_rec_lo;
@@ -168,6 +299,11 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
     __shared__ double red[NT / 32 * 16];
     __shared__ double tot[16];
     __shared__ float fzw[NT / 32][XI_MAX_DZ];
+    // background voxels above the lowest possible clip threshold (the only ones the iterations can drop)
+    __shared__ float cand_v[kClipCand];
+    __shared__ unsigned short cand_p[kClipCand];
+    __shared__ int s_ncand;
+    __shared__ double s_base[2];
 
     const int row = order ? order[blockIdx.x] : blockIdx.x;
     const int Dz = R.Dz[row], bx = R.bx[row];
@@ -176,8 +312,14 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
         return;
     }
     const int P = bx * bx;
-    float* u1s = dyn;
-    float* u2s = dyn + P;
+    const int Pm = max_bx * max_bx;                // the tables are laid out for the launch's largest box
+    unsigned long long* nblo = reinterpret_cast<unsigned long long*>(dyn1);
+    float* e1s = reinterpret_cast<float*>(dyn1 + (size_t)8 * Pm);
+    float* e2s = e1s + Pm;
+    float* brefs = e1s;                            // reuses the geometry scratch once u1 / u2 are out
+    unsigned* nbhi = reinterpret_cast<unsigned*>(e1s + Pm);
+    unsigned char* flags = dyn1 + (size_t)16 * Pm;
+    float* stage = reinterpret_cast<float*>(dyn1 + pass1_pix_bytes(Pm));
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
     const float fb = R.fb[row];
@@ -185,14 +327,28 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
     const float* sb = arena + R.sb_off[row];
     const int64_t po = R.pix_off[row], fo = R.frm_off[row];
     const float gain = B.gain;
+    auto voxel = [&](int z, int p) -> float {
+        return STAGED ? stage[(size_t)z * P + p] : sb[(size_t)z * P + p] - R.sb_bias;
+    };
+    // the shoebox streams into shared memory (bulk copy) while the geometry below is computed
+    __shared__ __align__(8) unsigned long long s_bar;
+    const unsigned vbytes = (unsigned)(((size_t)Dz * P * sizeof(float)) & ~(size_t)15);   // whole 16-byte units
+    const bool tma = STAGED && vbytes > 0 && ((reinterpret_cast<uintptr_t>(sb) & 15) == 0) &&
+                     ((reinterpret_cast<uintptr_t>(stage) & 15) == 0);
+    if (tma && threadIdx.x == 0) {
+        mbar_init(&s_bar, 1);
+        mbar_expect_tx(&s_bar, vbytes);
+        bulk_copy_g2s(stage, sb, vbytes, &s_bar);
+    }
 
+    const XiDetector det = cta_tables(det_g, B, T);
     if (threadIdx.x == 0) {
         float S[3] = {R.S[3 * row], R.S[3 * row + 1], R.S[3 * row + 2]};
         float e1[3], e2[3], zeta;
         kabsch_frame(S, B.s0, B.axis, e1, e2, &zeta);
         for (int c = 0; c < 3; ++c) { s_e1[c] = e1[c]; s_e2[c] = e2[c]; s_S[c] = S[c]; }
         s_zeta = zeta;
-        s_fgz_lo = 0ull; s_fgz_hi = 0u; s_rec_lo = 0ull; s_rec_hi = 0u;
+        s_rec_lo = 0ull; s_rec_hi = 0u;
     }
     for (int i = threadIdx.x; i < bx; i += NT) {
         xs[i] = box_coord(ix0, i, pxs);
@@ -201,24 +357,30 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
     for (int z = threadIdx.x; z < Dz; z += NT) fzz[z] = (float)iz0 + fb * ((float)z + 0.5f);
     __syncthreads();
     const float zeta = s_zeta;
-    // frame terms: rocking-curve fractions, e3 of the bin centres
+    rocking_curve_cta(Dz, iz0, fb, B, T.rcw, phi, zeta, terms, fR);
     for (int z = threadIdx.x; z < Dz; z += NT) {
         float lo, hi;
         bin_limits(iz0, fb, z, B.frames_phi0, B.osc, &lo, &hi);
-        fR[z] = rocking_fraction(lo, hi, phi, zeta, B.sm, B.rcw);
-        float phic = 0.5f * (lo + hi);
-        fe3[z] = zeta * (phic - phi);
+        fe3[z] = zeta * (0.5f * (lo + hi) - phi);
     }
     {
         float e1[3] = {s_e1[0], s_e1[1], s_e1[2]}, e2[3] = {s_e2[0], s_e2[1], s_e2[2]};
         float S[3] = {s_S[0], s_S[1], s_S[2]};
-        box_geometry(det, S, e1, e2, bx, xs, ys, B.sd, u1s, u2s, O.J + po, nullptr, &s_seff);
+        box_geometry(det, S, e1, e2, bx, xs, ys, B.sd, e1s, e2s, O.J + po, nullptr, &s_seff);
+    }
+    // u1 / u2 out, foreground / background-ring flags per pixel
+    for (int p = threadIdx.x; p < P; p += NT) {
+        const float u1 = e1s[p], u2 = e2s[p];
+        O.u1[po + p] = u1;
+        O.u2[po + p] = u2;
+        const float r2 = u1 * u1 + u2 * u2;
+        flags[p] = (r2 <= kFgR2 ? 1 : 0) | (r2 >= kBgR2 ? 2 : 0);
     }
     // foreground frames: R >= 1e-3 * Rmax + 1e-6
     if (threadIdx.x == 0) {
         float Rmax = fR[0];
         for (int z = 1; z < Dz; ++z) Rmax = fmaxf(Rmax, fR[z]);
-        float thr = 1e-3f * Rmax + 1e-6f;
+        const float thr = 1e-3f * Rmax + 1e-6f;
         Mask65 m;
         m.clear();
         for (int z = 0; z < Dz; ++z)
@@ -226,30 +388,43 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
         s_fgz_lo = m.lo;
         s_fgz_hi = m.hi;
     }
-    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, false, nb);
+    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, false, nb);     // ends with a barrier
+    pixel_tables(det, nb, bx, Dz, xs, ys, nblo, nbhi, brefs);
     Mask65 fgz;
     fgz.lo = s_fgz_lo;
     fgz.hi = s_fgz_hi;
     const float seff = s_seff;
 
     // ---- pass A: first background estimate, counts, recorded frames ------------------------------------------
-    double acc[16];
+    // The clip threshold (bp + 3 sqrt(gain max(bp, 0.5))) + 1 is non-decreasing in bp = b * bref >= 0 (every
+    // float operation in it is monotone), so it never falls below its value at bp = 0: background voxels at or
+    // below that bound pass every iteration. They are summed here once; the others are listed for the iterations.
+    if (STAGED) stage_wait(tma, &s_bar, stage, sb, Dz * P, status);
+    const float clip_floor = (0.0f + 3.0f * sqrtf(gain * fmaxf(0.0f, 0.5f))) + 1.0f;
+    if (threadIdx.x == 0) s_ncand = 0;
+    int neg_bref = 0;
+    for (int p = threadIdx.x; p < P; p += NT) neg_bref |= (brefs[p] < 0.0f);
+    const bool use_list = !__syncthreads_or(neg_bref);
     long long n_over = 0, n_fg_masked = 0, n_fg_nb = 0;
-    Mask65 rec;
-    rec.clear();
     {
-        double sc = 0.0, sb_ = 0.0;
+        Mask65 rec;
+        rec.clear();
+        double sc = 0.0, sb_ = 0.0, sc0 = 0.0, sb0 = 0.0;
         for (int p = threadIdx.x; p < P; p += NT) {
-            const int i = p % bx, j = p / bx;
-            const float u1 = u1s[p], u2 = u2s[p];
-            O.u1[po + p] = u1;
-            O.u2[po + p] = u2;
-            const float r2 = u1 * u1 + u2 * u2;
-            const bool fg2 = r2 <= kFgR2, ring = r2 >= kBgR2;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
+            const unsigned char fl = flags[p];
+            const bool fg2 = fl & 1, ring = fl & 2;
+            const float bref = brefs[p];
+            Mask65 nbm;
+            nbm.lo = nblo[p];
+            nbm.hi = nbhi[p];
             for (int z = 0; z < Dz; ++z) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
+                float v;
+                if (STAGED) {
+                    v = stage[(size_t)z * P + p] - R.sb_bias;
+                    stage[(size_t)z * P + p] = v;
+                } else {
+                    v = sb[(size_t)z * P + p] - R.sb_bias;
+                }
                 const bool valid = v >= 0.0f, recd = v > -2.5f, over = v == -2.0f;
                 const bool fg = fg2 && fgz.get(z);
                 const bool nbz = nbm.get(z);
@@ -260,40 +435,68 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
                 if (valid && !fg && !nbz && ring) {
                     sc += (double)v;
                     sb_ += (double)bref;
+                    if (v <= clip_floor) {
+                        sc0 += (double)v;
+                        sb0 += (double)bref;
+                    } else if (use_list) {
+                        const int k = atomicAdd(&s_ncand, 1);
+                        if (k < kClipCand) {
+                            cand_v[k] = v;
+                            cand_p[k] = (unsigned short)p;
+                        }
+                    }
                 }
             }
         }
-        acc[0] = sc;
-        acc[1] = sb_;
-        acc[2] = (double)n_over;
-        acc[3] = (double)n_fg_masked;
-        acc[4] = (double)n_fg_nb;
-        double a5[5] = {acc[0], acc[1], acc[2], acc[3], acc[4]};
+        double a7[7] = {sc, sb_, (double)n_over, (double)n_fg_masked, (double)n_fg_nb, sc0, sb0};
         atomicOr(&s_rec_lo, rec.lo);
         atomicOr(&s_rec_hi, rec.hi);
-        block_sum<NT, 5>(a5, red, tot);
-        if (threadIdx.x == 0) s_b = (float)tot[0] / fmaxf((float)tot[1], 1e-6f);
+        block_sum<NT, 7>(a7, red, tot);
+        if (threadIdx.x == 0) {
+            s_b = (float)tot[0] / fmaxf((float)tot[1], 1e-6f);
+            s_base[0] = tot[5];
+            s_base[1] = tot[6];
+        }
         __syncthreads();
         n_over = (long long)tot[2];
         n_fg_masked = (long long)tot[3];
         n_fg_nb = (long long)tot[4];
     }
-    // ---- passes B: Poisson-aware clipped background, 4 iterations ----------------------------------------------
+    const bool listed = use_list && s_ncand <= kClipCand && P <= 65536;
+    // ---- passes B: Poisson-aware clipped background, 4 iterations (background-ring pixels only) ---------------
     double nbg_d = 0.0;
     for (int it = 0; it < 4; ++it) {
         const float b = s_b;
         double sc = 0.0, sb_ = 0.0;
+        if (listed) {
+            for (int k = threadIdx.x; k < s_ncand; k += NT) {
+                const float v = cand_v[k];
+                const float bref = brefs[cand_p[k]];
+                const float bp = b * bref;
+                const float thr = (bp + 3.0f * sqrtf(gain * fmaxf(bp, 0.5f))) + 1.0f;
+                if (v <= thr) {
+                    sc += (double)v;
+                    sb_ += (double)bref;
+                }
+            }
+            double a2[2] = {sc, sb_};
+            block_sum<NT, 2>(a2, red, tot);
+            const double tc = s_base[0] + tot[0], tb = s_base[1] + tot[1];
+            if (threadIdx.x == 0) s_b = (float)tc / fmaxf((float)tb, 1e-6f);
+            nbg_d = tb;
+            __syncthreads();
+            continue;
+        }
         for (int p = threadIdx.x; p < P; p += NT) {
-            const float u1 = u1s[p], u2 = u2s[p];
-            const float r2 = u1 * u1 + u2 * u2;
-            if (!(r2 >= kBgR2)) continue;           // background only outside BG_R (r2 >= 12.25 implies not fg2)
-            const int i = p % bx, j = p / bx;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
+            if (!(flags[p] & 2)) continue;          // r2 >= 12.25 also excludes the foreground ellipse
+            const float bref = brefs[p];
             const float bp = b * bref;
             const float thr = (bp + 3.0f * sqrtf(gain * fmaxf(bp, 0.5f))) + 1.0f;
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
+            Mask65 nbm;
+            nbm.lo = nblo[p];
+            nbm.hi = nbhi[p];
             for (int z = 0; z < Dz; ++z) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
+                const float v = voxel(z, p);
                 if (v >= 0.0f && !nbm.get(z) && v <= thr) {
                     sc += (double)v;
                     sb_ += (double)bref;
@@ -308,8 +511,11 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
     }
     const float b = s_b;
     // ---- pass C: summation, centroid, moments, projected spot, per-frame net ---------------------------------
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-    double nfg = 0.0;
+    // Sums over a pixel column's foreground voxels are taken in float32 (<= 65 terms), then weighted by the
+    // pixel's constants (x, y, eps, template) and added in float64.
+    double acc[15];
+#pragma unroll
+    for (int q = 0; q < 15; ++q) acc[q] = 0.0;
     for (int z = threadIdx.x; z < Dz; z += NT)
         for (int w = 0; w < NT / 32; ++w) fzw[w][z] = 0.0f;
     __syncthreads();
@@ -320,69 +526,87 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
         const bool have = p < P;
         const int i = have ? p % bx : 0, j = have ? p / bx : 0;
         float u1 = 0.f, u2 = 0.f, bref = 1.f;
-        if (have) {
-            u1 = u1s[p];
-            u2 = u2s[p];
-            bref = bkg_ref(det, xs[i], ys[j]);
-        }
-        const float r2 = u1 * u1 + u2 * u2;
-        const bool fg2 = have && r2 <= kFgR2;
-        const float bpix = b * bref;
-        const float x = xs[i], y = ys[j];
-        const float eps1 = u1 * seff, eps2 = u2 * seff;
-        const float e12 = eps1 * eps1 + eps2 * eps2;
+        bool fg2 = false;
         Mask65 nbm;
         nbm.clear();
-        if (have) nbm = neighbour_frames(nb, i, j, Dz);
-        double img2 = 0.0;
+        if (have) {
+            u1 = O.u1[po + p];
+            u2 = O.u2[po + p];
+            bref = brefs[p];
+            fg2 = flags[p] & 1;
+            nbm.lo = nblo[p];
+            nbm.hi = nbhi[p];
+        }
+        const float bpix = b * bref;
+        const bool warp_fg = __any_sync(0xffffffffu, fg2);
+        float c_n = 0.f, c_net = 0.f, c_c = 0.f, c_w = 0.f, c_wz = 0.f, c_e3 = 0.f, c_e33 = 0.f, c_img = 0.f;
         bool okall = true;
+        unsigned long long fm = fgz.lo, nm = nbm.lo;
         for (int z = 0; z < Dz; ++z) {
+            if (z == 64) {
+                fm = fgz.hi;
+                nm = nbm.hi;
+            }
+            const bool fgzz = fm & 1ull, nbz = nm & 1ull;
+            fm >>= 1;
+            nm >>= 1;
             float fzc = 0.0f;
             if (have) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
+                const float v = voxel(z, p);
                 const bool valid = v >= 0.0f;
                 const float c = valid ? v : 0.0f;
-                const bool fgzz = fgz.get(z);
-                const bool nbz = nbm.get(z);
                 const bool clean = valid && !nbz;
                 const float net = c - bpix;
-                if (fg2 && fgzz && clean) {            // fgv: foreground, valid, not a neighbour's
-                    nfg += 1.0;
-                    acc[0] += (double)bref;            // sfb
-                    acc[1] += (double)net;             // isum
-                    acc[2] += (double)c;               // vsum counts
-                    acc[3] += (double)bpix;            // vsum0
-                    const float wpos = fmaxf(net, 0.0f);
-                    acc[4] += (double)wpos;            // sw
-                    acc[5] += (double)(wpos * x);
-                    acc[6] += (double)(wpos * y);
-                    acc[7] += (double)(wpos * fzz[z]);
-                    acc[8] += (double)net;             // sws
-                    acc[9] += (double)(net * eps1);
-                    acc[10] += (double)(net * eps2);
-                    acc[11] += (double)(net * e12);
-                    const float e3 = fe3[z];
-                    acc[12] += (double)(net * e3);
-                    acc[13] += (double)(net * (e3 * e3));
+                if (fg2 && clean) {
+                    fzc = net;
+                    if (fgzz) {                         // fgv: foreground, valid, not a neighbour's
+                        c_n += 1.0f;
+                        c_net += net;
+                        c_c += c;
+                        const float wpos = fmaxf(net, 0.0f);
+                        c_w += wpos;
+                        c_wz += wpos * fzz[z];
+                        const float e3 = fe3[z];
+                        c_e3 += net * e3;
+                        c_e33 += net * (e3 * e3);
+                    }
                 }
                 if (fgzz) {
-                    if (clean) img2 += (double)net;
+                    if (clean) c_img += net;
                     else okall = false;
                 }
-                if (fg2 && clean) fzc = net;
             }
-            fzc = warp_sumf(fzc);
-            if (lane == 0) fzw[wid][z] += fzc;
+            if (warp_fg) {
+                fzc = warp_sumf(fzc);
+                if (lane == 0) fzw[wid][z] += fzc;
+            }
         }
         if (have) {
-            O.img2[po + p] = (float)img2;
+            O.img2[po + p] = c_img;
             O.all_valid2[po + p] = okall ? 1 : 0;
+            if (c_n > 0.0f) {
+                const float x = xs[i], y = ys[j];
+                const float eps1 = u1 * seff, eps2 = u2 * seff;
+                const float e12 = eps1 * eps1 + eps2 * eps2;
+                acc[14] += (double)c_n;
+                acc[0] += (double)c_n * (double)bref;             // sfb
+                acc[1] += (double)c_net;                          // isum
+                acc[2] += (double)c_c;                            // vsum counts
+                acc[3] += (double)c_n * (double)bpix;             // vsum0
+                acc[4] += (double)c_w;                            // sw
+                acc[5] += (double)c_w * (double)x;
+                acc[6] += (double)c_w * (double)y;
+                acc[7] += (double)c_wz;
+                acc[8] += (double)c_net;                          // sws
+                acc[9] += (double)c_net * (double)eps1;
+                acc[10] += (double)c_net * (double)eps2;
+                acc[11] += (double)c_net * (double)e12;
+                acc[12] += (double)c_e3;
+                acc[13] += (double)c_e33;
+            }
         }
     }
-    double a15[15];
-    for (int q = 0; q < 14; ++q) a15[q] = acc[q];
-    a15[14] = nfg;
-    block_sum<NT, 15>(a15, red, tot);
+    block_sum<NT, 15>(acc, red, tot);
     for (int z = threadIdx.x; z < Dz; z += NT) {
         float s = 0.0f;
         for (int w = 0; w < NT / 32; ++w) s += fzw[w][z];
@@ -429,14 +653,25 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det, XiRows R, XiBlock 
 // ==================================================================================================================
 // pass 2
 // ==================================================================================================================
-template <int NT>
-__global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock B, const float* __restrict__ arena,
+// Dynamic shared memory: nblo (8P, first the partner's eps1 / eps2) | P2s (4P) | P2ps (4P) | brefs (4P, first the
+// partner's J) | nbhi (4P) | staged net counts of the fitted voxels (4V, when STAGED).
+__host__ __device__ inline size_t pass2_pix_bytes(int P) { return ((size_t)24 * P + 15) / 16 * 16; }
+__host__ __device__ inline size_t pass2_stage_offset(int P, int cap) {
+    return (pass2_pix_bytes(P) + (size_t)8 * cap + 15) / 16 * 16;
+}
+
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
                                               const float* __restrict__ prof, XiPass2In I2, XiPass2Out O,
-                                              const int32_t* __restrict__ order, int max_bx, int max_dz,
+                                              const int32_t* __restrict__ order, int max_bx, int max_dz, int cap,
                                               int* status) {
-    extern __shared__ float dyn[];
+    extern __shared__ __align__(16) unsigned char dyn2[];
+    __shared__ CtaTables T;
+    __shared__ float s_prof[XI_GRID * XI_GRID];
+    __shared__ int s_nlist;
     __shared__ float xs[XI_MAX_BX], ys[XI_MAX_BX];
     __shared__ float fR[XI_MAX_DZ], fRp[XI_MAX_DZ], fzz[XI_MAX_DZ];
+    __shared__ float terms[XI_MAX_DZ * XI_RC_K];
     __shared__ NbShared nb;
     __shared__ float s_e1[3], s_e2[3], s_S[3], s_zetap, s_seffp;
     __shared__ float s_I, s_Ip, s_pmax, s_ppmax;
@@ -453,6 +688,18 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
         return;
     }
     const int P = bx * bx;
+    const int Pm = max_bx * max_bx;
+    unsigned long long* nblo = reinterpret_cast<unsigned long long*>(dyn2);
+    float* e1s = reinterpret_cast<float*>(dyn2);          // partner geometry, before nblo is written
+    float* e2s = e1s + Pm;
+    float* P2s = reinterpret_cast<float*>(dyn2 + (size_t)8 * Pm);
+    float* P2ps = P2s + Pm;
+    float* brefs = P2ps + Pm;
+    float* Jps = brefs;                                   // partner J, before brefs is written
+    unsigned* nbhi = reinterpret_cast<unsigned*>(brefs + Pm);
+    float* ul_v = reinterpret_cast<float*>(dyn2 + pass2_pix_bytes(Pm));      // fit list: net counts
+    unsigned* ul_i = reinterpret_cast<unsigned*>(ul_v + cap);                 // fit list: z << 16 | pixel
+    float* stage = reinterpret_cast<float*>(dyn2 + pass2_stage_offset(Pm, cap));   // 16-byte aligned
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
     const float fb = R.fb[row];
@@ -464,12 +711,19 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
     const float gain = B.gain;
     const float zeta = I2.zeta[row], seff = I2.seff[row];
     const float bg = I2.bg[row], nbgv = I2.nbg[row];
-    const float* prof_r = prof + (size_t)R.region[row] * XI_GRID * XI_GRID;
-    float* P2s = dyn;               // [P]
-    float* P2ps = dyn + P;          // [P] partner
-    float* e1s = dyn + 2 * P;       // [P] partner geometry scratch
-    float* e2s = dyn + 3 * P;       // [P]
-    float* Jps = dyn + 4 * P;       // [P]
+    const float* prof_g = prof + (size_t)R.region[row] * XI_GRID * XI_GRID;
+    for (int q = threadIdx.x; q < XI_GRID * XI_GRID; q += NT) s_prof[q] = prof_g[q];
+    const float* prof_r = s_prof;
+    const XiDetector det = cta_tables(det_g, B, T);
+    __shared__ __align__(8) unsigned long long s_bar;
+    const unsigned vbytes = (unsigned)(((size_t)Dz * P * sizeof(float)) & ~(size_t)15);   // whole 16-byte units
+    const bool tma = STAGED && vbytes > 0 && ((reinterpret_cast<uintptr_t>(sb) & 15) == 0) &&
+                     ((reinterpret_cast<uintptr_t>(stage) & 15) == 0);
+    if (tma && threadIdx.x == 0) {
+        mbar_init(&s_bar, 1);
+        mbar_expect_tx(&s_bar, vbytes);
+        bulk_copy_g2s(stage, sb, vbytes, &s_bar);
+    }
 
     for (int i = threadIdx.x; i < bx; i += NT) {
         xs[i] = box_coord(ix0, i, pxs);
@@ -484,18 +738,16 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
         s_zetap = zp;
     }
     __syncthreads();
-    for (int z = threadIdx.x; z < Dz; z += NT) {
-        float lo, hi;
-        bin_limits(iz0, fb, z, B.frames_phi0, B.osc, &lo, &hi);
-        fR[z] = rocking_fraction(lo, hi, phi, zeta, B.sm, B.rcw);
-        fRp[z] = has_p ? rocking_fraction(lo, hi, R.pphi[row], s_zetap, B.sm, B.rcw) : 0.0f;
-    }
+    rocking_curve_cta(Dz, iz0, fb, B, T.rcw, phi, zeta, terms, fR);
     if (has_p) {
+        rocking_curve_cta(Dz, iz0, fb, B, T.rcw, R.pphi[row], s_zetap, terms, fRp);
         float e1[3] = {s_e1[0], s_e1[1], s_e1[2]}, e2[3] = {s_e2[0], s_e2[1], s_e2[2]};
         float S[3] = {s_S[0], s_S[1], s_S[2]};
         box_geometry(det, S, e1, e2, bx, xs, ys, B.sd, e1s, e2s, nullptr, Jps, &s_seffp);
+    } else {
+        for (int z = threadIdx.x; z < Dz; z += NT) fRp[z] = 0.0f;
+        __syncthreads();
     }
-    __syncthreads();
     // per-pixel profile planes; the profile maxima follow from them (f32 products are monotone in R)
     float Rmax = fR[0], Rpmax = fRp[0];
     for (int z = 1; z < Dz; ++z) {
@@ -539,33 +791,86 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
         }
         __syncthreads();
     }
-    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, has_p, nb);
+    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, has_p, nb);     // ends with a barrier (partner scratch free)
+    pixel_tables(det, nb, bx, Dz, xs, ys, nblo, nbhi, brefs);
     const float pthr = 0.01f * s_pmax;
     const float ppthr = 0.01f * fmaxf(s_ppmax, 1e-12f);
 
-    // ---- pass U: use mask, initial intensity ---------------------------------------------------------------
-    // per-thread pixels (at most ceil(97^2 / NT)); use masks are recomputed per pass (cheap) to spare registers
-    double acc[16];
+    // ---- pass U: the profile sums, the fit mask, the fit sums that do not depend on I. The fitted voxels (net count
+    // and packed frame / pixel index) are compacted into a shared-memory list that every later pass iterates
+    // densely; when the list overflows, the later passes fall back to scanning the box (staged copy or global).
+    Mask65 fgz;
+    fgz.lo = s_fgz_lo;
+    fgz.hi = s_fgz_hi;
+    if (STAGED) stage_wait(tma, &s_bar, stage, sb, Dz * P, status);
+    if (threadIdx.x == 0) s_nlist = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
     {
-        double s_net = 0.0, s_w = 0.0;
-        for (int p = threadIdx.x; p < P; p += NT) {
-            const int i = p % bx, j = p / bx;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
+        double a8[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // s_net, s_w, p_total, p_valid, p_fgn, a110, C0, nuse
+        const int n_iter = (P + NT - 1) / NT;
+        for (int q = 0; q < n_iter; ++q) {
+            const int p = threadIdx.x + q * NT;
+            const bool have = p < P;
+            float bref = 1.0f, P2 = 0.0f, P2p = 0.0f;
+            bool fg2 = false;
+            Mask65 nbm;
+            nbm.clear();
+            if (have) {
+                bref = brefs[p];
+                P2 = P2s[p];
+                P2p = P2ps[p];
+                const float u1 = I2.u1[po + p], u2 = I2.u2[po + p];
+                fg2 = (u1 * u1 + u2 * u2) <= kFgR2;
+                nbm.lo = nblo[p];
+                nbm.hi = nbhi[p];
+            }
             const float bpix = bg * bref;
-            const float P2 = P2s[p], P2p = P2ps[p];
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
+            const float iv0 = __frcp_rn(gain * fmaxf(bpix, kVarFloor));
+            Mask65 um;                           // frames of this pixel that enter the fit
+            um.clear();
             for (int z = 0; z < Dz; ++z) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
-                if (!(v >= 0.0f) || nbm.get(z)) continue;
-                const float pv = P2 * fR[z];
-                const float ppv = (P2p * fRp[z]) * hp;
-                if (!(pv > pthr || ppv > ppthr)) continue;
-                s_net += (double)(v - bpix);
-                s_w += (double)(pv + ppv);
+                bool use = false;
+                float net = 0.0f;
+                if (have) {
+                    const float v = (STAGED ? stage[(size_t)z * P + p] : sb[(size_t)z * P + p]) - R.sb_bias;
+                    const float pv = P2 * fR[z];
+                    const float ppv = (P2p * fRp[z]) * hp;
+                    const bool valid = v >= 0.0f, nbz = nbm.get(z);
+                    a8[2] += (double)pv;
+                    if (valid && !nbz) a8[3] += (double)pv;
+                    if (fg2 && fgz.get(z)) a8[4] += (double)pv;
+                    use = valid && !nbz && (pv > pthr || ppv > ppthr);
+                    net = v - bpix;
+                    if (STAGED) stage[(size_t)z * P + p] = use ? net : __int_as_float(0x7fc00000);
+                    if (use) {
+                        um.set(z);
+                        a8[0] += (double)net;
+                        a8[1] += (double)(pv + ppv);
+                        a8[5] += (double)((pv * pv) * iv0);
+                        a8[6] += (double)((pv * bref) * iv0);
+                        a8[7] += 1.0;
+                    }
+                }
+                // warp-aggregated append to the fit list
+                const unsigned ball = __ballot_sync(0xffffffffu, use);
+                if (ball) {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(&s_nlist, __popc(ball));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    const int k = base + __popc(ball & ((1u << lane) - 1u));
+                    if (use && k < cap) {
+                        ul_v[k] = net;
+                        ul_i[k] = ((unsigned)z << 16) | (unsigned)p;
+                    }
+                }
+            }
+            if (have && STAGED) {                // the neighbour mask is not needed any more: keep the fit mask
+                nblo[p] = um.lo;
+                nbhi[p] = um.hi;
             }
         }
-        double a2[2] = {s_net, s_w};
-        block_sum<NT, 2>(a2, red, tot);
+        block_sum<NT, 8>(a8, red, tot);
         if (threadIdx.x == 0) {
             const float I0 = (float)tot[0] / fmaxf((float)tot[1], 1e-6f);
             s_I = I0;
@@ -573,43 +878,72 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
         }
         __syncthreads();
     }
-    // ---- IRLS: Poisson-weighted 2x2 normal equations, float64 sums, N_IRLS iterations ----------------------
-    double a11 = 0.0, a12 = 0.0, a22 = 1.0, b1 = 0.0, b2 = 0.0, det2 = 1.0;
-    float Iw = 0.0f, Ipw = 0.0f;        // intensities of the last iteration's weights (the variance tail uses them)
-    for (int it = 0; it < kIrls; ++it) {
-        const float I = s_I, Ip = s_Ip;
-        Iw = I;
-        Ipw = Ip;
-        const float Ipos = fmaxf(I, 0.0f), Ippos = fmaxf(Ip, 0.0f);
-        double s11 = 0.0, s1 = 0.0, s12 = 0.0, s22 = 0.0, s2 = 0.0;
+    const double s_net_use = tot[0];
+    const float p_total = (float)tot[2], p_valid = (float)tot[3], p_fgn = (float)tot[4];
+    const double a110 = fmax(tot[5], 1e-12), C0 = tot[6];
+    const float nuse = (float)tot[7];
+    const int nlist = s_nlist;
+    const bool listed = nlist <= cap;
+
+    // every fitted voxel of this thread: f(net, pv, ppv, bpix, bref)
+    auto each_fitted = [&](auto&& f) {
+        if (listed) {
+            for (int k = threadIdx.x; k < nlist; k += NT) {
+                const unsigned id = ul_i[k];
+                const int z = (int)(id >> 16), p = (int)(id & 0xffffu);
+                const float bref = brefs[p];
+                f(ul_v[k], P2s[p] * fR[z], (P2ps[p] * fRp[z]) * hp, bg * bref, bref);
+            }
+            return;
+        }
         for (int p = threadIdx.x; p < P; p += NT) {
-            const int i = p % bx, j = p / bx;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
+            const float bref = brefs[p];
             const float bpix = bg * bref;
             const float P2 = P2s[p], P2p = P2ps[p];
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
+            Mask65 nbm;
+            nbm.lo = nblo[p];
+            nbm.hi = nbhi[p];
             for (int z = 0; z < Dz; ++z) {
+                if (STAGED) {
+                    if (!nbm.get(z)) continue;   // fit mask
+                    f(stage[(size_t)z * P + p], P2 * fR[z], (P2p * fRp[z]) * hp, bpix, bref);
+                    continue;
+                }
                 const float v = sb[(size_t)z * P + p] - R.sb_bias;
                 if (!(v >= 0.0f) || nbm.get(z)) continue;
                 const float pv = P2 * fR[z];
                 const float ppv = (P2p * fRp[z]) * hp;
                 if (!(pv > pthr || ppv > ppthr)) continue;
-                const float net = v - bpix;
-                float mu = bpix + Ipos * pv;
-                if (has_p) mu = mu + Ippos * ppv;
-                const float iv = 1.0f / (gain * fmaxf(mu, kVarFloor));
-                const float wpp = pv * pv, wpn = pv * net;
-                s11 += (double)(wpp * iv);
-                s1 += (double)(wpn * iv);
-                if (has_p) {
-                    s12 += (double)((pv * ppv) * iv);
-                    s22 += (double)((ppv * ppv) * iv);
-                    s2 += (double)((ppv * net) * iv);
-                }
+                f(v - bpix, pv, ppv, bpix, bref);
             }
         }
-        double a5[5] = {s11, s1, s12, s22, s2};
-        block_sum<NT, 5>(a5, red, tot);
+    };
+
+    // ---- IRLS: Poisson-weighted 2x2 normal equations, float64 sums, N_IRLS iterations; the last iteration's
+    // weights also give C of the variance tail and the sum of the fitted profile values
+    double a11 = 0.0, a12 = 0.0, a22 = 1.0, b1 = 0.0, b2 = 0.0, det2 = 1.0, Cc = 0.0, swp = 0.0;
+    for (int it = 0; it < kIrls; ++it) {
+        const bool last = it == kIrls - 1;
+        const float I = s_I, Ip = s_Ip;
+        const float Ipos = fmaxf(I, 0.0f), Ippos = fmaxf(Ip, 0.0f);
+        double a7[7] = {0, 0, 0, 0, 0, 0, 0};   // a11, b1, a12, a22, b2, C, sum p
+        each_fitted([&](float net, float pv, float ppv, float bpix, float bref) {
+            float mu = bpix + Ipos * pv;
+            if (has_p) mu = mu + Ippos * ppv;
+            const float iv = __frcp_rn(gain * fmaxf(mu, kVarFloor));
+            a7[0] += (double)((pv * pv) * iv);
+            a7[1] += (double)((pv * net) * iv);
+            if (has_p) {
+                a7[2] += (double)((pv * ppv) * iv);
+                a7[3] += (double)((ppv * ppv) * iv);
+                a7[4] += (double)((ppv * net) * iv);
+            }
+            if (last) {
+                a7[5] += (double)((pv * bref) * iv);
+                a7[6] += (double)pv;
+            }
+        });
+        block_sum<NT, 7>(a7, red, tot);
         a11 = tot[0];
         b1 = tot[1];
         if (has_p) {
@@ -621,6 +955,10 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
             a22 = 1.0;
             b2 = 0.0;
         }
+        if (last) {
+            Cc = tot[5];
+            swp = tot[6];
+        }
         det2 = fmax(a11 * a22 - a12 * a12, 1e-30);
         if (threadIdx.x == 0) {
             s_I = (float)((a22 * b1 - a12 * b2) / det2);
@@ -630,78 +968,28 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det, XiRows R, XiBlock 
     }
     const float I = s_I, Ip = s_Ip;
     const float Ippos = fmaxf(Ip, 0.0f);
-    const float Iwpos = fmaxf(Iw, 0.0f), Ipwpos = fmaxf(Ipw, 0.0f);
-    // ---- tail pass 1: C, a110, C0 (last iteration's weights), use counts, sums for pm / nm, p_valid, p_total, p_fg
-    {
-        Mask65 fgz;
-        fgz.lo = s_fgz_lo;
-        fgz.hi = s_fgz_hi;
-        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-        for (int p = threadIdx.x; p < P; p += NT) {
-            const int i = p % bx, j = p / bx;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
-            const float bpix = bg * bref;
-            const float iv0 = 1.0f / (gain * fmaxf(bpix, kVarFloor));
-            const float P2 = P2s[p], P2p = P2ps[p];
-            const float u1 = I2.u1[po + p], u2 = I2.u2[po + p];
-            const bool fg2 = (u1 * u1 + u2 * u2) <= kFgR2;
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
-            for (int z = 0; z < Dz; ++z) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
-                const float pv = P2 * fR[z];
-                const float ppv = (P2p * fRp[z]) * hp;
-                const bool valid = v >= 0.0f, nbz = nbm.get(z);
-                acc[5] += (double)pv;                                       // p_total
-                if (valid && !nbz) acc[6] += (double)pv;                    // p_valid
-                if (fg2 && fgz.get(z)) acc[7] += (double)pv;                // p_fg numerator
-                if (!valid || nbz || !(pv > pthr || ppv > ppthr)) continue;
-                const float net = v - bpix;
-                float mu = bpix + Iwpos * pv;
-                if (has_p) mu = mu + Ipwpos * ppv;
-                const float iv = 1.0f / (gain * fmaxf(mu, kVarFloor));
-                const float wb = pv * bref;
-                acc[0] += (double)(wb * iv);                                // C
-                acc[1] += (double)((pv * pv) * iv0);                        // a110
-                acc[2] += (double)(wb * iv0);                               // C0
-                acc[3] += 1.0;                                              // n use
-                acc[4] += (double)pv;                                       // sum wp
-                const float resid = has_p ? net - Ippos * ppv : net;
-                acc[8] += (double)resid;
-            }
-        }
-        double a9[9];
-        for (int q = 0; q < 9; ++q) a9[q] = acc[q];
-        block_sum<NT, 9>(a9, red, tot);
+    const float pm = (float)swp / fmaxf(nuse, 1.0f);
+    // mean residual over the fitted voxels (with a partner the residual removes the partner's fitted share)
+    double s_resid = s_net_use;
+    if (has_p) {
+        double a1[1] = {0.0};
+        each_fitted([&](float net, float pv, float ppv, float bpix, float bref) {
+            a1[0] += (double)(net - Ippos * ppv);
+        });
+        block_sum<NT, 1>(a1, red, tot);
+        s_resid = tot[0];
     }
-    const double Cc = tot[0], a110 = fmax(tot[1], 1e-12), C0 = tot[2];
-    const float nuse = (float)tot[3];
-    const float pm = (float)tot[4] / fmaxf(nuse, 1.0f);
-    const float nm = (float)tot[8] / fmaxf(nuse, 1.0f);
-    const float p_total = (float)tot[5], p_valid = (float)tot[6], p_fgn = (float)tot[7];
-    // ---- tail pass 2: profile / residual correlation -----------------------------------------------------------
+    const float nm = (float)s_resid / fmaxf(nuse, 1.0f);
+    // ---- profile / residual correlation ------------------------------------------------------------------------
     {
-        double sdd = 0.0, spp = 0.0, snn = 0.0;
-        for (int p = threadIdx.x; p < P; p += NT) {
-            const int i = p % bx, j = p / bx;
-            const float bref = bkg_ref(det, xs[i], ys[j]);
-            const float bpix = bg * bref;
-            const float P2 = P2s[p], P2p = P2ps[p];
-            const Mask65 nbm = neighbour_frames(nb, i, j, Dz);
-            for (int z = 0; z < Dz; ++z) {
-                const float v = sb[(size_t)z * P + p] - R.sb_bias;
-                if (!(v >= 0.0f) || nbm.get(z)) continue;
-                const float pv = P2 * fR[z];
-                const float ppv = (P2p * fRp[z]) * hp;
-                if (!(pv > pthr || ppv > ppthr)) continue;
-                const float net = v - bpix;
-                const float resid = has_p ? net - Ippos * ppv : net;
-                const float dp = pv - pm, dn = resid - nm;
-                sdd += (double)(dp * dn);
-                spp += (double)(dp * dp);
-                snn += (double)(dn * dn);
-            }
-        }
-        double a3[3] = {sdd, spp, snn};
+        double a3[3] = {0.0, 0.0, 0.0};
+        each_fitted([&](float net, float pv, float ppv, float bpix, float bref) {
+            const float resid = has_p ? net - Ippos * ppv : net;
+            const float dp = pv - pm, dn = resid - nm;
+            a3[0] += (double)(dp * dn);
+            a3[1] += (double)(dp * dp);
+            a3[2] += (double)(dn * dn);
+        });
         block_sum<NT, 3>(a3, red, tot);
     }
     if (threadIdx.x == 0) {
@@ -914,9 +1202,6 @@ int* status_ptr() {
     return p;
 }
 
-size_t pass1_smem(int max_bx) { return (size_t)2 * max_bx * max_bx * sizeof(float); }
-size_t pass2_smem(int max_bx) { return (size_t)5 * max_bx * max_bx * sizeof(float); }
-
 int rows_check(const XiRows* R) {
     if (!R) return fail(XI_E_ARG, "rows: null");
     if (R->n < 0 || (R->order && R->n_order < 0)) return fail(XI_E_ARG, "rows: negative count");
@@ -926,24 +1211,30 @@ int rows_check(const XiRows* R) {
     return XI_OK;
 }
 
-template <int NT>
-int launch_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena,
-                        XiPass1Out* O, cudaStream_t s, int nblk) {
-    size_t sm = pass1_smem(R->max_bx);
-    cudaFuncSetAttribute(k_pass1<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_pass1<NT><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, *O, R->order, R->max_bx, R->max_dz, status_ptr());
+template <int NT, bool STAGED>
+int launch_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, XiPass1Out* O,
+                 cudaStream_t s, int nblk) {
+    const size_t P = (size_t)R->max_bx * R->max_bx;
+    size_t sm = pass1_pix_bytes((int)P) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0);
+    cudaFuncSetAttribute(k_pass1<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_pass1<NT, STAGED><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, *O, R->order, R->max_bx, R->max_dz,
+                                              status_ptr());
     return cuda_check("xi_pass1");
 }
 
-template <int NT>
-int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena,
-                        const float* prof, const XiPass2In* in, XiPass2Out* O, cudaStream_t s, int nblk) {
-    size_t sm = pass2_smem(R->max_bx);
-    cudaFuncSetAttribute(k_pass2<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_pass2<NT><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, prof, *in, *O, R->order, R->max_bx, R->max_dz,
-                                     status_ptr());
+template <int NT, bool STAGED>
+int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, const float* prof,
+                 const XiPass2In* in, XiPass2Out* O, cudaStream_t s, int nblk, int cap) {
+    const size_t P = (size_t)R->max_bx * R->max_bx;
+    size_t sm = pass2_stage_offset((int)P, cap) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0);
+    cudaFuncSetAttribute(k_pass2<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_pass2<NT, STAGED><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, prof, *in, *O, R->order, R->max_bx, R->max_dz,
+                                              cap, status_ptr());
     return cuda_check("xi_pass2");
 }
+
+// Dynamic shared memory available for a staged shoebox beside the kernels' static arrays (bytes).
+constexpr size_t kStageBudget = 190 * 1024;
 
 }  // namespace
 
@@ -982,10 +1273,16 @@ int xi_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     const int nblk = R->order ? R->n_order : R->n;
     if (nblk == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    const int P = R->max_bx * R->max_bx;
-    if (P <= 96) return launch_pass1<64>(det, R, B, arena, O, s, nblk);
-    if (P <= 200) return launch_pass1<128>(det, R, B, arena, O, s, nblk);
-    return launch_pass1<256>(det, R, B, arena, O, s, nblk);
+    const size_t P = (size_t)R->max_bx * R->max_bx;
+    const bool staged = pass1_pix_bytes((int)P) + P * R->max_dz * sizeof(float) + 16 <= kStageBudget;
+    if (staged) {
+        if (P <= 96) return launch_pass1<64, true>(det, R, B, arena, O, s, nblk);
+        if (P <= 200) return launch_pass1<128, true>(det, R, B, arena, O, s, nblk);
+        return launch_pass1<256, true>(det, R, B, arena, O, s, nblk);
+    }
+    if (P <= 96) return launch_pass1<64, false>(det, R, B, arena, O, s, nblk);
+    if (P <= 200) return launch_pass1<128, false>(det, R, B, arena, O, s, nblk);
+    return launch_pass1<256, false>(det, R, B, arena, O, s, nblk);
 }
 
 
@@ -997,10 +1294,24 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     const int nblk = R->order ? R->n_order : R->n;
     if (nblk == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    const int P = R->max_bx * R->max_bx;
-    if (P <= 96) return launch_pass2<64>(det, R, B, arena, prof, in, O, s, nblk);
-    if (P <= 200) return launch_pass2<128>(det, R, B, arena, prof, in, O, s, nblk);
-    return launch_pass2<256>(det, R, B, arena, prof, in, O, s, nblk);
+    const size_t P = (size_t)R->max_bx * R->max_bx;
+    const size_t V = P * R->max_dz;
+    if (pass2_pix_bytes((int)P) > kStageBudget)
+        return fail(XI_E_LIMIT, "xi_pass2: box side above 89 pixels (per-pixel tables exceed shared memory)");
+    // the fit list holds up to every voxel of small boxes and 4096 fitted voxels of large ones; the box itself is
+    // staged only when small (it is read once: staging buys the copy's overlap with the set-up, not re-reads)
+    const int cap = (int)(V < 4096 ? V : 4096);
+    const size_t base = pass2_stage_offset((int)P, cap);
+    if (base > kStageBudget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
+    const bool staged = V * sizeof(float) <= 48 * 1024 && base + V * sizeof(float) + 16 <= kStageBudget;
+    if (staged) {
+        if (P <= 96) return launch_pass2<64, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
+        if (P <= 200) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
+        return launch_pass2<256, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
+    }
+    if (P <= 96) return launch_pass2<64, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
+    if (P <= 200) return launch_pass2<128, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
+    return launch_pass2<256, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
 }
 
 int xi_gather(const XiFrames* F, const XiGatherRows* G, float* arena, int32_t* cnt, void* stream) {

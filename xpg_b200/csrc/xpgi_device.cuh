@@ -240,6 +240,48 @@ __device__ __forceinline__ float profile_value(const float* prof_r, float u1, fl
 }
 
 // ------------------------------------------------------------------------------------------------------------------
+// bulk asynchronous copy of a contiguous global range into shared memory (TMA, no multicast), completion counted on
+// an mbarrier. Addresses 16-byte aligned, size a multiple of 16 bytes.
+// ------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier; gives up after `max_tries` polls (returns false).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long max_tries) {
+    for (long long t = 0; t < max_tries; ++t) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000000;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------------------------------------------------------
 // reductions
 // ------------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

@@ -128,11 +128,12 @@ class RowSet:
         self.bx = np.asarray(bx, np.int64)
         V = self.Dz * self.bx * self.bx
         self.vox = V
-        self.sb_off = np.concatenate([[0], np.cumsum(V)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        Vp = (V + 3) // 4 * 4 if sb_bias == 3.0 else V     # arena rows start on 16 bytes (bulk copies)
+        self.sb_off = np.concatenate([[0], np.cumsum(Vp)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
         P = self.bx * self.bx
         self.pix_off = np.concatenate([[0], np.cumsum(P)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
         self.frm_off = np.concatenate([[0], np.cumsum(self.Dz)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
-        self.n_vox = int(V.sum())
+        self.n_vox = int(Vp.sum()) + 4
         self.n_pix = int(P.sum())
         self.n_frm = int(self.Dz.sum())
         K = int(np.asarray(nb["x"]).shape[1]) if n else 0
@@ -164,12 +165,13 @@ class RowSet:
         self.device = device
 
     def groups(self):
-        """Launch groups: rows of one box side, each with its own row order (deepest first)."""
+        """Launch groups: rows of one shoebox shape (side, depth), so that each launch sizes its shared memory
+        (and decides whether the shoebox is staged there) for exactly its rows. Largest shapes first."""
         out = []
-        for b in np.unique(self.bx):
-            rows = np.flatnonzero(self.bx == b)
-            rows = rows[np.argsort(-self.Dz[rows], kind="stable")]
-            out.append((int(b), int(self.Dz[rows].max()), rows.astype(np.int32)))
+        shapes = sorted({(int(b), int(d)) for b, d in zip(self.bx, self.Dz)}, key=lambda s: -s[0] * s[0] * s[1])
+        for b, d in shapes:
+            rows = np.flatnonzero((self.bx == b) & (self.Dz == d))
+            out.append((b, d, rows.astype(np.int32)))
         return out
 
     def view(self, order=None, max_bx=None, max_dz=None):

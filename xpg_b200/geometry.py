@@ -10,11 +10,38 @@ handed to `xpg_b200.integrate` unchanged: the integration path reads only the at
 """
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field, replace
 
 import numpy as np
 
 PIX0 = 1.0      # continuous coordinate of the centre of array element 0
+
+_POOL = None
+
+
+def _pool():
+    global _POOL
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(max(1, min(16, len(os.sched_getaffinity(0)))))
+    return _POOL
+
+
+def row_chunks(n, min_rows=65536):
+    """Contiguous row ranges for the host thread pool (numpy releases the GIL in its array loops)."""
+    k = max(1, min(_pool()._max_workers, n // min_rows))
+    e = np.linspace(0, n, k + 1).astype(int)
+    return [(int(a), int(b)) for a, b in zip(e[:-1], e[1:])]
+
+
+def par_rows(fn, n, min_rows=65536):
+    """fn(a, b) over row ranges of [0, n) on the host thread pool, results in order. Element-wise work split this
+    way is bit-identical to one call over all rows."""
+    ch = row_chunks(n, min_rows)
+    if len(ch) == 1:
+        return [fn(0, n)]
+    return list(_pool().map(lambda ab: fn(*ab), ch))
 
 
 def unit(v):
@@ -300,10 +327,13 @@ def generate_hkl(Astar, dmin, dmax=1e9):
     real = np.linalg.inv(Astar)
     hmax = [int(np.ceil(np.linalg.norm(real[i]) / dmin)) for i in range(3)]
     axes = [np.arange(-m, m + 1) for m in hmax]
-    H = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
-    p = H @ Astar.T
-    q2 = np.einsum("ij,ij->i", p, p)
-    return H[(q2 <= 1.0 / dmin ** 2) & (q2 > 1.0 / dmax ** 2)].astype(np.int32)
+
+    def part(a, b):             # h values axes[0][a:b] (the grid is h-major: chunks keep the order)
+        H = np.stack(np.meshgrid(axes[0][a:b], axes[1], axes[2], indexing="ij"), -1).reshape(-1, 3)
+        p = H @ Astar.T
+        q2 = np.einsum("ij,ij->i", p, p)
+        return H[(q2 <= 1.0 / dmin ** 2) & (q2 > 1.0 / dmax ** 2)].astype(np.int32)
+    return np.concatenate(par_rows(part, len(axes[0]), min_rows=8))
 
 
 def diffraction_angles(geom, p0):
@@ -333,7 +363,8 @@ def predict_reflections(geom, Astar, dmin, dmax=1e9, z_range=None, hkl=None):
     if hkl is None:
         hkl = generate_hkl(Astar, dmin, dmax)
     p0 = hkl @ Astar.T
-    pa, pb, ok = diffraction_angles(geom, p0)
+    ang = par_rows(lambda a, b: diffraction_angles(geom, p0[a:b]), len(p0))
+    pa, pb, ok = (np.concatenate([x[i] for x in ang]) for i in range(3))
     if z_range is None:
         z_range = (geom.starting_frame - 1, geom.starting_frame - 1 + 360.0 / abs(geom.osc))
     lo, hi = sorted(geom.z_to_phi(np.array(z_range, float)))
@@ -346,17 +377,22 @@ def predict_reflections(geom, Astar, dmin, dmax=1e9, z_range=None, hkl=None):
             sel = (phs >= lo) & (phs < hi)
             if not sel.any():
                 continue
-            R = axis_angle_matrices(geom.axis, np.radians(phs[sel]))
-            S_all.append(np.einsum("nij,nj->ni", R, p0[ok][sel]) + geom.s0)
+            ph_sel, p_sel = phs[sel], p0[ok][sel]
+            S_all.append(np.concatenate(par_rows(
+                lambda a, b: np.einsum("nij,nj->ni", axis_angle_matrices(geom.axis, np.radians(ph_sel[a:b])),
+                                       p_sel[a:b]) + geom.s0, len(ph_sel))))
             H_all.append(hkl[ok][sel])
             ph_all.append(phs[sel])
     if not H_all:
         e = np.zeros(0)
         return dict(hkl=np.zeros((0, 3), np.int32), phi=e, S=np.zeros((0, 3)), x=e, y=e, z=e, zeta=e, polarization=e)
     res = dict(hkl=np.concatenate(H_all), phi=np.concatenate(ph_all), S=np.concatenate(S_all))
-    res["x"], res["y"] = geom.s_to_pixel(res["S"])
+    S = res["S"]
+    xy = par_rows(lambda a, b: geom.s_to_pixel(S[a:b]), len(S))
+    res["x"], res["y"] = np.concatenate([v[0] for v in xy]), np.concatenate([v[1] for v in xy])
     res["z"] = geom.phi_to_z(res["phi"])
-    res["zeta"], res["polarization"] = geom.lp_factor(res["S"])
+    lp = par_rows(lambda a, b: geom.lp_factor(S[a:b]), len(S))
+    res["zeta"], res["polarization"] = np.concatenate([v[0] for v in lp]), np.concatenate([v[1] for v in lp])
     keep = np.isfinite(res["x"])
     return {k: v[keep] for k, v in res.items()}
 

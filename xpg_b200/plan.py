@@ -74,17 +74,17 @@ def predict_blocks(exps_by_block, block_edges, dmin, dmax, z_lo, z_hi, minimum_z
     return {k: v[ok] for k, v in res.items()}
 
 
-def _depth_bucket(d):
-    for b in DZ_BUCKETS:
-        if d <= b:
-            return b
-    return -1
+def _depth_buckets(dz):
+    """Smallest DZ_BUCKETS entry >= dz, -1 beyond the deepest (`xpg/integrate.py:157-161`)."""
+    b = np.asarray(DZ_BUCKETS)
+    k = np.searchsorted(b, dz, side="left")
+    return np.where(k < len(b), b[np.minimum(k, len(b) - 1)], -1).astype(int)
 
 
 def neighbour_lists(x, y, z, sx, sz, k=K_NEIGHBOURS):
     """k nearest reflections within 4 N_FG in (x / sx, y / sx, z / sz) (`xpg/integrate.py:164-172`)."""
     pts = np.c_[x / sx, y / sx, z / sz]
-    d, j = cKDTree(pts).query(pts, k=k + 1, distance_upper_bound=4.0 * N_FG)
+    d, j = cKDTree(pts).query(pts, k=k + 1, distance_upper_bound=4.0 * N_FG, workers=-1)
     j, d = j[:, 1:], d[:, 1:]
     has = np.isfinite(d)
     return np.where(has, j, 0), has, np.where(has, d, np.inf)
@@ -145,7 +145,7 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
     iz_c = np.floor(refl["z"] - (fb - 1) / 2.0).astype(int)
     iz0 = iz_c - hz * fb
     dz = 2 * hz + 1
-    Dz = np.array([_depth_bucket(d) for d in dz], int)
+    Dz = _depth_buckets(dz)
     zc = refl["z"]
     cov = 0.5 * (erf((iz0 + dz * fb - zc) / (np.sqrt(2) * sz_frames)) - erf((iz0 - zc) / (np.sqrt(2) * sz_frames)))
     refl["coverage"] = np.where(trunc, np.clip(cov, 0, 1), 1.0).astype(np.float32)
