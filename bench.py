@@ -95,20 +95,39 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def reduce_over_ranks(t, n, dist=None, device="cuda"):
+    """Whole-job timing of replicas: the slowest rank's time and the total units over all ranks."""
+    if dist is None:
+        return t, n
+    import torch
+    tt = torch.tensor([t], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    nn = torch.tensor([float(n)], device=device, dtype=torch.float64)
+    dist.all_reduce(nn)
+    return float(tt.item()), int(nn.item())
+
+
+def replica_seed(workload, rank):
+    """Seed of the sweep a rank integrates: replicas integrate independent sweeps (different crystal orientation
+    and noise), so no data is exchanged between ranks."""
+    return (2 if workload.startswith("config2") else 1) + rank
+
+
 class Block:
     """One phi block of a synthetic sweep, planned and rendered on the device."""
 
     def __init__(self, name, seed_offset=0, device="cuda"):
         from xpg_b200 import synth
         from xpg_b200.plan import IntegrationModel, plan_integration
+        seed = replica_seed(name, seed_offset)
         if name == "config2-block":
-            self.spec = synth.config2(seed=2 + seed_offset)
+            self.spec = synth.config2(seed=seed)
             self.edges = np.array([0.0, 360.0])
         elif name == "config2-small":          # a 20-frame block of the same sweep (profiling captures)
-            self.spec = synth.config2(seed=2 + seed_offset)
+            self.spec = synth.config2(seed=seed)
             self.edges = np.array([0.0, 20.0])
         elif name == "config1":
-            self.spec = synth.config1(seed=1 + seed_offset)
+            self.spec = synth.config1(seed=seed)
             self.edges = np.array([0.0, 100.0])
         else:
             raise ValueError(name)
@@ -251,15 +270,7 @@ def run(args):
     t = e0.elapsed_time(e1) * 1e-3
     ksum = D.TIMER.summary()
     launches = D.TIMER.launches
-    t_max = t
-    n_total = blk.n_refl * args.steps
-    if dist is not None:
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        nn = torch.tensor([n_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(nn)
-        n_total = int(nn.item())
+    t_max, n_total = reduce_over_ranks(t, blk.n_refl * args.steps, dist)
     value = n_total / t_max
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
@@ -292,11 +303,7 @@ def run(args):
             res = blk.integrate(hsrc)
         f1.record()
         torch.cuda.synchronize()
-        te = f0.elapsed_time(f1) * 1e-3
-        if dist is not None:
-            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te, _ = reduce_over_ranks(f0.elapsed_time(f1) * 1e-3, 0, dist)
         n_out = sum(v.nbytes for v in res.refl.values() if isinstance(v, np.ndarray))
         e2e = {"value": round(blk.n_refl * world * k2 / te, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(host.numel() * 4), "d2h_bytes_per_step": int(n_out), "steps": k2}

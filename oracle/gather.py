@@ -78,6 +78,13 @@ def gather_shoebox(prepared, frame_ids, iz0, fb, Dz, bx, iy0, ix0):
             v[neg] = np.where(v[neg] == -2.0, F32(np.nan), F32(np.inf))
             acc[k] = (acc[k] + v).astype(F32)
             cnt[k] += 1
-    arr = np.nan_to_num(acc, nan=-2.0, posinf=-1.0, neginf=-1.0).astype(F32) + SB_OFF
-    arr[cnt < fb] = F32(0.0)
-    return (arr - SB_OFF).astype(F32)
+    return (decode_bins(acc, cnt, fb) - SB_OFF).astype(F32)
+
+
+def decode_bins(acc, cnt, fb):
+    """Stored (value + 3) form of binned sums (`xpg/shoebox.py:264-268` and `xpg/integrate.py:483-488`): an
+    overloaded frame (NaN) makes the bin -2, a masked one (+inf) -1 (overload wins), bins holding fewer than fb
+    frames are unrecorded (0). acc: (Dz, ...) IEEE-encoded sums; cnt: (Dz,) frames per bin."""
+    arr = np.nan_to_num(np.asarray(acc, F32), nan=-2.0, posinf=-1.0, neginf=-1.0).astype(F32) + SB_OFF
+    arr[np.asarray(cnt) < fb] = F32(0.0)
+    return arr

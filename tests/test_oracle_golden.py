@@ -1,0 +1,115 @@
+"""The oracle pinned to the reference (CPU): on every golden fixture, the oracle's pass 1 / pass 2 reproduce the
+reference's outputs (integers exactly, floats within tolerance.py), its gather reproduces the reference's stored
+shoeboxes bit for bit from the re-rendered frames, its accumulation reproduces the reference's profile grids, and
+the binned-bin decoding satisfies the reference's known-answer test."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import golden_io as G
+import tolerance as T
+from oracle import gather as OG
+from oracle import kernels as OK
+
+
+@pytest.mark.parametrize("case", G.CASES)
+def test_oracle_kernels_match_reference(case):
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    g = spec.geometry()
+    det = OK.detector_consts(g, tmpl)
+    z = G.load(case)
+    for k in ("P0", "Bx", "By", "U1", "U2", "UN"):
+        assert np.array_equal(det[k], z["det_" + k]), k
+    for i in G.chunks(case):
+        d, rc, nb, o1, o2 = G.chunk(case, i)
+        for j in range(d["sb"].shape[0]):
+            r = G.row_dict(rc, j)
+            nbr = G.nb_row(nb, j)
+            o = OK.pass1(d["sb"][j], r, nbr, det, d["s0"], d["axis"], d["frames_phi0"], d["osc"], d["sd"], d["sm"],
+                         d["gain"], d["rcw"])
+            ctx = {k: o1[k][j] for k in o1}
+            for k in ("n_over", "n_fg_masked", "n_fg_nb", "nfg"):
+                assert int(o[k]) == int(o1[k][j]), (case, i, j, k)
+            assert np.array_equal(o["all_valid2"], o1["all_valid2"][j]), (case, i, j)
+            for k in ("bg", "nbg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "zeta",
+                      "seff", "J", "u1", "u2", "img2", "fz"):
+                ok, worst = T.within(k, o[k], o1[k][j], ctx)
+                assert ok, (case, i, j, k, worst)
+            if not o2:
+                continue
+            pix = dict(zeta=o1["zeta"][j], J=o1["J"][j], u1=o1["u1"][j], u2=o1["u2"][j], seff=o1["seff"][j])
+            q = OK.pass2(d["sb"][j], r, nbr, det, d["s0"], d["axis"], d["frames_phi0"], d["osc"], d["p2_sd"],
+                         d["p2_sm"], d["p2_gain"], d["prof"], o1["bg"][j], o1["nbg"][j], d["p2_rcw"], pix)
+            ctx2 = {k: o2[k][j] for k in o2}
+            for k in ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "ipartner", "rho", "p_fg"):
+                ok, worst = T.within(k, q[k], o2[k][j], ctx2)
+                assert ok, (case, i, j, k, worst, q[k], o2[k][j])
+
+
+@pytest.mark.parametrize("case", ("binned", "superpix", "crowded"))
+def test_oracle_gather_matches_reference_shoeboxes(case):
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    frames = G.frames_of(case)
+    read = [f - 1 for f in range(1, spec.nframes + 1) if f not in set(excl)]
+    prepared = {}
+    for i in G.chunks(case):
+        d, rc, nb, o1, o2 = G.chunk(case, i)
+        Dz, bx = int(d["shape"][0]), int(d["shape"][2])
+        for j in range(d["sb"].shape[0]):
+            s = int(rc["pxs"][j]) if "pxs" in rc else 1
+            iz0, fb = int(rc["iz0"][j]), int(rc["fb"][j])
+            need = [fi for fi in read if iz0 <= fi < iz0 + Dz * fb]
+            for fi in need:
+                if (s, fi) not in prepared:
+                    pf = OG.prepare_frame(frames[fi], spec.overload, 0, mask)
+                    prepared[(s, fi)] = pf if s == 1 else OG.superpixel_frame(pf, s)
+            # the reference's block takes every frame read up to the first read frame at / after its last needed
+            # frame; the stored rows of a one-block sweep see every frame of their box range that was read
+            sb = OG.gather_shoebox({fi: prepared[(s, fi)] for fi in need}, need, iz0, fb, Dz, bx, int(rc["iy0"][j]),
+                                   int(rc["ix0"][j]))
+            assert np.array_equal(sb, d["sb"][j], equal_nan=True), (case, i, j)
+
+
+@pytest.mark.parametrize("case", ("adaptive", "config1"))
+def test_oracle_accumulation_matches_reference_grids(case):
+    z = G.load(case)
+    accs = sorted(int(k[1:].split("_")[0]) for k in z if k.startswith("a") and k.endswith("_num"))
+    assert accs
+    for a in accs:
+        p = f"a{a}_"
+        inp = {k[len(p) + 3:]: v for k, v in z.items() if k.startswith(p + "in_")}
+        num = np.zeros_like(z[p + "num"])
+        den = np.zeros_like(z[p + "den"])
+        for j in range(inp["img2"].shape[0]):
+            o = dict(img2=inp["img2"][j], isum=inp["isum"][j], J=inp["J"][j], seff=inp["seff"][j], u1=inp["u1"][j],
+                     u2=inp["u2"][j], all_valid2=inp["ok2"][j])
+            OK.accumulate(num, den, o, int(inp["region"][j]))
+        np.testing.assert_allclose(num, z[p + "num"], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(den, z[p + "den"], rtol=1e-12, atol=1e-12)
+
+
+def test_decode_bins_known_answer():
+    """XPG's known-answer test of binned sums (`tests/test_robustness.py:44-54`): an overload in any frame wins (-2),
+    then masked (-1); an empty bin is unrecorded; values are stored + 3."""
+    acc = np.array([[[5.0, np.inf], [np.nan, 0.0]], [[2.0, 3.0], [4.0, 1.0]]], np.float32)
+    cnt = np.array([2, 0])
+    out = OG.decode_bins(acc, cnt, fb=2)
+    np.testing.assert_array_equal(out[0], np.array([[5.0 + 3, 3 - 1.0], [3 - 2.0, 3.0]], np.float32))
+    assert np.all(out[1] == 0.0)
+    assert np.isnan(np.float32(np.nan) + np.float32(np.inf)) and np.isinf(np.float32(np.inf) + np.float32(3.0))
+
+
+@pytest.mark.parametrize("case", ("binned", "superpix"))
+def test_oracle_profile_finalisation_matches_reference(case):
+    """Profiles of one-block sweeps (every accumulation call stored) from the reference's accumulated grids."""
+    z = G.load(case)
+    nreg = z["prof_0"].shape[0]
+    num = np.zeros((nreg, 41, 41))
+    den = np.zeros((nreg, 41, 41))
+    for k in z:
+        if k.startswith("a") and k.endswith("_num"):
+            num += z[k]
+            den += z[k[:-4] + "_den"]
+    prof = OK.finalize_profiles(num, den)
+    np.testing.assert_allclose(prof, z["prof_0"], rtol=2e-7, atol=0)

@@ -59,14 +59,19 @@ def fit_rocking_width(sel_fit, g, sm_guess, lo_fac=0.2, hi_fac=3.0):
     lo = g.z_to_phi(k.astype(float))
     hi = g.z_to_phi(k + 1.0)
     lo, hi = np.minimum(lo, hi), np.maximum(lo, hi)
-    best = (np.inf, sm_guess)
-    for sm in sm_guess * np.exp(np.linspace(np.log(lo_fac), np.log(hi_fac), 61)):
+    grid = sm_guess * np.exp(np.linspace(np.log(lo_fac), np.log(hi_fac), 61))
+
+    def cost(sm):
         s = sm / zeta[:, None] * np.sqrt(2)
         R = 0.5 * (erf((hi - phi[:, None]) / s) - erf((lo - phi[:, None]) / s))
         R = R / np.maximum(R.sum(1, keepdims=True), 1e-9)
-        cost = np.sum(tot * (frac - R) ** 2)
-        if cost < best[0]:
-            best = (cost, sm)
+        return np.sum(tot * (frac - R) ** 2)
+    from .geometry import _pool
+    costs = list(_pool().map(cost, grid))           # every candidate's cost is computed whole, as one call
+    best = (np.inf, sm_guess)
+    for c, sm in zip(costs, grid):
+        if c < best[0]:
+            best = (c, sm)
     return float(best[1])
 
 
@@ -95,7 +100,10 @@ def adapt_block(g, strong_sets, sd_run, sm_run, sd_b, sm_b, rcw_b):
     lo = g.z_to_phi(k.astype(float))
     hi = g.z_to_phi(k + 1.0)
     lo, hi = np.radians(np.minimum(lo, hi)), np.radians(np.maximum(lo, hi))
-    Bm = rc_basis(lo, hi, np.radians(PH), ZK, sm_new)
+    from .geometry import par_rows
+    PHr = np.radians(PH)
+    Bm = np.concatenate(par_rows(lambda a, b: rc_basis(lo[a:b], hi[a:b], PHr[a:b], ZK[a:b], sm_new), len(PH),
+                                 min_rows=2048))
     tot = np.maximum(F.sum(1, keepdims=True), 1e-9)
     A = (Bm * np.sqrt(tot)[:, :, None]).reshape(-1, len(RC_C))
     y = (F / tot * np.sqrt(tot)).reshape(-1)

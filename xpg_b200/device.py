@@ -168,10 +168,15 @@ class RowSet:
         """Launch groups: rows of one shoebox shape (side, depth), so that each launch sizes its shared memory
         (and decides whether the shoebox is staged there) for exactly its rows. Largest shapes first."""
         out = []
-        shapes = sorted({(int(b), int(d)) for b, d in zip(self.bx, self.Dz)}, key=lambda s: -s[0] * s[0] * s[1])
-        for b, d in shapes:
-            rows = np.flatnonzero((self.bx == b) & (self.Dz == d))
-            out.append((b, d, rows.astype(np.int32)))
+        if self.n == 0:
+            return out
+        key = self.bx * 128 + self.Dz
+        order = np.argsort(key, kind="stable")
+        uk, start = np.unique(key[order], return_index=True)
+        stop = np.append(start[1:], order.size)
+        for k, a, e in zip(uk, start, stop):
+            out.append((int(k // 128), int(k % 128), order[a:e].astype(np.int32)))
+        out.sort(key=lambda g: -g[0] * g[0] * g[1])
         return out
 
     def view(self, order=None, max_bx=None, max_dz=None):

@@ -43,15 +43,12 @@ class IntegrationResult:
 
 def _reference_row_order(rows, bucket, bxs, pxs, has_partner):
     """The block's rows in XPG's kernel-call order (`xpg/integrate.py:375-381`): depth bucket, then box side, then
-    super-pixel side (both ascending), partners first within a group."""
-    out = []
-    for B in DZ_BUCKETS:
-        for bx in np.unique(bxs[rows]):
-            for sp in np.unique(pxs[rows]):
-                sel = rows[(bucket[rows] == B) & (bxs[rows] == bx) & (pxs[rows] == sp)]
-                sel = sel[np.argsort(~has_partner[sel], kind="stable")]
-                out.append(sel)
-    return np.concatenate(out) if out else np.zeros(0, int)
+    super-pixel side (all ascending), partners first within a group, block-row order otherwise (a stable sort on
+    one combined key)."""
+    if rows.size == 0:
+        return rows
+    key = ((bucket[rows].astype(np.int64) * 1024 + bxs[rows]) * 64 + pxs[rows]) * 2 + (~has_partner[rows]).astype(np.int64)
+    return rows[np.argsort(key, kind="stable")]
 
 
 class _Block:
