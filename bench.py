@@ -157,7 +157,9 @@ class Block:
                          device=self.device)
 
     def bytes_per_kernel(self):
-        """Algorithmic bytes of every kernel over one step ("Roofline accounting")."""
+        """Algorithmic bytes of every kernel over one step: each shoebox voxel read once (4 B), the per-pixel and
+        per-frame tables written or read once, the row's scalars; the gather reads every raw pixel its boxes cover
+        and writes the box once; decode_bins reads and writes the binned rows."""
         p = self.plan
         V = (p.Dz * p.bx * p.bx).astype(np.float64)
         P = (p.bx * p.bx).astype(np.float64)
@@ -360,8 +362,9 @@ def reference_arm(args):
 
     import torch
     from oracle import pipeline as OP
+    from oracle.plan import plan_integration
     from xpg_b200 import synth
-    from xpg_b200.plan import IntegrationModel, plan_integration
+    from xpg_b200.plan import IntegrationModel
     cores = len(os.sched_getaffinity(0))
     spec = synth.config2() if args.workload == "config2-block" else synth.config1()
     edges = np.array([0.0, 360.0]) if args.workload == "config2-block" else np.array([0.0, 100.0])

@@ -144,6 +144,14 @@ int xi_version(void);
  * because its shape exceeded its call's max_bx / max_dz. */
 int xi_status(void *stream);
 
+/* Launch tuning (process-wide; no counterpart in XPG, whose torch kernels have no launch shape): the largest
+ * shoebox (bytes) pass 1 / pass 2 stage in shared memory, and pass 2's fit-list capacity (voxels). Results do not
+ * depend on these. */
+#define XI_TUNE_PASS1_STAGE_BYTES 1
+#define XI_TUNE_PASS2_STAGE_BYTES 2
+#define XI_TUNE_PASS2_LIST_CAP 3
+int xi_tune(int key, long long value);
+
 /* Frame gather (xpg/integrate.py:704-787 with the preparation of :667-699 and the encoding of
  * xpg/io/images.py:72-102): every row's box window of every frame of the wedge inside its frame range is written
  * to its arena slot (value + 3), or, for binned rows (fb > 1), added to its bin in IEEE encoding (overloaded: NaN,
@@ -174,6 +182,120 @@ int xi_finalize_profiles(const double *num, const double *den, int n_regions, fl
  * partner, variances, correlation and recorded fractions. prof: (n_regions, 41, 41). */
 int xi_pass2(const XiDetector *det, const XiRows *rows, const XiBlock *blk, const float *arena, const float *prof,
              const XiPass2In *in, XiPass2Out *out, void *stream);
+
+/* ---- Planning: predictions, shoebox boxes and neighbour lists (float64) -------------------------------------
+ * XPG plans an integration run in numpy on the host (xpg/integrate.py:222-316 with the predictions of
+ * xpg/geometry.py:468-545 and the neighbour search of xpg/integrate.py:164-172); these entry points do the same on
+ * the device. Row order is the reference's: block by block, then solution (phi_a, phi_b), then turn (0, +360 deg),
+ * then Miller-index order (h slowest, l fastest on the generated grid; list order for an explicit list). Device
+ * workspace is the caller's (sizes from the *_workspace functions). */
+
+#define XI_PANEL_F64 28           /* doubles per panel record of XiPlanDetector.panels */
+
+/* Detector of the planner (xpg/geometry.py:246-410; the panel maps of xpg/detector.py:79-90). Panel record k:
+ * P0[3] Bx[3] By[3] n[3] u1[3] u2[3] un[3] P0.n Bx.Bx By.By x1 x2 y1 y2 with n = Bx x By, u1 = Bx / qx,
+ * u2 = By / qy, un = u1 x u2 and the panel's inclusive 1-based pixel rectangle. Device pointers. */
+typedef struct {
+    int n_panels;
+    const double *panels;           /* (n_panels, XI_PANEL_F64) */
+    int segmented;                  /* panel rectangles bound the hits; pixel_to_lab looks the panel up in segmap */
+    const int16_t *segmap;          /* (seg_ny, seg_nx) panel of each pixel, -1 in gaps */
+    int seg_nx, seg_ny;
+    const double *geo_x, *geo_y;    /* (geo_ny, geo_nx) distortion tables (pixels); NULL: none */
+    int geo_nx, geo_ny;
+    int parallax;                   /* thick-sensor parallax (tsens > 0 and mu > 0) */
+    double tsens, mu;
+    double orgx, orgy, qx, qy, distance;
+    double ed1[3], ed2[3], ed3[3];  /* detector axes as given, ed3 = ed1 x ed2 (single-panel lab map) */
+    double beam[3];                 /* incident beam direction as given (Lorentz factor) */
+    double pol_n[3], pol_main[3];   /* polarisation plane normal and its in-plane partner (lp_factor) */
+    double pol_f;                   /* polarisation fraction */
+    double nx, ny;                  /* detector size in pixels (acceptance test, regions) */
+} XiPlanDetector;
+
+/* Predictions of one phi block (xpg/geometry.py:468-545 and the acceptance test of xpg/integrate.py:101-122). */
+typedef struct {
+    double astar[9];                /* A* row-major (columns a*, b*, c*): p = A* h */
+    int hmax[3];                    /* generated grid: |h| <= hmax[0], |k| <= hmax[1], |l| <= hmax[2] */
+    double q2_max, q2_min;          /* keep q2_min < |p|^2 <= q2_max (1 / dmin^2, 1 / dmax^2) */
+    int centring;                   /* lattice centring letter: 'P' (none), 'C', 'A', 'B', 'I', 'F', 'R' */
+    const int32_t *hkl;             /* explicit Miller indices (n_hkl, 3) instead of the grid; NULL: grid */
+    int64_t n_hkl;
+    double axis[3];                 /* rotation axis as given */
+    double rot_K[9], rot_kk[9];     /* R(phi) = cos I + sin K + (1 - cos) kk of the unit axis */
+    double s0[3];                   /* incident wave vector */
+    double phi_lo, phi_hi;          /* accepted spindle angles [lo, hi) in degrees */
+    double phi0, osc, z_shift;      /* z = (phi - phi0) / osc + z_shift */
+    double deg, rad;                /* 180 / pi and pi / 180 as the host rounds them */
+    double acc_s0[3], acc_axis[3];  /* first block's s0 and axis: zeta_k of the acceptance test */
+    double min_zeta;                /* |zeta_k| >= min_zeta */
+    double x_hi, y_hi;              /* 0.5 <= x < x_hi, 0.5 <= y < y_hi (first block's detector + 0.5) */
+    double z_lo, z_hi;              /* z_lo <= z < z_hi */
+    int block, lattice;             /* written to every row */
+} XiPredict;
+
+/* Prediction rows (device, capacity rows each). */
+typedef struct {
+    int32_t *hkl;                   /* (cap, 3) */
+    double *phi, *S, *x, *y, *z, *zeta, *polarization, *zeta_k;     /* S: (cap, 3) */
+    int32_t *block, *lattice;
+} XiPredictOut;
+
+/* Device workspace of xi_predict_count / xi_predict_write (bytes). */
+size_t xi_predict_workspace(const XiPredict *P);
+/* Counts the block's predictions (synchronises the stream; *n_rows on the host). The workspace keeps the counts for
+ * the write that follows. */
+int xi_predict_count(const XiPredict *P, const XiPlanDetector *det, void *ws, size_t ws_bytes, int64_t *n_rows,
+                     void *stream);
+/* Writes the block's predictions (the count call must precede it with the same arguments) into rows [0, n_rows)
+ * of out; fails with XI_E_LIMIT when n_rows > cap. */
+int xi_predict_write(const XiPredict *P, const XiPlanDetector *det, void *ws, size_t ws_bytes, const XiPredictOut *out,
+                     int64_t cap, void *stream);
+
+/* Shoebox rules per prediction (xpg/integrate.py:233-285 and :288-291): depth, phi binning, coverage, side,
+ * super-pixels, origin, neighbour-ellipsoid widths, region, frame range. */
+typedef struct {
+    int64_t n;
+    const double *x, *y, *z, *zeta_k;
+    double sigma_m;                 /* model sigma_M (deg) */
+    double abs_osc;                 /* |osc| of the first block (deg) */
+    double osc2_12;                 /* osc^2 / 12 */
+    double rsd_box;                 /* radians(sigma_D * widen): box side */
+    double rsd;                     /* radians(sigma_D): neighbour ellipsoids */
+    double qmin;                    /* min(qx, qy) */
+    int box;                        /* global box side */
+    int box_fixed;                  /* model.box_xy: every side is box, no super-pixels */
+    int n_xyb;
+    int xyb[16];                    /* side buckets below box, then box */
+    int f_first, f_last;            /* frame numbers of the run */
+    int n_regions_xy;
+} XiBoxRules;
+
+typedef struct {
+    int32_t *iz0, *dz, *fb, *Dz, *bx, *pxs, *ix0, *iy0, *region, *zstart, *zend;
+    uint8_t *flags;                 /* bit 0 wide, bit 1 truncated, bit 2 kept (a depth bucket exists) */
+    float *coverage;
+    double *sx_px, *sz_f;           /* neighbour-ellipsoid widths (pixels, frames) */
+} XiBoxOut;
+
+int xi_plan_boxes(const XiBoxRules *B, const XiPlanDetector *det, const XiBoxOut *out, void *stream);
+
+/* Nearest neighbours (scipy cKDTree.query(pts, k + 1, distance_upper_bound=radius) on pts = (x / sx, y / sx,
+ * z / sz), first column dropped: xpg/integrate.py:164-172): for every point its k nearest other points closer than
+ * radius, by increasing distance (ties by index); missing entries j = 0, d = +inf. lo / hi bound the scaled points
+ * (a cell grid over them; points outside are clamped into the edge cells, which keeps the result exact). */
+#define XI_KNN_MAX 16
+typedef struct {
+    int64_t n;
+    const double *x, *y, *z;
+    double sx, sz;
+    double lo[3], hi[3];
+    double radius;
+    int k;
+} XiKnn;
+
+size_t xi_knn_workspace(const XiKnn *q);
+int xi_knn(const XiKnn *q, void *ws, size_t ws_bytes, int32_t *nbj, double *nbd, void *stream);
 
 #ifdef __cplusplus
 }

