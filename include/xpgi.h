@@ -297,6 +297,19 @@ typedef struct {
 size_t xi_knn_workspace(const XiKnn *q);
 int xi_knn(const XiKnn *q, void *ws, size_t ws_bytes, int32_t *nbj, double *nbd, void *stream);
 
+/* xi_knn without a workspace argument; it has no counterpart in XPG (whose neighbour search runs on the host).
+ * For callers that cannot allocate device memory: a program binding this library through a plain C FFI beside a
+ * framework that has already reserved the GPU's memory in its own pool (cudaMalloc would fail there, and
+ * cudaMalloc / cudaFree can stall the whole device). The scratch memory is an array inside the library, sized for at
+ * most XI_KNN_NOALLOC_MAX_POINTS points (larger calls fail with XI_E_LIMIT); bounds that would need more than
+ * XI_KNN_NOALLOC_MAX_CELLS grid cells get coarser cells, with the same result. Same inputs, outputs and results as
+ * xi_knn; nothing is allocated. The first call on each device looks up the array's device address: make it before
+ * any stream capture. Every call on a device shares the one array, so calls that may overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+#define XI_KNN_NOALLOC_MAX_POINTS (1 << 19)
+#define XI_KNN_NOALLOC_MAX_CELLS (1 << 18)
+int xi_knn_noalloc(const XiKnn *q, int32_t *nbj, double *nbd, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

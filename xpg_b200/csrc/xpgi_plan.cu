@@ -13,6 +13,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <mutex>
+
 #include <cub/device/device_scan.cuh>
 
 #include "xpgi.h"
@@ -470,7 +472,7 @@ struct KnnGrid {
     int64_t n_cells;
 };
 
-bool knn_grid(const XiKnn* q, KnnGrid* g) {
+bool knn_grid(const XiKnn* q, KnnGrid* g, int64_t max_cells = kMaxCells) {
     if (!(q->radius > 0.0) || !isfinite(q->radius)) return false;
     double ext[3];
     for (int a = 0; a < 3; ++a) {
@@ -486,7 +488,7 @@ bool knn_grid(const XiKnn* q, KnnGrid* g) {
             if (d > 1e9) over = true;
             g->dims[a] = d < 1.0 ? 1 : (int)(d > 1e9 ? 1e9 : d);
             n *= g->dims[a];
-            if (n > kMaxCells) over = true;
+            if (n > max_cells) over = true;
         }
         if (!over) {
             g->cs = cs;
@@ -612,14 +614,56 @@ __global__ void k_knn_query(XiKnn q, KnnGrid g, const int* __restrict__ cell_of,
     }
 }
 
-int knn_check(const XiKnn* q, KnnGrid* g) {
+int knn_check(const XiKnn* q, KnnGrid* g, int64_t max_cells = kMaxCells) {
     if (!q) return xi_fail(XI_E_ARG, "knn: null argument");
     if (q->n < 0 || q->k < 0) return xi_fail(XI_E_ARG, "knn: negative size");
     if (q->k > XI_KNN_MAX) return xi_fail(XI_E_LIMIT, "knn: k beyond XI_KNN_MAX");
     if (q->n >= INT32_MAX) return xi_fail(XI_E_LIMIT, "knn: more than 2^31 points");
     if (q->n && (!q->x || !q->y || !q->z)) return xi_fail(XI_E_ARG, "knn: null coordinates");
     if (!(q->sx > 0.0) || !(q->sz > 0.0)) return xi_fail(XI_E_ARG, "knn: scales must be positive");
-    if (!knn_grid(q, g)) return xi_fail(XI_E_ARG, "knn: bounds or radius not finite");
+    if (!knn_grid(q, g, max_cells)) return xi_fail(XI_E_ARG, "knn: bounds or radius not finite");
+    return XI_OK;
+}
+
+}  // namespace
+
+// ---- neighbour search in library-owned scratch memory (xi_knn_noalloc) -----------------------------------------
+// The scratch of xi_knn (cell counters, sorted points, the scan's temporary storage) laid out for at most
+// XI_KNN_NOALLOC_MAX_POINTS points on at most XI_KNN_NOALLOC_MAX_CELLS grid cells, in one array that every device
+// loading the library holds (about 21 MB) until the process exits.
+namespace {
+
+constexpr size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr int64_t kNoAllocPoints = XI_KNN_NOALLOC_MAX_POINTS;
+constexpr int64_t kNoAllocCells = XI_KNN_NOALLOC_MAX_CELLS;
+constexpr size_t kNoAllocScanBytes = (size_t)1 << 20;
+constexpr size_t kNoAllocBytes = 3 * round256(sizeof(int) * kNoAllocCells) + 2 * round256(sizeof(int) * kNoAllocPoints) +
+                                 round256(3 * sizeof(double) * kNoAllocPoints) + kNoAllocScanBytes;
+constexpr int kNoAllocDevices = 64;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_knn_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kNoAllocDevices] = {};
+
+// Device address of g_knn_scratch on the current device (host code sees only a stand-in for the array), looked up
+// once per device.
+int knn_scratch(void** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return xi_cuda_check("xi_knn_noalloc: current device");
+    if (dev < 0 || dev >= kNoAllocDevices) return xi_fail(XI_E_LIMIT, "xi_knn_noalloc: device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_knn_scratch) != cudaSuccess || !p)
+            return xi_cuda_check("xi_knn_noalloc: address of the scratch array");
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
     return XI_OK;
 }
 
@@ -716,6 +760,34 @@ int xi_knn(const XiKnn* q, void* ws, size_t ws_bytes, int32_t* nbj, double* nbd,
     k_knn_scatter<<<nb, 256, 0, s>>>(*q, w.cell_of, w.start, w.fill, w.spts, w.sidx);
     if (q->k > 0) k_knn_query<<<nb, 256, 0, s>>>(*q, g, w.cell_of, w.start, w.count, w.spts, w.sidx, nbj, nbd);
     return xi_cuda_check("xi_knn");
+}
+
+int xi_knn_noalloc(const XiKnn* q, int32_t* nbj, double* nbd, void* stream) {
+    KnnGrid g;
+    int rc = knn_check(q, &g, kNoAllocCells);       // coarser cells when the bounds need more: same neighbours
+    if (rc) return rc;
+    if (q->n > kNoAllocPoints)
+        return xi_fail(XI_E_LIMIT, "xi_knn_noalloc: more points than XI_KNN_NOALLOC_MAX_POINTS (524288); "
+                                   "use xi_knn with a workspace");
+    if (q->n == 0) return XI_OK;
+    if (!nbj || !nbd) return xi_fail(XI_E_ARG, "xi_knn_noalloc: null output");
+    void* base = nullptr;
+    rc = knn_scratch(&base);
+    if (rc) return rc;
+    KnnWs w = knn_ws(q, g, base);
+    if (w.bytes > kNoAllocBytes) return xi_fail(XI_E_LIMIT, "xi_knn_noalloc: scratch layout beyond the array");
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned nb = (unsigned)((q->n + 255) / 256);
+    // the array keeps the previous call's contents: the cell counters and fill cursors start from zero
+    cudaMemsetAsync(w.count, 0, sizeof(int) * g.n_cells, s);
+    cudaMemsetAsync(w.fill, 0, sizeof(int) * g.n_cells, s);
+    k_knn_bin<<<nb, 256, 0, s>>>(*q, g, w.count, w.cell_of);
+    size_t cb = w.cub_bytes;
+    if (cub::DeviceScan::ExclusiveSum(w.cub, cb, w.count, w.start, (int)g.n_cells, s) != cudaSuccess)
+        return xi_cuda_check("xi_knn_noalloc scan");
+    k_knn_scatter<<<nb, 256, 0, s>>>(*q, w.cell_of, w.start, w.fill, w.spts, w.sidx);
+    if (q->k > 0) k_knn_query<<<nb, 256, 0, s>>>(*q, g, w.cell_of, w.start, w.count, w.spts, w.sidx, nbj, nbd);
+    return xi_cuda_check("xi_knn_noalloc");
 }
 
 }  // extern "C"

@@ -78,6 +78,7 @@ class XiSynthBackground(C.Structure):
 
 XI_PANEL_F64 = 28
 XI_KNN_MAX = 16
+XI_KNN_NOALLOC_MAX_POINTS, XI_KNN_NOALLOC_MAX_CELLS = 1 << 19, 1 << 18
 _d3 = C.c_double * 3
 
 
@@ -126,7 +127,7 @@ XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP = 1
 
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
-           "xi_plan_boxes", "xi_knn", "xi_predict_workspace", "xi_knn_workspace")
+           "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_predict_workspace", "xi_knn_workspace")
 
 _LIB = None
 
@@ -154,6 +155,7 @@ def load(path=None):
     lib.xi_plan_boxes.argtypes = [C.POINTER(XiBoxRules), C.POINTER(XiPlanDetector), C.POINTER(XiBoxOut), C.c_void_p]
     lib.xi_knn_workspace.argtypes = [C.POINTER(XiKnn)]
     lib.xi_knn.argtypes = [C.POINTER(XiKnn), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.xi_knn_noalloc.argtypes = [C.POINTER(XiKnn), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_status.argtypes = [C.c_void_p]
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
