@@ -103,7 +103,7 @@ def adapt_block(g, strong_sets, sd_run, sm_run, sd_b, sm_b, rcw_b):
     from .geometry import par_rows
     PHr = np.radians(PH)
     Bm = np.concatenate(par_rows(lambda a, b: rc_basis(lo[a:b], hi[a:b], PHr[a:b], ZK[a:b], sm_new), len(PH),
-                                 min_rows=2048))
+                                 min_rows=128))
     tot = np.maximum(F.sum(1, keepdims=True), 1e-9)
     A = (Bm * np.sqrt(tot)[:, :, None]).reshape(-1, len(RC_C))
     y = (F / tot * np.sqrt(tot)).reshape(-1)

@@ -63,6 +63,8 @@ TIMER = KernelTimer()
 
 
 def _dev(a, dtype, device):
+    if torch.is_tensor(a):                  # already a tensor (the planner's device columns): convert in place
+        return a.to(device=device, dtype=dtype).contiguous()
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(device, non_blocking=False)
 
 
@@ -136,20 +138,20 @@ class RowSet:
         self.n_vox = int(Vp.sum()) + 4
         self.n_pix = int(P.sum())
         self.n_frm = int(self.Dz.sum())
-        K = int(np.asarray(nb["x"]).shape[1]) if n else 0
+        K = int(nb["x"].shape[1]) if n else 0
         if K > N.XI_MAX_K:
             raise ValueError(f"{K} neighbour columns > {N.XI_MAX_K}")
         d = device
         self.t = dict(
-            S=_dev(np.asarray(S, np.float32).reshape(n, 3), F32, d), phi=_dev(phi, F32, d),
+            S=_dev(S, F32, d).reshape(n, 3), phi=_dev(phi, F32, d),
             ix0=_dev(ix0, torch.int32, d), iy0=_dev(iy0, torch.int32, d), iz0=_dev(iz0, torch.int32, d),
-            fb=_dev(np.asarray(fb, np.float32), F32, d), region=_dev(region, torch.int32, d),
-            has_p=_dev(np.asarray(has_p, np.float32), F32, d), pS=_dev(np.asarray(pS, np.float32).reshape(n, 3), F32, d),
+            fb=_dev(fb, F32, d), region=_dev(region, torch.int32, d),
+            has_p=_dev(has_p, F32, d), pS=_dev(pS, F32, d).reshape(n, 3),
             pphi=_dev(pphi, F32, d), pxs=_dev(pxs, torch.int32, d), Dz=_dev(self.Dz, torch.int32, d),
             bx=_dev(self.bx, torch.int32, d), sb_off=_dev(self.sb_off, torch.int64, d),
             pix_off=_dev(self.pix_off, torch.int64, d), frm_off=_dev(self.frm_off, torch.int64, d))
         for k in ("x", "y", "z", "sx", "sz"):
-            self.t["nb" + k] = _dev(np.asarray(nb[k], np.float32).reshape(n, K), F32, d)
+            self.t["nb" + k] = _dev(nb[k], F32, d).reshape(n, K)
         r = N.XiRows()
         r.n = n
         for k in ("S", "phi", "ix0", "iy0", "iz0", "fb", "region", "has_p", "pS", "pphi", "pxs", "Dz", "bx",
@@ -307,7 +309,6 @@ class GatherRows:
         g.order = None
         g.n_order = 0
         self.s = g
-        self.iz0 = np.asarray(iz0, np.int64)
         self.span = rows.Dz * fb
         self.binned = binned
 

@@ -58,18 +58,28 @@ class _Block:
         self.b = b
         self.rows = rows                                  # global row indices, reference kernel-call order
         p = plan
-        refl = p.refl
-        pj = p.partner[rows]
+        dv = p.dev                                        # the planner's device columns
+        rt = torch.as_tensor(rows).to(device)
+        sel = lambda t: t.index_select(0, rt)
+        pj = dv["nbj"][:, 0].long().index_select(0, rt)   # nearest neighbour: the partner where there is one
+        rad = lambda phi: (phi * (np.pi / 180.0)).float()  # numpy's radians, then float32
+        nb = {k: sel(dv["nb" + k]) for k in ("x", "y", "z", "sx", "sz")}
+        if nb["x"].shape[1] != p.nb["x"].shape[1]:        # foreign-spot columns were added on the host
+            nb = {k: v[rows] for k, v in p.nb.items()}
+        ix0, iy0, iz0, fb, pxs = (sel(dv[k]) for k in ("ix0", "iy0", "iz0", "fb", "pxs"))
         self.rowset = D.RowSet(
-            S=refl["S"][rows].astype(np.float32), phi=np.radians(refl["phi"][rows]).astype(np.float32),
-            ix0=p.ix0[rows], iy0=p.iy0[rows], iz0=p.iz0[rows], fb=p.fb[rows], region=p.region[rows],
-            has_p=p.has_partner[rows], pS=refl["S"][pj].astype(np.float32),
-            pphi=np.radians(refl["phi"][pj]).astype(np.float32), pxs=p.pxs[rows], Dz=p.Dz[rows], bx=p.bx[rows],
-            nb={k: v[rows] for k, v in p.nb.items()}, device=device, sb_bias=3.0)
-        self.grows = D.GatherRows(self.rowset, p.ix0[rows], p.iy0[rows], p.iz0[rows], p.fb[rows], p.pxs[rows],
-                                  device)
+            S=sel(dv["S"]).float(), phi=rad(sel(dv["phi"])), ix0=ix0, iy0=iy0, iz0=iz0, fb=fb,
+            region=sel(dv["region"]), has_p=sel(dv["has_partner"]), pS=dv["S"].index_select(0, pj).float(),
+            pphi=rad(dv["phi"].index_select(0, pj)), pxs=pxs, Dz=p.Dz[rows], bx=p.bx[rows], nb=nb, device=device,
+            sb_bias=3.0)
+        self.grows = D.GatherRows(self.rowset, ix0, iy0, iz0, p.fb[rows], pxs, device)
         self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
+        order = np.argsort(rows, kind="stable")            # local rows by global row: outputs leave in plan order
+        self.perm_t = torch.as_tensor(order).to(device)
+        self.rows_sorted = rows[order]
+        srt = self.rows_sorted
+        self.span = (int(srt[0]), int(srt[-1]) + 1) if srt.size and srt[-1] - srt[0] + 1 == srt.size else None
         self.z_lo = p.iz0[rows].astype(np.int64)
         self.z_hi = self.z_lo + self.grows.span - 1      # last frame index a row's box can take
 
@@ -156,38 +166,36 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         den = torch.zeros_like(num)
         if learn_profiles:
             D.accumulate(rs, p1, nreg, num, den)
-        h1 = _host_pass1(p1, rs)
+        h1 = _host_rows(p1.t, ADAPT_KEYS)
         rows = blk.rows
         if adaptive:
             st = _adapt_rows(h1, plan, rows)
             sets = []
             if st.any():
-                F = _fz_padded(h1, rs, st)
-                sets.append((F, refl["phi"][rows][st], refl["zeta_k"][rows][st], plan.iz0[rows][st],
-                             h1["m_d"][st], refl["x"][rows][st], refl["y"][rows][st]))
+                F = _fz_padded(p1, rs, st)
+                rst = rows[st]
+                sets.append((F, refl["phi"][rst], refl["zeta_k"][rst], plan.iz0[rst], h1["m_d"][st], refl["x"][rst],
+                             refl["y"][rst]))
             sm_b, rcw_b, sd_next, params = A.adapt_block(g, sets, sd, sm, sd_b, sm_b, rcw_b)
             if sd_next is not None:
                 state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
             block_params[b] = params
         prof = torch.empty((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
         D.finalize_profiles(num, den, prof)
-        h2 = None
+        cols = {k: p1.t[k] for k in P1_OUT}
         if not moments_only:
             c2, k2 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
             p2 = D.Pass2Buffers(rs)
             D.pass2(det, rs, c2, blk.arena, prof, p1, p2)
-            h2 = {k: v.double().cpu().numpy() for k, v in p2.t.items()}
+            cols.update({k: p2.t[k] for k in P2_OUT})
         D.status()
         prof_by_block[b] = prof.cpu().numpy()
-        for k in ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m"):
-            out[k][rows] = h1[k]
-        out["n_over"][rows] = h1["n_over"]
-        out["n_fg_masked"][rows] = h1["n_fg_masked"]
+        h = _host_rows(cols, tuple(cols), blk.perm_t)     # in plan (global row) order
+        dst = slice(*blk.span) if blk.span is not None else blk.rows_sorted
+        for k, v in h.items():
+            out[k][dst] = v
         if fz_out is not None:
-            fz_out[rows] = _fz_padded(h1, rs, np.ones(rs.n, bool))
-        if h2 is not None:
-            for k in ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "rho", "p_fg"):
-                out[k][rows] = h2[k]
+            fz_out[rows] = _fz_padded(p1, rs, np.ones(rs.n, bool)).astype(np.float32)
         t_dev += time.time() - tg
 
     # ---- frame loop: wedges of consecutive frame numbers --------------------------------------------------------
@@ -241,24 +249,38 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     return res
 
 
-def _host_pass1(p1: D.Pass1Buffers, rs: D.RowSet):
-    """Per-row pass-1 outputs on the host (one stacked float64 copy, `xpg/integrate_kernels.py:169-183`), plus the
-    per-frame fz array."""
-    keys = D.Pass1Buffers.SCALARS + D.Pass1Buffers.COUNTS
-    st = torch.stack([p1.t[k].double() for k in keys]).cpu().numpy()
-    h = {k: st[i].astype(np.float32 if k in D.Pass1Buffers.SCALARS else np.int64) for i, k in enumerate(keys)}
-    h["fz"] = p1.t["fz"].cpu().numpy()
-    return h
+ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")
+P1_OUT = ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m", "n_over", "n_fg_masked")
+P2_OUT = ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "rho", "p_fg")
 
 
-def _fz_padded(h1, rs: D.RowSet, sel):
-    """fz of the selected rows, padded to the deepest box (zeros)."""
+def _host_rows(t, keys, perm=None):
+    """Per-row device outputs on the host (`xpg/integrate_kernels.py:169-183`), optionally permuted on the device
+    first: one stacked copy per dtype."""
+    out = {}
+    for dt in (torch.float32, torch.int64):
+        ks = [k for k in keys if t[k].dtype == dt]
+        if not ks:
+            continue
+        st = torch.stack([t[k] for k in ks])
+        if perm is not None:
+            st = st.index_select(1, perm)
+        st = st.cpu().numpy()
+        out.update({k: st[i] for i, k in enumerate(ks)})
+    return out
+
+
+def _fz_padded(p1: D.Pass1Buffers, rs: D.RowSet, sel):
+    """fz of the selected rows, padded to the deepest box (zeros): gathered on the device, float64 on the host."""
     rows = np.flatnonzero(sel)
-    F = np.zeros((rows.size, MAX_DZ), np.float32)
-    for k, j in enumerate(rows):
-        o, dz = rs.frm_off[j], rs.Dz[j]
-        F[k, :dz] = h1["fz"][o:o + dz]
-    return F.astype(np.float64) if rows.size else F
+    if rows.size == 0:
+        return np.zeros((0, MAX_DZ), np.float32)
+    r = torch.as_tensor(rows).to(rs.device)
+    k = torch.arange(MAX_DZ, device=rs.device)
+    off = rs.t["frm_off"].index_select(0, r)[:, None] + k
+    ok = k[None] < rs.t["Dz"].index_select(0, r)[:, None]
+    F = torch.where(ok, p1.t["fz"][torch.where(ok, off, 0)], torch.zeros((), device=rs.device))
+    return F.cpu().numpy().astype(np.float64)
 
 
 def _adapt_rows(h1, plan, rows):
