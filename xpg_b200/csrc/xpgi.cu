@@ -278,11 +278,13 @@ __device__ void stage_wait(bool tma, unsigned long long* bar, float* stage, cons
 // ==================================================================================================================
 // pass 1
 // ==================================================================================================================
-constexpr int kClipCand = 2048;     // background voxels above the lowest clip threshold kept per CTA
+constexpr int kClipCand = 1024;     // background voxels above the lowest clip threshold kept per CTA
+constexpr int kFgList = 2048;       // foreground pixels listed per CTA (pass C iterates them densely)
+constexpr int kZBatch = 8;          // voxels of a pixel column loaded together (memory-level parallelism)
 
-// Dynamic shared memory: nblo (8P) | geometry scratch e1s/e2s (8P), then brefs (4P) + nbhi (4P) | flags (P, padded
-// to 16) | staged shoebox (4V, when STAGED).
-__host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)17 * P + 15) / 16 * 16; }
+// Dynamic shared memory: nblo (8P) | geometry scratch e1s/e2s (8P), then brefs (4P) + nbhi (4P) | flags (P) |
+// img2 counts (P, padded to 16) | staged shoebox (4V, when STAGED).
+__host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * P + 15) / 16 * 16; }
 
 template <int NT, bool STAGED>
 __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
@@ -304,6 +306,9 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
     __shared__ float cand_v[kClipCand];
     __shared__ unsigned short cand_p[kClipCand];
     __shared__ int s_ncand;
+    __shared__ unsigned short fgl[kFgList];
+    __shared__ int s_nfgl;
+    __shared__ int wcnt[NT / 32];
     __shared__ double s_base[2];
 
     const int row = order ? order[blockIdx.x] : blockIdx.x;
@@ -320,6 +325,7 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
     float* brefs = e1s;                            // reuses the geometry scratch once u1 / u2 are out
     unsigned* nbhi = reinterpret_cast<unsigned*>(e1s + Pm);
     unsigned char* flags = dyn1 + (size_t)16 * Pm;
+    unsigned char* imgn = dyn1 + (size_t)17 * Pm;   // per pixel: clean foreground-frame voxels | all-clean bit 7
     float* stage = reinterpret_cast<float*>(dyn1 + pass1_pix_bytes(Pm));
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
@@ -369,13 +375,36 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
         float S[3] = {s_S[0], s_S[1], s_S[2]};
         box_geometry(det, S, e1, e2, bx, xs, ys, B.sd, e1s, e2s, O.J + po, nullptr, &s_seff);
     }
-    // u1 / u2 out, foreground / background-ring flags per pixel
-    for (int p = threadIdx.x; p < P; p += NT) {
-        const float u1 = e1s[p], u2 = e2s[p];
-        O.u1[po + p] = u1;
-        O.u2[po + p] = u2;
-        const float r2 = u1 * u1 + u2 * u2;
-        flags[p] = (r2 <= kFgR2 ? 1 : 0) | (r2 >= kBgR2 ? 2 : 0);
+    // u1 / u2 out, foreground / background-ring flags per pixel, and the foreground pixels listed in pixel order
+    // (a block-wide ballot scan: the list, and so every later sum over it, is the same on every run)
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        int base = 0;
+        for (int q0 = 0; q0 < P; q0 += NT) {
+            const int p = q0 + threadIdx.x;
+            bool f = false;
+            if (p < P) {
+                const float u1 = e1s[p], u2 = e2s[p];
+                O.u1[po + p] = u1;
+                O.u2[po + p] = u2;
+                const float r2 = u1 * u1 + u2 * u2;
+                f = r2 <= kFgR2;
+                flags[p] = (f ? 1 : 0) | (r2 >= kBgR2 ? 2 : 0);
+            }
+            const unsigned ball = __ballot_sync(0xffffffffu, f);
+            if (lane == 0) wcnt[wid] = __popc(ball);
+            __syncthreads();
+            int off = base, all = 0;
+            for (int w = 0; w < NT / 32; ++w) {
+                off += w < wid ? wcnt[w] : 0;
+                all += wcnt[w];
+            }
+            const int k = off + __popc(ball & ((1u << lane) - 1u));
+            if (f && k < kFgList) fgl[k] = (unsigned short)p;
+            base += all;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) s_nfgl = base;
     }
     // foreground frames: R >= 1e-3 * Rmax + 1e-6
     if (threadIdx.x == 0) {
@@ -396,62 +425,108 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
     fgz.hi = s_fgz_hi;
     const float seff = s_seff;
 
-    // ---- pass A: first background estimate, counts, recorded frames ------------------------------------------
+    // ---- pass A: first background estimate, counts, recorded frames, the b-independent part of img2 --------
     // The clip threshold (bp + 3 sqrt(gain max(bp, 0.5))) + 1 is non-decreasing in bp = b * bref >= 0 (every
     // float operation in it is monotone), so it never falls below its value at bp = 0: background voxels at or
     // below that bound pass every iteration. They are summed here once; the others are listed for the iterations.
+    // A pixel column's background counts are summed in float32 (exact for detector counts: integers whose column
+    // sum stays below 2^24; a larger column is summed again in float64) and its template weight as count * bref,
+    // so the float64 totals equal voxel-by-voxel float64 sums.
     if (STAGED) stage_wait(tma, &s_bar, stage, sb, Dz * P, status);
     const float clip_floor = (0.0f + 3.0f * sqrtf(gain * fmaxf(0.0f, 0.5f))) + 1.0f;
     if (threadIdx.x == 0) s_ncand = 0;
     int neg_bref = 0;
     for (int p = threadIdx.x; p < P; p += NT) neg_bref |= (brefs[p] < 0.0f);
     const bool use_list = !__syncthreads_or(neg_bref);
+    const unsigned fgw[3] = {(unsigned)fgz.lo, (unsigned)(fgz.lo >> 32), fgz.hi};
     long long n_over = 0, n_fg_masked = 0, n_fg_nb = 0;
     {
-        Mask65 rec;
-        rec.clear();
+        unsigned recw[3] = {0u, 0u, 0u};
+        int t_over = 0, t_fgm = 0, t_fgnb = 0;
         double sc = 0.0, sb_ = 0.0, sc0 = 0.0, sb0 = 0.0;
         for (int p = threadIdx.x; p < P; p += NT) {
             const unsigned char fl = flags[p];
             const bool fg2 = fl & 1, ring = fl & 2;
             const float bref = brefs[p];
-            Mask65 nbm;
-            nbm.lo = nblo[p];
-            nbm.hi = nbhi[p];
-            for (int z = 0; z < Dz; ++z) {
-                float v;
-                if (STAGED) {
-                    v = stage[(size_t)z * P + p] - R.sb_bias;
-                    stage[(size_t)z * P + p] = v;
-                } else {
-                    v = sb[(size_t)z * P + p] - R.sb_bias;
-                }
-                const bool valid = v >= 0.0f, recd = v > -2.5f, over = v == -2.0f;
-                const bool fg = fg2 && fgz.get(z);
-                const bool nbz = nbm.get(z);
-                if (recd) rec.set(z);
-                n_over += (over && fg);
-                n_fg_masked += (fg && !valid && recd);
-                n_fg_nb += (fg && nbz);
-                if (valid && !fg && !nbz && ring) {
-                    sc += (double)v;
-                    sb_ += (double)bref;
-                    if (v <= clip_floor) {
-                        sc0 += (double)v;
-                        sb0 += (double)bref;
-                    } else if (use_list) {
-                        const int k = atomicAdd(&s_ncand, 1);
-                        if (k < kClipCand) {
-                            cand_v[k] = v;
-                            cand_p[k] = (unsigned short)p;
+            const unsigned long long nl = nblo[p];
+            const unsigned nbw[3] = {(unsigned)nl, (unsigned)(nl >> 32), nbhi[p]};
+            float cs = 0.0f, cs0 = 0.0f, ic = 0.0f;
+            int cn = 0, cn0 = 0, in_ = 0;
+            bool okall = true;
+#pragma unroll
+            for (int w = 0; w < 3; ++w) {
+                if (32 * w >= Dz) break;
+                const int zn = min(32, Dz - 32 * w);
+                const unsigned fw = fgw[w], nw = nbw[w];
+                const unsigned fgm = fg2 ? fw : 0u;       // foreground voxels of this column
+                unsigned rw = 0u;
+                const float* col = (STAGED ? stage : sb) + (size_t)32 * w * P + p;
+                for (int t0 = 0; t0 < zn; t0 += kZBatch) {
+                  float vv[kZBatch];                     // independent loads in flight before any is used
+#pragma unroll
+                  for (int u = 0; u < kZBatch; ++u) vv[u] = t0 + u < zn ? col[(size_t)(t0 + u) * P] : 0.0f;
+#pragma unroll
+                  for (int u = 0; u < kZBatch; ++u) {
+                    const int t = t0 + u;
+                    if (t >= zn) break;
+                    const float v = vv[u] - R.sb_bias;
+                    if (STAGED) stage[(size_t)(32 * w + t) * P + p] = v;
+                    const bool valid = v >= 0.0f, recd = v > -2.5f;
+                    const bool fgzz = (fw >> t) & 1u, nbz = (nw >> t) & 1u, fg = (fgm >> t) & 1u;
+                    const bool clean = valid && !nbz;
+                    rw |= (unsigned)recd << t;
+                    if (fg) {
+                        t_over += (v == -2.0f);
+                        t_fgm += (!valid && recd);
+                        t_fgnb += nbz;
+                    }
+                    if (fgzz) {
+                        if (clean) {
+                            ic += v;
+                            ++in_;
+                        } else {
+                            okall = false;
                         }
                     }
+                    if (clean && ring) {                 // background (the ring excludes the foreground ellipse)
+                        if (v <= clip_floor) {
+                            cs0 += v;
+                            ++cn0;
+                        } else {
+                            cs += v;
+                            ++cn;
+                            if (use_list) {
+                                const int k = atomicAdd(&s_ncand, 1);
+                                if (k < kClipCand) {
+                                    cand_v[k] = v;
+                                    cand_p[k] = (unsigned short)p;
+                                }
+                            }
+                        }
+                    }
+                  }
+                }
+                recw[w] |= rw;
+            }
+            double csd = (double)cs;
+            if (cs >= 16777216.0f) {                     // float32 may have rounded: this column again in float64
+                csd = 0.0;
+                for (int z = 0; z < Dz; ++z) {
+                    const float v = voxel(z, p);
+                    const bool nbz = z < 64 ? ((nl >> z) & 1ull) : (nbw[2] & 1u);
+                    if (ring && v >= 0.0f && !nbz && v > clip_floor) csd += (double)v;
                 }
             }
+            sc += csd + (double)cs0;
+            sb_ += (double)(cn + cn0) * (double)bref;
+            sc0 += (double)cs0;
+            sb0 += (double)cn0 * (double)bref;
+            O.img2[po + p] = ic;                         // completed with the background after pass B
+            imgn[p] = (unsigned char)(in_ | (okall ? 0x80 : 0));
         }
-        double a7[7] = {sc, sb_, (double)n_over, (double)n_fg_masked, (double)n_fg_nb, sc0, sb0};
-        atomicOr(&s_rec_lo, rec.lo);
-        atomicOr(&s_rec_hi, rec.hi);
+        double a7[7] = {sc, sb_, (double)t_over, (double)t_fgm, (double)t_fgnb, sc0, sb0};
+        atomicOr(&s_rec_lo, (unsigned long long)recw[0] | ((unsigned long long)recw[1] << 32));
+        atomicOr(&s_rec_hi, recw[2]);
         block_sum<NT, 7>(a7, red, tot);
         if (threadIdx.x == 0) {
             s_b = (float)tot[0] / fmaxf((float)tot[1], 1e-6f);
@@ -511,9 +586,16 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
         __syncthreads();
     }
     const float b = s_b;
-    // ---- pass C: summation, centroid, moments, projected spot, per-frame net ---------------------------------
-    // Sums over a pixel column's foreground voxels are taken in float32 (<= 65 terms), then weighted by the
-    // pixel's constants (x, y, eps, template) and added in float64.
+    // ---- pass C: summation, centroid, moments, per-frame net over the listed foreground pixels; img2 ---------
+    // img2 is linear in the background: each pixel's clean foreground-frame count sum (pass A) minus its count of
+    // such voxels times b * bref. The foreground sums run over the pixel list (every lane a foreground pixel);
+    // a column's sums are taken in float32 (<= 65 terms), then weighted by the pixel's constants and added in
+    // float64.
+    for (int p = threadIdx.x; p < P; p += NT) {
+        const unsigned char m = imgn[p];
+        O.img2[po + p] = O.img2[po + p] - (float)(m & 0x7f) * (b * brefs[p]);
+        O.all_valid2[po + p] = m >> 7;
+    }
     double acc[15];
 #pragma unroll
     for (int q = 0; q < 15; ++q) acc[q] = 0.0;
@@ -521,90 +603,94 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
         for (int w = 0; w < NT / 32; ++w) fzw[w][z] = 0.0f;
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int n_iter = (P + NT - 1) / NT;
+    const int nfl = s_nfgl;
+    const bool fl_listed = nfl <= kFgList;
+    const int n_items = fl_listed ? nfl : P;
+    const int n_iter = (n_items + NT - 1) / NT;
     for (int q = 0; q < n_iter; ++q) {
-        const int p = threadIdx.x + q * NT;
-        const bool have = p < P;
-        const int i = have ? p % bx : 0, j = have ? p / bx : 0;
+        const int k = threadIdx.x + q * NT;
+        int p = 0;
+        bool have = false;
+        if (k < n_items) {
+            p = fl_listed ? (int)fgl[k] : k;
+            have = fl_listed || (flags[p] & 1);
+        }
+        if (!__any_sync(0xffffffffu, have)) continue;      // warp-uniform: no foreground pixel in this warp
+        const int i = p % bx, j = p / bx;
         float u1 = 0.f, u2 = 0.f, bref = 1.f;
-        bool fg2 = false;
-        Mask65 nbm;
-        nbm.clear();
+        unsigned nbw[3] = {0u, 0u, 0u};
         if (have) {
             u1 = O.u1[po + p];
             u2 = O.u2[po + p];
             bref = brefs[p];
-            fg2 = flags[p] & 1;
-            nbm.lo = nblo[p];
-            nbm.hi = nbhi[p];
+            const unsigned long long nl = nblo[p];
+            nbw[0] = (unsigned)nl;
+            nbw[1] = (unsigned)(nl >> 32);
+            nbw[2] = nbhi[p];
         }
         const float bpix = b * bref;
-        const bool warp_fg = __any_sync(0xffffffffu, fg2);
-        float c_n = 0.f, c_net = 0.f, c_c = 0.f, c_w = 0.f, c_wz = 0.f, c_e3 = 0.f, c_e33 = 0.f, c_img = 0.f;
-        bool okall = true;
-        unsigned long long fm = fgz.lo, nm = nbm.lo;
-        for (int z = 0; z < Dz; ++z) {
-            if (z == 64) {
-                fm = fgz.hi;
-                nm = nbm.hi;
-            }
-            const bool fgzz = fm & 1ull, nbz = nm & 1ull;
-            fm >>= 1;
-            nm >>= 1;
-            float fzc = 0.0f;
-            if (have) {
-                const float v = voxel(z, p);
-                const bool valid = v >= 0.0f;
-                const float c = valid ? v : 0.0f;
-                const bool clean = valid && !nbz;
-                const float net = c - bpix;
-                if (fg2 && clean) {
-                    fzc = net;
-                    if (fgzz) {                         // fgv: foreground, valid, not a neighbour's
-                        c_n += 1.0f;
-                        c_net += net;
-                        c_c += c;
-                        const float wpos = fmaxf(net, 0.0f);
-                        c_w += wpos;
-                        c_wz += wpos * fzz[z];
-                        const float e3 = fe3[z];
-                        c_e3 += net * e3;
-                        c_e33 += net * (e3 * e3);
+        float c_n = 0.f, c_net = 0.f, c_c = 0.f, c_w = 0.f, c_wz = 0.f, c_e3 = 0.f, c_e33 = 0.f;
+#pragma unroll
+        for (int w = 0; w < 3; ++w) {
+            if (32 * w >= Dz) break;
+            const int zn = min(32, Dz - 32 * w);
+            const unsigned fw = fgw[w], nw = nbw[w];
+            const float* col = (STAGED ? stage : sb) + (size_t)32 * w * P + p;
+            for (int t0 = 0; t0 < zn; t0 += kZBatch) {
+              float vv[kZBatch];
+#pragma unroll
+              for (int u = 0; u < kZBatch; ++u) vv[u] = have && t0 + u < zn ? col[(size_t)(t0 + u) * P] : 0.0f;
+#pragma unroll
+              for (int u = 0; u < kZBatch; ++u) {
+                const int t = t0 + u;
+                if (t >= zn) break;
+                const int z = 32 * w + t;
+                float fzc = 0.0f;
+                if (have) {
+                    const float v = STAGED ? vv[u] : vv[u] - R.sb_bias;
+                    const bool valid = v >= 0.0f;
+                    const float c = valid ? v : 0.0f;
+                    const bool clean = valid && !((nw >> t) & 1u);
+                    const float net = c - bpix;
+                    if (clean) {
+                        fzc = net;
+                        if ((fw >> t) & 1u) {                // fgv: foreground, valid, not a neighbour's
+                            c_n += 1.0f;
+                            c_net += net;
+                            c_c += c;
+                            const float wpos = fmaxf(net, 0.0f);
+                            c_w += wpos;
+                            c_wz += wpos * fzz[z];
+                            const float e3 = fe3[z];
+                            c_e3 += net * e3;
+                            c_e33 += net * (e3 * e3);
+                        }
                     }
                 }
-                if (fgzz) {
-                    if (clean) c_img += net;
-                    else okall = false;
-                }
-            }
-            if (warp_fg) {
                 fzc = warp_sumf(fzc);
                 if (lane == 0) fzw[wid][z] += fzc;
+              }
             }
         }
-        if (have) {
-            O.img2[po + p] = c_img;
-            O.all_valid2[po + p] = okall ? 1 : 0;
-            if (c_n > 0.0f) {
-                const float x = xs[i], y = ys[j];
-                const float eps1 = u1 * seff, eps2 = u2 * seff;
-                const float e12 = eps1 * eps1 + eps2 * eps2;
-                acc[14] += (double)c_n;
-                acc[0] += (double)c_n * (double)bref;             // sfb
-                acc[1] += (double)c_net;                          // isum
-                acc[2] += (double)c_c;                            // vsum counts
-                acc[3] += (double)c_n * (double)bpix;             // vsum0
-                acc[4] += (double)c_w;                            // sw
-                acc[5] += (double)c_w * (double)x;
-                acc[6] += (double)c_w * (double)y;
-                acc[7] += (double)c_wz;
-                acc[8] += (double)c_net;                          // sws
-                acc[9] += (double)c_net * (double)eps1;
-                acc[10] += (double)c_net * (double)eps2;
-                acc[11] += (double)c_net * (double)e12;
-                acc[12] += (double)c_e3;
-                acc[13] += (double)c_e33;
-            }
+        if (have && c_n > 0.0f) {
+            const float x = xs[i], y = ys[j];
+            const float eps1 = u1 * seff, eps2 = u2 * seff;
+            const float e12 = eps1 * eps1 + eps2 * eps2;
+            acc[14] += (double)c_n;
+            acc[0] += (double)c_n * (double)bref;             // sfb
+            acc[1] += (double)c_net;                          // isum
+            acc[2] += (double)c_c;                            // vsum counts
+            acc[3] += (double)c_n * (double)bpix;             // vsum0
+            acc[4] += (double)c_w;                            // sw
+            acc[5] += (double)c_w * (double)x;
+            acc[6] += (double)c_w * (double)y;
+            acc[7] += (double)c_wz;
+            acc[8] += (double)c_net;                          // sws
+            acc[9] += (double)c_net * (double)eps1;
+            acc[10] += (double)c_net * (double)eps2;
+            acc[11] += (double)c_net * (double)e12;
+            acc[12] += (double)c_e3;
+            acc[13] += (double)c_e33;
         }
     }
     block_sum<NT, 15>(acc, red, tot);
@@ -807,6 +893,21 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBloc
     if (threadIdx.x == 0) s_nlist = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    // frame sums of the rocking curve: a pixel's profile total is P2 * sum_z R (all frames) and its foreground
+    // share P2 * sum_{z in fgz} R, both taken per pixel in float64; p_valid subtracts the frames a pixel loses
+    // (masked voxels, neighbours), summed per column
+    __shared__ double s_rsum[2];
+    if (threadIdx.x == 0) {
+        double ra = 0.0, rf = 0.0;
+        for (int z = 0; z < Dz; ++z) {
+            ra += (double)fR[z];
+            if (fgz.get(z)) rf += (double)fR[z];
+        }
+        s_rsum[0] = ra;
+        s_rsum[1] = rf;
+    }
+    __syncthreads();
+    const double r_all = s_rsum[0], r_fg = s_rsum[1];
     {
         double a8[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // s_net, s_w, p_total, p_valid, p_fgn, a110, C0, nuse
         const int n_iter = (P + NT - 1) / NT;
@@ -815,60 +916,83 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBloc
             const bool have = p < P;
             float bref = 1.0f, P2 = 0.0f, P2p = 0.0f;
             bool fg2 = false;
-            Mask65 nbm;
-            nbm.clear();
+            unsigned nbw[3] = {0u, 0u, 0u};
             if (have) {
                 bref = brefs[p];
                 P2 = P2s[p];
                 P2p = P2ps[p];
                 const float u1 = I2.u1[po + p], u2 = I2.u2[po + p];
                 fg2 = (u1 * u1 + u2 * u2) <= kFgR2;
-                nbm.lo = nblo[p];
-                nbm.hi = nbhi[p];
+                const unsigned long long nl = nblo[p];
+                nbw[0] = (unsigned)nl;
+                nbw[1] = (unsigned)(nl >> 32);
+                nbw[2] = nbhi[p];
             }
             const float bpix = bg * bref;
             const float iv0 = __frcp_rn(gain * fmaxf(bpix, kVarFloor));
-            Mask65 um;                           // frames of this pixel that enter the fit
-            um.clear();
-            for (int z = 0; z < Dz; ++z) {
-                bool use = false;
-                float net = 0.0f;
-                if (have) {
-                    const float v = (STAGED ? stage[(size_t)z * P + p] : sb[(size_t)z * P + p]) - R.sb_bias;
-                    const float pv = P2 * fR[z];
-                    const float ppv = (P2p * fRp[z]) * hp;
-                    const bool valid = v >= 0.0f, nbz = nbm.get(z);
-                    a8[2] += (double)pv;
-                    if (valid && !nbz) a8[3] += (double)pv;
-                    if (fg2 && fgz.get(z)) a8[4] += (double)pv;
-                    use = valid && !nbz && (pv > pthr || ppv > ppthr);
-                    net = v - bpix;
-                    if (STAGED) stage[(size_t)z * P + p] = use ? net : __int_as_float(0x7fc00000);
-                    if (use) {
-                        um.set(z);
-                        a8[0] += (double)net;
-                        a8[1] += (double)(pv + ppv);
-                        a8[5] += (double)((pv * pv) * iv0);
-                        a8[6] += (double)((pv * bref) * iv0);
-                        a8[7] += 1.0;
+            unsigned umw[3] = {0u, 0u, 0u};      // frames of this pixel that enter the fit
+            float lost = 0.0f;                   // rocking-curve weight of the frames this pixel loses
+#pragma unroll
+            for (int w = 0; w < 3; ++w) {
+                if (32 * w >= Dz) break;
+                const int zn = min(32, Dz - 32 * w);
+                const unsigned nw = nbw[w];
+                const float* col = (STAGED ? stage : sb) + (size_t)32 * w * P + p;
+                unsigned uw = 0u;
+                for (int t0 = 0; t0 < zn; t0 += kZBatch) {
+                  float vv[kZBatch];
+#pragma unroll
+                  for (int u = 0; u < kZBatch; ++u) vv[u] = have && t0 + u < zn ? col[(size_t)(t0 + u) * P] : 0.0f;
+#pragma unroll
+                  for (int u = 0; u < kZBatch; ++u) {
+                    const int t = t0 + u;
+                    if (t >= zn) break;
+                    const int z = 32 * w + t;
+                    bool use = false;
+                    float net = 0.0f;
+                    if (have) {
+                        const float v = vv[u] - R.sb_bias;
+                        const float pv = P2 * fR[z];
+                        const float ppv = (P2p * fRp[z]) * hp;
+                        const bool clean = v >= 0.0f && !((nw >> t) & 1u);
+                        if (!clean) lost += fR[z];
+                        use = clean && (pv > pthr || ppv > ppthr);
+                        net = v - bpix;
+                        if (STAGED) stage[(size_t)z * P + p] = use ? net : __int_as_float(0x7fc00000);
+                        if (use) {
+                            uw |= 1u << t;
+                            a8[0] += (double)net;
+                            a8[1] += (double)(pv + ppv);
+                            a8[5] += (double)((pv * pv) * iv0);
+                            a8[6] += (double)((pv * bref) * iv0);
+                            a8[7] += 1.0;
+                        }
                     }
-                }
-                // warp-aggregated append to the fit list
-                const unsigned ball = __ballot_sync(0xffffffffu, use);
-                if (ball) {
-                    int base = 0;
-                    if (lane == 0) base = atomicAdd(&s_nlist, __popc(ball));
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    const int k = base + __popc(ball & ((1u << lane) - 1u));
-                    if (use && k < cap) {
-                        ul_v[k] = net;
-                        ul_i[k] = ((unsigned)z << 16) | (unsigned)p;
+                    // warp-aggregated append to the fit list
+                    const unsigned ball = __ballot_sync(0xffffffffu, use);
+                    if (ball) {
+                        int base = 0;
+                        if (lane == 0) base = atomicAdd(&s_nlist, __popc(ball));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        const int k = base + __popc(ball & ((1u << lane) - 1u));
+                        if (use && k < cap) {
+                            ul_v[k] = net;
+                            ul_i[k] = ((unsigned)z << 16) | (unsigned)p;
+                        }
                     }
+                  }
                 }
+                umw[w] = uw;
             }
-            if (have && STAGED) {                // the neighbour mask is not needed any more: keep the fit mask
-                nblo[p] = um.lo;
-                nbhi[p] = um.hi;
+            if (have) {
+                const double tp = (double)P2 * r_all;
+                a8[2] += tp;
+                a8[3] += tp - (double)P2 * (double)lost;
+                if (fg2) a8[4] += (double)P2 * r_fg;
+                if (STAGED) {                    // the neighbour mask is not needed any more: keep the fit mask
+                    nblo[p] = (unsigned long long)umw[0] | ((unsigned long long)umw[1] << 32);
+                    nbhi[p] = umw[2];
+                }
             }
         }
         block_sum<NT, 8>(a8, red, tot);
