@@ -40,15 +40,36 @@ struct NbShared {
     int nact;
     int act[XI_MAX_K];
     int zmin[XI_MAX_K];             // frame of the smallest dz^2 of each active neighbour
-    float dx2[XI_MAX_K][XI_MAX_BX];
-    float dy2[XI_MAX_K][XI_MAX_BX];
-    float dz2[XI_MAX_K][XI_MAX_DZ];
 };
+
+// The per-axis terms of the active neighbours, in dynamic shared memory sized for the launch's neighbour columns
+// and largest box: dx2 / dy2 (K x max_bx), dz2 (K x max_dz).
+struct NbTab {
+    float *dx2, *dy2, *dz2;
+    int sxy, sz;
+    __device__ __forceinline__ float& x2(int a, int i) const { return dx2[a * sxy + i]; }
+    __device__ __forceinline__ float& y2(int a, int j) const { return dy2[a * sxy + j]; }
+    __device__ __forceinline__ float* z2(int a) const { return dz2 + a * sz; }
+};
+
+__host__ __device__ inline size_t nb_bytes(int K, int max_bx, int max_dz) {
+    return ((size_t)K * (2 * max_bx + max_dz) * sizeof(float) + 15) / 16 * 16;
+}
+
+__device__ __forceinline__ NbTab nb_tab(unsigned char* base, int K, int max_bx, int max_dz) {
+    NbTab t;
+    t.dx2 = reinterpret_cast<float*>(base);
+    t.dy2 = t.dx2 + (size_t)K * max_bx;
+    t.dz2 = t.dy2 + (size_t)K * max_bx;
+    t.sxy = max_bx;
+    t.sz = max_dz;
+    return t;
+}
 
 // Neighbour columns whose ellipsoid reaches the box (the separable pre-test of xpg/integrate_kernels.py:192-203;
 // skipping the others is exact) and their per-axis terms.
 __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const float* xs, const float* ys,
-                                const float* zzs, bool skip_first, NbShared& nb) {
+                                const float* zzs, bool skip_first, NbShared& nb, const NbTab& tb) {
     const int K = R.K;
     if (threadIdx.x == 0) {
         int n = 0;
@@ -73,19 +94,19 @@ __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const 
         for (int i = threadIdx.x; i < bx; i += blockDim.x) {
             float dx = (xs[i] - nx_) / sx;
             float dy = (ys[i] - ny_) / sx;
-            nb.dx2[a][i] = dx * dx;
-            nb.dy2[a][i] = dy * dy;
+            tb.x2(a, i) = dx * dx;
+            tb.y2(a, i) = dy * dy;
         }
         for (int z = threadIdx.x; z < Dz; z += blockDim.x) {
             float dz = (zzs[z] - nz_) / sz;
-            nb.dz2[a][z] = dz * dz;
+            tb.z2(a)[z] = dz * dz;
         }
     }
     __syncthreads();
     for (int a = threadIdx.x; a < nb.nact; a += blockDim.x) {
         int zm = 0;
         for (int z = 1; z < Dz; ++z)
-            if (nb.dz2[a][z] < nb.dz2[a][zm]) zm = z;
+            if (tb.z2(a)[z] < tb.z2(a)[zm]) zm = z;
         nb.zmin[a] = zm;
     }
     __syncthreads();
@@ -95,12 +116,12 @@ __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const 
 // is unimodal (the bin centres increase, float subtraction, division and squaring are monotone), so for a given
 // dx^2 + dy^2 the frames that pass form one interval around the minimum: found by two binary searches on the same
 // float comparisons as a full scan.
-__device__ __forceinline__ Mask65 neighbour_frames(const NbShared& nb, int i, int j, int Dz) {
+__device__ __forceinline__ Mask65 neighbour_frames(const NbShared& nb, const NbTab& tb, int i, int j, int Dz) {
     Mask65 m;
     m.clear();
     for (int a = 0; a < nb.nact; ++a) {
-        const float dxy = nb.dx2[a][i] + nb.dy2[a][j];
-        const float* d2 = nb.dz2[a];
+        const float dxy = tb.x2(a, i) + tb.y2(a, j);
+        const float* d2 = tb.z2(a);
         const int zm = nb.zmin[a];
         if (!(dxy + d2[zm] < 1.0f)) continue;
         int lo = 0, hi = zm;                 // first z in [0, zm] that passes
@@ -214,12 +235,12 @@ __device__ void rocking_curve_cta(int Dz, int iz0, float fb, const XiBlock& B, c
 }
 
 // Per-pixel neighbour frame masks and background template of a box, computed once (shared memory).
-__device__ void pixel_tables(const XiDetector& det, const NbShared& nb, int bx, int Dz, const float* xs,
+__device__ void pixel_tables(const XiDetector& det, const NbShared& nb, const NbTab& tb, int bx, int Dz, const float* xs,
                              const float* ys, unsigned long long* nblo, unsigned* nbhi, float* brefs) {
     const int P = bx * bx;
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const int i = p % bx, j = p / bx;
-        const Mask65 m = neighbour_frames(nb, i, j, Dz);
+        const Mask65 m = neighbour_frames(nb, tb, i, j, Dz);
         nblo[p] = m.lo;
         nbhi[p] = m.hi;
         brefs[p] = bkg_ref(det, xs[i], ys[j]);
@@ -286,15 +307,23 @@ constexpr int kZBatch = 8;          // voxels of a pixel column loaded together 
 // img2 counts (P, padded to 16) | staged shoebox (4V, when STAGED).
 __host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * P + 15) / 16 * 16; }
 
+// resident CTAs per SM the pass kernels are compiled for (registers per thread <= 65536 / (NT * blocks))
+template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 4 : 8); }
+
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
                                               XiPass1Out O, const int32_t* __restrict__ order, int max_bx,
                                               int max_dz, int* status) {
     extern __shared__ __align__(16) unsigned char dyn1[];
     __shared__ CtaTables T;
     __shared__ float xs[XI_MAX_BX], ys[XI_MAX_BX];
     __shared__ float fR[XI_MAX_DZ], fzz[XI_MAX_DZ], fe3[XI_MAX_DZ];
-    __shared__ float terms[XI_MAX_DZ * XI_RC_K];
+    // the rocking-curve terms (set-up) and the clip-candidate list (passes A and B) share one array
+    constexpr int kScratch = kClipCand * 6 > XI_MAX_DZ * XI_RC_K * 4 ? kClipCand * 6 : XI_MAX_DZ * XI_RC_K * 4;
+    __shared__ __align__(16) unsigned char scr[kScratch];
+    float* terms = reinterpret_cast<float*>(scr);
+    float* cand_v = reinterpret_cast<float*>(scr);
+    unsigned short* cand_p = reinterpret_cast<unsigned short*>(scr + 4 * kClipCand);
     __shared__ NbShared nb;
     __shared__ float s_e1[3], s_e2[3], s_S[3], s_zeta, s_seff, s_b;
     __shared__ unsigned long long s_fgz_lo, s_rec_lo;
@@ -302,9 +331,8 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
     __shared__ double red[NT / 32 * 16];
     __shared__ double tot[16];
     __shared__ float fzw[NT / 32][XI_MAX_DZ];
-    // background voxels above the lowest possible clip threshold (the only ones the iterations can drop)
-    __shared__ float cand_v[kClipCand];
-    __shared__ unsigned short cand_p[kClipCand];
+    // background voxels above the lowest possible clip threshold (the only ones the iterations can drop): cand_v,
+    // cand_p above
     __shared__ int s_ncand;
     __shared__ unsigned short fgl[kFgList];
     __shared__ int s_nfgl;
@@ -327,6 +355,8 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
     unsigned char* flags = dyn1 + (size_t)16 * Pm;
     unsigned char* imgn = dyn1 + (size_t)17 * Pm;   // per pixel: clean foreground-frame voxels | all-clean bit 7
     float* stage = reinterpret_cast<float*>(dyn1 + pass1_pix_bytes(Pm));
+    const NbTab tb = nb_tab(dyn1 + pass1_pix_bytes(Pm) + (STAGED ? ((size_t)Pm * max_dz * 4 + 15) / 16 * 16 : 0), R.K,
+                            max_bx, max_dz);
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
     const float fb = R.fb[row];
@@ -418,8 +448,8 @@ __global__ void __launch_bounds__(NT) k_pass1(XiDetector det_g, XiRows R, XiBloc
         s_fgz_lo = m.lo;
         s_fgz_hi = m.hi;
     }
-    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, false, nb);     // ends with a barrier
-    pixel_tables(det, nb, bx, Dz, xs, ys, nblo, nbhi, brefs);
+    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, false, nb, tb);     // ends with a barrier
+    pixel_tables(det, nb, tb, bx, Dz, xs, ys, nblo, nbhi, brefs);
     Mask65 fgz;
     fgz.lo = s_fgz_lo;
     fgz.hi = s_fgz_hi;
@@ -748,7 +778,7 @@ __host__ __device__ inline size_t pass2_stage_offset(int P, int cap) {
 }
 
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
                                               const float* __restrict__ prof, XiPass2In I2, XiPass2Out O,
                                               const int32_t* __restrict__ order, int max_bx, int max_dz, int cap,
                                               int* status) {
@@ -787,6 +817,8 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBloc
     float* ul_v = reinterpret_cast<float*>(dyn2 + pass2_pix_bytes(Pm));      // fit list: net counts
     unsigned* ul_i = reinterpret_cast<unsigned*>(ul_v + cap);                 // fit list: z << 16 | pixel
     float* stage = reinterpret_cast<float*>(dyn2 + pass2_stage_offset(Pm, cap));   // 16-byte aligned
+    const NbTab tb = nb_tab(dyn2 + pass2_stage_offset(Pm, cap) + (STAGED ? ((size_t)Pm * max_dz * 4 + 15) / 16 * 16 : 0),
+                            R.K, max_bx, max_dz);
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
     const float fb = R.fb[row];
@@ -878,8 +910,8 @@ __global__ void __launch_bounds__(NT) k_pass2(XiDetector det_g, XiRows R, XiBloc
         }
         __syncthreads();
     }
-    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, has_p, nb);     // ends with a barrier (partner scratch free)
-    pixel_tables(det, nb, bx, Dz, xs, ys, nblo, nbhi, brefs);
+    neighbour_setup(R, row, Dz, bx, xs, ys, fzz, has_p, nb, tb);     // ends with a barrier (partner scratch free)
+    pixel_tables(det, nb, tb, bx, Dz, xs, ys, nblo, nbhi, brefs);
     const float pthr = 0.01f * s_pmax;
     const float ppthr = 0.01f * fmaxf(s_ppmax, 1e-12f);
 
@@ -1340,8 +1372,11 @@ template <int NT, bool STAGED>
 int launch_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, XiPass1Out* O,
                  cudaStream_t s, int nblk) {
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    size_t sm = pass1_pix_bytes((int)P) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0);
+    size_t sm = pass1_pix_bytes((int)P) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0) +
+                nb_bytes(R->K, R->max_bx, R->max_dz);
     cudaFuncSetAttribute(k_pass1<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_pass1<NT, STAGED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     k_pass1<NT, STAGED><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, *O, R->order, R->max_bx, R->max_dz,
                                               status_ptr());
     return cuda_check("xi_pass1");
@@ -1351,8 +1386,11 @@ template <int NT, bool STAGED>
 int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, const float* prof,
                  const XiPass2In* in, XiPass2Out* O, cudaStream_t s, int nblk, int cap) {
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    size_t sm = pass2_stage_offset((int)P, cap) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0);
+    size_t sm = pass2_stage_offset((int)P, cap) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0) +
+                nb_bytes(R->K, R->max_bx, R->max_dz);
     cudaFuncSetAttribute(k_pass2<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_pass2<NT, STAGED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     k_pass2<NT, STAGED><<<nblk, NT, sm, s>>>(*det, *R, *B, arena, prof, *in, *O, R->order, R->max_bx, R->max_dz,
                                               cap, status_ptr());
     return cuda_check("xi_pass2");

@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 from . import native as N
+from .device import TIMER
 from .geometry import centring_allowed, generate_hkl, unit
 
 N_FG = 3.0
@@ -215,8 +216,9 @@ def predict_device(exp_blocks, block_edges, dmin, dmax, z_lo, z_hi, minimum_zeta
             det_cache[key] = plan_detector(exp.geom, device)
         ws = torch.empty(max(int(lib.xi_predict_workspace(C.byref(P))), 1), dtype=torch.uint8, device=device)
         n = C.c_int64(0)
-        N.check(lib.xi_predict_count(C.byref(P), C.byref(det_cache[key][0]), N.ptr(ws), ws.numel(), C.byref(n), st),
-                "xi_predict_count")
+        with TIMER.span("plan", 2):             # k_predict_count, k_total (plus the library scan)
+            N.check(lib.xi_predict_count(C.byref(P), C.byref(det_cache[key][0]), N.ptr(ws), ws.numel(), C.byref(n),
+                                         st), "xi_predict_count")
         jobs.append((P, keep, key, ws, int(n.value)))
     total = sum(j[4] for j in jobs)
     cols = _columns(total, PRED_F64, torch.float64, device)
@@ -230,8 +232,9 @@ def predict_device(exp_blocks, block_edges, dmin, dmax, z_lo, z_hi, minimum_zeta
             out = N.XiPredictOut()
             for k, v in cols.items():
                 setattr(out, k, N.ptr(v[o:o + n]))
-            N.check(lib.xi_predict_write(C.byref(P), C.byref(det_cache[key][0]), N.ptr(ws), ws.numel(),
-                                         C.byref(out), n, st), "xi_predict_write")
+            with TIMER.span("plan"):
+                N.check(lib.xi_predict_write(C.byref(P), C.byref(det_cache[key][0]), N.ptr(ws), ws.numel(),
+                                             C.byref(out), n, st), "xi_predict_write")
         o += n
     return cols
 
@@ -281,7 +284,8 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
     O = N.XiBoxOut()
     for k, v in bcols.items():
         setattr(O, k, N.ptr(v))
-    N.check(lib.xi_plan_boxes(C.byref(B), C.byref(det0), C.byref(O), st), "xi_plan_boxes")
+    with TIMER.span("plan"):
+        N.check(lib.xi_plan_boxes(C.byref(B), C.byref(det0), C.byref(O), st), "xi_plan_boxes")
     flags = bcols.pop("flags")
     fl = flags.cpu().numpy()
     info = dict(n_predicted=n_pred, n_wide=int((fl & 1).sum()), n_trunc=int(((fl & 2) > 0).sum()), box=box)
@@ -305,7 +309,8 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
         q.hi[:] = [(g0.nx + 0.5) / sxm, (g0.ny + 0.5) / sxm, z_hi / szm]
         q.radius, q.k = 4.0 * N_FG, K
         ws = torch.empty(max(int(lib.xi_knn_workspace(C.byref(q))), 1), dtype=torch.uint8, device=device)
-        N.check(lib.xi_knn(C.byref(q), N.ptr(ws), ws.numel(), N.ptr(nbj), N.ptr(nbd), st), "xi_knn")
+        with TIMER.span("plan", 3):             # k_knn_bin, k_knn_scatter, k_knn_query (plus the library scan)
+            N.check(lib.xi_knn(C.byref(q), N.ptr(ws), ws.numel(), N.ptr(nbj), N.ptr(nbd), st), "xi_knn")
     has = torch.isfinite(nbd)
     jl = nbj.long()
     has_partner = (has[:, 0] & (nbd[:, 0] < 2.0)) if (deconvolve_overlaps and n) else torch.zeros(n, dtype=torch.bool,
