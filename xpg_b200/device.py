@@ -62,10 +62,20 @@ class _Span:
 TIMER = KernelTimer()
 
 
+def h2d(a, dtype=None, device="cuda"):
+    """Host array -> device tensor without blocking the host: staged through pinned memory (torch's caching host
+    allocator keeps the staging block until the copy has run), copied on the current stream. A pageable copy would
+    wait for every kernel queued before it."""
+    t = torch.as_tensor(np.ascontiguousarray(a), dtype=dtype)
+    if t.numel() == 0:
+        return t.to(device)
+    return t.pin_memory().to(device, non_blocking=True)
+
+
 def _dev(a, dtype, device):
     if torch.is_tensor(a):                  # already a tensor (the planner's device columns): convert in place
         return a.to(device=device, dtype=dtype).contiguous()
-    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(device, non_blocking=False)
+    return h2d(a, dtype, device)
 
 
 class DeviceDetector:
@@ -281,7 +291,7 @@ def status(stream=None):
 def _device_groups(rows: RowSet):
     cache = getattr(rows, "_groups", None)
     if cache is None:
-        cache = [(b, dz, torch.as_tensor(o).to(rows.device)) for b, dz, o in rows.groups()]
+        cache = [(b, dz, h2d(o, None, rows.device)) for b, dz, o in rows.groups()]
         rows._groups = cache
     return cache
 

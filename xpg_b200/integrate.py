@@ -59,7 +59,7 @@ class _Block:
         self.rows = rows                                  # global row indices, reference kernel-call order
         p = plan
         dv = p.dev                                        # the planner's device columns
-        rt = torch.as_tensor(rows).to(device)
+        rt = D.h2d(rows, None, device)
         sel = lambda t: t.index_select(0, rt)
         pj = dv["nbj"][:, 0].long().index_select(0, rt)   # nearest neighbour: the partner where there is one
         rad = lambda phi: (phi * (np.pi / 180.0)).float()  # numpy's radians, then float32
@@ -76,7 +76,7 @@ class _Block:
         self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
         order = np.argsort(rows, kind="stable")            # local rows by global row: outputs leave in plan order
-        self.perm_t = torch.as_tensor(order).to(device)
+        self.perm_t = D.h2d(order, None, device)
         self.rows_sorted = rows[order]
         srt = self.rows_sorted
         self.span = (int(srt[0]), int(srt[-1]) + 1) if srt.size and srt[-1] - srt[0] + 1 == srt.size else None
@@ -211,7 +211,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         ok = np.array([(g_ not in excl) for g_ in range(f, f_b + 1)], bool)
         if ok.any() and opened:
             data, is_f = src.wedge(f, f_b, ok)
-            ok_t = torch.as_tensor(ok.astype(np.uint8)).to(device) if not ok.all() else None
+            ok_t = D.h2d(ok.astype(np.uint8), None, device) if not ok.all() else None
             for b in open_order:
                 blk = opened.get(b)
                 if blk is None or eff_hi[b] < fi_a:
@@ -222,7 +222,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
                     continue
                 fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
                                      mask_t, ok_t[:nf] if ok_t is not None else None)
-                D.gather(fs, blk.grows, torch.as_tensor(loc).to(device), blk.arena, blk.cnt)
+                D.gather(fs, blk.grows, D.h2d(loc, None, device), blk.arena, blk.cnt)
         done = sorted((b for b in open_order if b in opened and eff_hi[b] <= fi_b),
                       key=lambda b: (eff_hi[b], open_order.index(b)))
         for b in done:
@@ -275,7 +275,7 @@ def _fz_padded(p1: D.Pass1Buffers, rs: D.RowSet, sel):
     rows = np.flatnonzero(sel)
     if rows.size == 0:
         return np.zeros((0, MAX_DZ), np.float32)
-    r = torch.as_tensor(rows).to(rs.device)
+    r = D.h2d(rows, None, rs.device)
     k = torch.arange(MAX_DZ, device=rs.device)
     off = rs.t["frm_off"].index_select(0, r)[:, None] + k
     ok = k[None] < rs.t["Dz"].index_select(0, r)[:, None]

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import native as N
-from .device import TIMER
+from .device import TIMER, h2d
 from .geometry import centring_allowed, generate_hkl, unit
 
 N_FG = 3.0
@@ -115,7 +115,7 @@ def plan_detector(g, device="cuda"):
         rec[k, 21], rec[k, 22], rec[k, 23] = P0[k] @ n, Bx[k] @ Bx[k], By[k] @ By[k]
         s = segs[min(k, len(segs) - 1)]
         rec[k, 24:28] = (s.x1, s.x2, s.y1, s.y2)
-    keep = {"panels": torch.as_tensor(rec).to(device)}
+    keep = {"panels": h2d(rec, None, device)}
     d = N.XiPlanDetector()
     d.n_panels = K
     d.panels = N.ptr(keep["panels"])
@@ -166,7 +166,7 @@ def _predict_struct(exp, g0, za, zb, dmin, dmax, z_lo, z_hi, minimum_zeta, block
     else:                                   # a caller's own absence rule: its Miller-index list, in order
         hkl = generate_hkl(A, dmin, dmax)
         hkl = np.ascontiguousarray(hkl[allowed(hkl, exp.crystal.space_group)], np.int32)
-        keep = torch.as_tensor(hkl).to(device)
+        keep = h2d(hkl, None, device)
         P.hkl, P.n_hkl = N.ptr(keep), int(hkl.shape[0])
     axis = np.asarray(g.axis, np.float64)
     k = unit(axis)
@@ -290,7 +290,7 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
     fl = flags.cpu().numpy()
     info = dict(n_predicted=n_pred, n_wide=int((fl & 1).sum()), n_trunc=int(((fl & 2) > 0).sum()), box=box)
     if not (fl & 4).all():                  # rows without a depth bucket leave the plan
-        keep_t = torch.as_tensor((fl & 4) > 0).to(device)
+        keep_t = h2d((fl & 4) > 0, None, device)
         pred, bcols = _select(pred, keep_t), _select(bcols, keep_t)
     n = int(pred["x"].shape[0])
     # neighbour lists on the mean scales (`xpg/integrate.py:164-172`, `:287-303`)
