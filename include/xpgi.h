@@ -297,6 +297,30 @@ typedef struct {
 size_t xi_knn_workspace(const XiKnn *q);
 int xi_knn(const XiKnn *q, void *ws, size_t ws_bytes, int32_t *nbj, double *nbd, void *stream);
 
+/* ---- Adaptation of the rocking curve (float64) -----------------------------------------------------------------
+ * The per-block adaptation XPG runs in numpy on the host (xpg/integrate.py:404-461 with the grid search of
+ * :1130-1154), on the block's strong reflections: their per-frame net counts fz (zero beyond each box's depth). */
+typedef struct {
+    int64_t n;                      /* strong reflections */
+    const double *fz;               /* (n, 65) per-frame net counts */
+    const int32_t *iz0;             /* (n) first frame index of each box */
+    const double *phi;              /* (n) predicted spindle angle (deg) */
+    const double *zeta;             /* (n) Kabsch zeta */
+    double phi0, osc, z_shift;      /* frame k spans phi(k) .. phi(k + 1), phi(z) = phi0 + osc (z - z_shift) (deg) */
+} XiRocking;
+
+/* The sigma_M grid search (xpg/integrate.py:1130-1154): for each width grid[g] (deg), cost[g] = the sum over rows
+ * with a positive fz total tot of tot * (fz / tot - R)^2, R the Gaussian rocking curve of that width integrated
+ * over each of the 65 frames and normalised over them. */
+int xi_rocking_costs(const XiRocking *q, const double *grid, int n_grid, double *cost, void *stream);
+
+/* Normal equations of the rocking-curve mixture fit (xpg/integrate.py:437-447, the Gram form of _nnls_gram,
+ * :1095-1104): gram = A^T A (21 x 21, row-major) and rhs = A^T y with A = B sqrt(tot), y = fz / tot sqrt(tot),
+ * tot = max(sum fz, 1e-9), B the frame integrals of the 21 mixture components at width sm (rad). */
+size_t xi_rocking_gram_workspace(const XiRocking *q);
+int xi_rocking_gram(const XiRocking *q, double sm, void *ws, size_t ws_bytes, double *gram, double *rhs,
+                    void *stream);
+
 /* xi_knn without a workspace argument; it has no counterpart in XPG (whose neighbour search runs on the host).
  * For callers that cannot allocate device memory: a program binding this library through a plain C FFI beside a
  * framework that has already reserved the GPU's memory in its own pool (cudaMalloc would fail there, and

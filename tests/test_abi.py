@@ -32,7 +32,8 @@ def test_struct_layouts_match_header(tmp_path):
     structs = {"XiDetector": N.XiDetector, "XiRows": N.XiRows, "XiBlock": N.XiBlock, "XiPass1Out": N.XiPass1Out,
                "XiPass2In": N.XiPass2In, "XiPass2Out": N.XiPass2Out, "XiGatherRows": N.XiGatherRows,
                "XiFrames": N.XiFrames, "XiPlanDetector": N.XiPlanDetector, "XiPredict": N.XiPredict,
-               "XiPredictOut": N.XiPredictOut, "XiBoxRules": N.XiBoxRules, "XiBoxOut": N.XiBoxOut, "XiKnn": N.XiKnn}
+               "XiPredictOut": N.XiPredictOut, "XiBoxRules": N.XiBoxRules, "XiBoxOut": N.XiBoxOut, "XiKnn": N.XiKnn,
+               "XiRocking": N.XiRocking}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "xpgi.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')

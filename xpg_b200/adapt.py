@@ -1,5 +1,6 @@
-"""Per-block adaptation of the spot widths and the rocking-curve shape, and the spot-width estimate of a sweep:
-host float64 algorithms on the pass-1 outputs of strong reflections.
+"""Per-block adaptation of the spot widths and the rocking-curve shape, and the spot-width estimate of a sweep,
+on the pass-1 outputs of strong reflections: the two float64 sweeps over the strong rows' frames (the sigma_M grid
+search, the Gram system of the rocking-curve fit) run on the device, the small solves and medians on the host.
 
 References: `_adapt_block` (`xpg/integrate.py:404-461`), `_fit_rocking_width` (`:1130-1154`), `_nnls_gram`
 (`:1095-1104`), `_rocking_resolved` (`:1107-1127`), `_estimate_sigmas` (`:1002-1092`), `rc_basis_np`
@@ -7,6 +8,8 @@ References: `_adapt_block` (`xpg/integrate.py:404-461`), `_fit_rocking_width` (`
 pass 2 and to the next block are the same numbers.
 """
 from __future__ import annotations
+
+import ctypes as C
 
 import numpy as np
 from scipy.special import erf
@@ -33,41 +36,43 @@ def rc_basis(phi_lo, phi_hi, phi_c, zeta, sm):
     return 0.5 * (erf(a) - erf(b))
 
 
-def nnls_gram(A, y):
-    """argmin ||A w - y||, w >= 0, solved on the K x K Cholesky factor of A^T A."""
-    from scipy.linalg import LinAlgError, cholesky, solve_triangular
-    from scipy.optimize import nnls
-    try:
-        R = cholesky(A.T @ A)
-        return nnls(R, solve_triangular(R.T, A.T @ y, lower=True))[0]
-    except (LinAlgError, ValueError):
-        return nnls(A, y)[0]
+def _rocking_struct(F, IZ, PH, ZK, g):
+    """XiRocking of strong rows: F (n, 65) float64 on the device; iz0 / phi (deg) / zeta host arrays."""
+    import torch
+    from . import native as N
+    from .device import h2d
+    dev = F.device
+    keep = dict(F=F.contiguous(), iz0=h2d(np.asarray(IZ, np.int32), None, dev), phi=h2d(np.asarray(PH, np.float64),
+                None, dev), zeta=h2d(np.asarray(ZK, np.float64), None, dev))
+    q = N.XiRocking()
+    q.n = int(F.shape[0])
+    q.fz, q.iz0, q.phi, q.zeta = (N.ptr(keep[k]) for k in ("F", "iz0", "phi", "zeta"))
+    q.phi0, q.osc, q.z_shift = float(g.phi0), float(g.osc), float(g.starting_frame - 1)
+    return q, keep
 
 
 def fit_rocking_width(sel_fit, g, sm_guess, lo_fac=0.2, hi_fac=3.0):
     """Grid search (61 points in log sigma_M) of the frame-integrated Gaussian rocking curve against the per-frame
-    intensity fractions of strong reflections."""
-    fz = np.concatenate([s[0] for s in sel_fit])
-    iz0 = np.concatenate([s[1] for s in sel_fit])
-    phi = np.concatenate([s[2] for s in sel_fit])
-    zeta = np.abs(np.concatenate([s[3] for s in sel_fit]))
-    tot = fz.sum(1, keepdims=True)
-    ok = tot[:, 0] > 0
-    fz, iz0, phi, zeta, tot = fz[ok], iz0[ok], phi[ok], zeta[ok], tot[ok]
-    frac = fz / tot
-    k = iz0[:, None] + np.arange(fz.shape[1])[None]
-    lo = g.z_to_phi(k.astype(float))
-    hi = g.z_to_phi(k + 1.0)
-    lo, hi = np.minimum(lo, hi), np.maximum(lo, hi)
+    intensity fractions of strong reflections; each candidate's cost is one device reduction (xi_rocking_costs).
+    sel_fit: list of (fz (n, 65), iz0, phi (deg), zeta) with fz a host array or a device tensor."""
+    import torch
+    from . import native as N
+    from .device import TIMER
+    Fs = [torch.as_tensor(s[0], dtype=torch.float64) for s in sel_fit]
+    dev = next((f.device for f in Fs if f.is_cuda), torch.device("cuda"))
+    F = torch.cat([f.to(dev) for f in Fs]) if Fs else torch.zeros((0, MAX_DZ), dtype=torch.float64, device=dev)
+    iz0 = np.concatenate([s[1] for s in sel_fit]) if sel_fit else np.zeros(0, np.int32)
+    phi = np.concatenate([s[2] for s in sel_fit]) if sel_fit else np.zeros(0)
+    zeta = np.concatenate([s[3] for s in sel_fit]) if sel_fit else np.zeros(0)
     grid = sm_guess * np.exp(np.linspace(np.log(lo_fac), np.log(hi_fac), 61))
-
-    def cost(sm):
-        s = sm / zeta[:, None] * np.sqrt(2)
-        R = 0.5 * (erf((hi - phi[:, None]) / s) - erf((lo - phi[:, None]) / s))
-        R = R / np.maximum(R.sum(1, keepdims=True), 1e-9)
-        return np.sum(tot * (frac - R) ** 2)
-    from .geometry import _pool
-    costs = list(_pool().map(cost, grid))           # every candidate's cost is computed whole, as one call
+    q, keep = _rocking_struct(F, iz0, phi, zeta, g)
+    grid_t = torch.as_tensor(grid, dtype=torch.float64).to(dev)
+    cost_t = torch.empty(len(grid), dtype=torch.float64, device=dev)
+    lib = N.load()
+    with TIMER.span("adapt"):
+        N.check(lib.xi_rocking_costs(C.byref(q), N.ptr(grid_t), len(grid), N.ptr(cost_t), N.stream_handle()),
+                "xi_rocking_costs")
+    costs = cost_t.cpu().numpy()
     best = (np.inf, sm_guess)
     for c, sm in zip(costs, grid):
         if c < best[0]:
@@ -75,39 +80,61 @@ def fit_rocking_width(sel_fit, g, sm_guess, lo_fac=0.2, hi_fac=3.0):
     return float(best[1])
 
 
+def _rocking_weights(q, sm_new, F, IZ, PH, ZK, g):
+    """Non-negative rocking-curve mixture weights at width sm_new (rad): the Gram system of A w = y on the device
+    (xi_rocking_gram), solved on its 21 x 21 Cholesky factor; the full least-squares form when the Gram matrix is not
+    positive definite."""
+    import torch
+    from scipy.linalg import LinAlgError, cholesky, solve_triangular
+    from scipy.optimize import nnls
+    from . import native as N
+    from .device import TIMER
+    lib = N.load()
+    dev = F.device
+    ws = torch.empty(max(int(lib.xi_rocking_gram_workspace(C.byref(q))), 1), dtype=torch.uint8, device=dev)
+    gram = torch.empty((len(RC_C), len(RC_C)), dtype=torch.float64, device=dev)
+    rhs = torch.empty(len(RC_C), dtype=torch.float64, device=dev)
+    with TIMER.span("adapt", 3):
+        N.check(lib.xi_rocking_gram(C.byref(q), float(sm_new), N.ptr(ws), ws.numel(), N.ptr(gram), N.ptr(rhs),
+                                    N.stream_handle()), "xi_rocking_gram")
+    G, h = gram.cpu().numpy(), rhs.cpu().numpy()
+    try:
+        R = cholesky(G)
+        return nnls(R, solve_triangular(R.T, h, lower=True))[0]
+    except (LinAlgError, ValueError):
+        Fh = F.cpu().numpy()
+        k = np.asarray(IZ)[:, None] + np.arange(Fh.shape[1])[None]
+        lo = g.z_to_phi(k.astype(float))
+        hi = g.z_to_phi(k + 1.0)
+        lo, hi = np.radians(np.minimum(lo, hi)), np.radians(np.maximum(lo, hi))
+        Bm = rc_basis(lo, hi, np.radians(PH), ZK, sm_new)
+        tot = np.maximum(Fh.sum(1, keepdims=True), 1e-9)
+        A = (Bm * np.sqrt(tot)[:, :, None]).reshape(-1, len(RC_C))
+        y = (Fh / tot * np.sqrt(tot)).reshape(-1)
+        return nnls(A, y)[0]
+
+
 def _truncation_factor():
     """<r^2/2> / sigma^2 of a 2D Gaussian inside radius FG_R."""
     return 1.0 - (FG_R ** 2 / 2) * np.exp(-FG_R ** 2 / 2) / (1 - np.exp(-FG_R ** 2 / 2))
 
 
-def adapt_block(g, strong_sets, sd_run, sm_run, sd_b, sm_b, rcw_b):
+def adapt_block(g, strong, sd_run, sm_run, sd_b, sm_b, rcw_b):
     """sigma_M and the rocking-curve weights of this block's pass 2, sigma_D of the next block.
 
-    strong_sets: list of (F (n, 65) per-frame net, phi (deg), zeta_k, iz0, m_d, x, y) of the block's strong rows in
-    the reference's chunk order. Returns (sm_new, rcw_new, sd_next or None, params dict)."""
-    if strong_sets:
-        F, PH, ZK, IZ, MD, X, Y = (np.concatenate([s[i] for s in strong_sets]) for i in range(7))
-    else:
-        F = np.zeros((0, MAX_DZ))
-    n = len(F)
+    strong: None, or the block's strong rows in the reference's chunk order: dict F (n, 65) float64 per-frame net
+    on the device, phi (deg), zeta_k, iz0, m_d, x, y (host arrays). Returns (sm_new, rcw_new, sd_next or None,
+    params dict)."""
+    n = 0 if strong is None else int(strong["F"].shape[0])
     if n < 100:
         params = dict(sigma_d=float(np.degrees(sd_b)), sigma_m=float(np.degrees(sm_b)), n=n,
                       rcw=np.asarray(rcw_b).round(3).tolist())
         return sm_b, rcw_b, None, params
+    F, PH, ZK, IZ, MD, X, Y = (strong[k] for k in ("F", "phi", "zeta_k", "iz0", "m_d", "x", "y"))
     sm_fit = np.radians(fit_rocking_width([(F, IZ, PH, ZK)], g, np.degrees(sm_run), 0.5, 2.0))
     sm_new = float(np.exp((n * np.log(sm_fit) + PRIOR_N * np.log(sm_run)) / (n + PRIOR_N)))
-    k = IZ[:, None] + np.arange(F.shape[1])[None]
-    lo = g.z_to_phi(k.astype(float))
-    hi = g.z_to_phi(k + 1.0)
-    lo, hi = np.radians(np.minimum(lo, hi)), np.radians(np.maximum(lo, hi))
-    from .geometry import par_rows
-    PHr = np.radians(PH)
-    Bm = np.concatenate(par_rows(lambda a, b: rc_basis(lo[a:b], hi[a:b], PHr[a:b], ZK[a:b], sm_new), len(PH),
-                                 min_rows=128))
-    tot = np.maximum(F.sum(1, keepdims=True), 1e-9)
-    A = (Bm * np.sqrt(tot)[:, :, None]).reshape(-1, len(RC_C))
-    y = (F / tot * np.sqrt(tot)).reshape(-1)
-    w = nnls_gram(A, y)
+    q, keep = _rocking_struct(F, IZ, PH, ZK, g)
+    w = _rocking_weights(q, sm_new, F, IZ, PH, ZK, g)
     lam = PRIOR_RC / n
     w = (w / max(w.sum(), 1e-9) + lam * rc_default_weights()) / (1 + lam)
     Xv = g.pixel_to_lab(X, Y)

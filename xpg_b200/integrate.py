@@ -170,13 +170,12 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         rows = blk.rows
         if adaptive:
             st = _adapt_rows(h1, plan, rows)
-            sets = []
+            strong = None
             if st.any():
-                F = _fz_padded(p1, rs, st)
                 rst = rows[st]
-                sets.append((F, refl["phi"][rst], refl["zeta_k"][rst], plan.iz0[rst], h1["m_d"][st], refl["x"][rst],
-                             refl["y"][rst]))
-            sm_b, rcw_b, sd_next, params = A.adapt_block(g, sets, sd, sm, sd_b, sm_b, rcw_b)
+                strong = dict(F=_fz_rows(p1, rs, np.flatnonzero(st)), phi=refl["phi"][rst], zeta_k=refl["zeta_k"][rst],
+                              iz0=plan.iz0[rst], m_d=h1["m_d"][st], x=refl["x"][rst], y=refl["y"][rst])
+            sm_b, rcw_b, sd_next, params = A.adapt_block(g, strong, sd, sm, sd_b, sm_b, rcw_b)
             if sd_next is not None:
                 state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
             block_params[b] = params
@@ -195,7 +194,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         for k, v in h.items():
             out[k][dst] = v
         if fz_out is not None:
-            fz_out[rows] = _fz_padded(p1, rs, np.ones(rs.n, bool)).astype(np.float32)
+            fz_out[rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
         t_dev += time.time() - tg
 
     # ---- frame loop: wedges of consecutive frame numbers --------------------------------------------------------
@@ -270,17 +269,15 @@ def _host_rows(t, keys, perm=None):
     return out
 
 
-def _fz_padded(p1: D.Pass1Buffers, rs: D.RowSet, sel):
-    """fz of the selected rows, padded to the deepest box (zeros): gathered on the device, float64 on the host."""
-    rows = np.flatnonzero(sel)
+def _fz_rows(p1: D.Pass1Buffers, rs: D.RowSet, rows):
+    """fz of the given local rows, padded to the deepest box with zeros: a (n, 65) float64 device tensor."""
     if rows.size == 0:
-        return np.zeros((0, MAX_DZ), np.float32)
+        return torch.zeros((0, MAX_DZ), dtype=torch.float64, device=rs.device)
     r = D.h2d(rows, None, rs.device)
     k = torch.arange(MAX_DZ, device=rs.device)
     off = rs.t["frm_off"].index_select(0, r)[:, None] + k
     ok = k[None] < rs.t["Dz"].index_select(0, r)[:, None]
-    F = torch.where(ok, p1.t["fz"][torch.where(ok, off, 0)], torch.zeros((), device=rs.device))
-    return F.cpu().numpy().astype(np.float64)
+    return torch.where(ok, p1.t["fz"][torch.where(ok, off, 0)], torch.zeros((), device=rs.device)).double()
 
 
 def _adapt_rows(h1, plan, rows):

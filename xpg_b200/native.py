@@ -123,11 +123,17 @@ class XiKnn(C.Structure):
                 ("lo", _d3), ("hi", _d3), ("radius", C.c_double), ("k", C.c_int)]
 
 
+class XiRocking(C.Structure):
+    _fields_ = [("n", C.c_int64), ("fz", _fp), ("iz0", _fp), ("phi", _fp), ("zeta", _fp), ("phi0", C.c_double),
+                ("osc", C.c_double), ("z_shift", C.c_double)]
+
+
 XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP = 1, 2, 3
 
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
-           "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_predict_workspace", "xi_knn_workspace")
+           "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
+           "xi_knn_workspace", "xi_rocking_gram_workspace")
 
 _LIB = None
 
@@ -156,6 +162,11 @@ def load(path=None):
     lib.xi_knn_workspace.argtypes = [C.POINTER(XiKnn)]
     lib.xi_knn.argtypes = [C.POINTER(XiKnn), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_knn_noalloc.argtypes = [C.POINTER(XiKnn), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.xi_rocking_costs.argtypes = [C.POINTER(XiRocking), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    lib.xi_rocking_gram_workspace.restype = C.c_size_t
+    lib.xi_rocking_gram_workspace.argtypes = [C.POINTER(XiRocking)]
+    lib.xi_rocking_gram.argtypes = [C.POINTER(XiRocking), C.c_double, C.c_void_p, C.c_size_t, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
     lib.xi_status.argtypes = [C.c_void_p]
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
