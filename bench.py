@@ -172,6 +172,11 @@ class Block:
 
 SAMPLE = dict(a=100, wz=24, crop=1024)     # frame window and detector crop of the CPU sample
 
+# DRAM bytes (read + write) per shoebox voxel of the pass kernels, from one ncu capture of a launch of the same
+# kernels on the config-2 geometry (a 20-frame block: the 2,597-reflection launch of 31 x 31 x 33 boxes, 82.4 M
+# voxels, profiles/pass_kernels_config2_small_full.md); the traffic of a launch here is that figure times its voxels
+DRAM_BYTES_PER_VOXEL = {"pass1": 4.489, "pass2": 4.419}
+
 
 def _sample_rows(p, nx, ny):
     """Rows of the CPU sample: boxes inside frames [a, a + wz) and inside a crop x crop detector patch."""
@@ -283,8 +288,11 @@ def run(args):
         n_l, t_k = ksum[dom]
         per_launch = bpk.get(dom, 0.0) * args.steps / max(n_l, 1)
         achieved = per_launch / (t_k / n_l) / 1e9
+        vox = float((blk.plan.Dz * blk.plan.bx.astype(np.float64) ** 2).sum()) * args.steps / max(n_l, 1)
+        traffic = round(DRAM_BYTES_PER_VOXEL[dom] * vox / 1e9, 3) if dom in DRAM_BYTES_PER_VOXEL else None
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_unit": "GB per launch",
+                "algorithmic": round(per_launch / 1e9, 3), "peak_kind": peak_kind,
                 "launches": n_l, "ms_per_launch": round(t_k / n_l * 1e3, 4),
                 "share": {k: round(v[1] / max(sum(x[1] for x in ksum.values()), 1e-12), 4) for k, v in ksum.items()}}
     # end to end: frames from pinned host memory, uploaded inside every step; results read back by the API
