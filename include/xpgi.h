@@ -159,7 +159,8 @@ int xi_tune(int key, long long value);
 int xi_gather(const XiFrames *frames, const XiGatherRows *rows, float *arena, int32_t *cnt, void *stream);
 
 /* Binned-bin decode (xpg/shoebox.py:264-268, xpg/integrate.py:483-488): NaN -> -2, inf -> -1, stored + 3; bins
- * with fewer than fb frames recorded become unrecorded (0). Applies to rows with cnt_off >= 0. */
+ * with fewer than fb frames recorded become unrecorded (0). Applies to rows with cnt_off >= 0 (of rows->order when
+ * given), once each, after their last frame has been gathered. */
 int xi_decode_bins(const XiGatherRows *rows, float *arena, const int32_t *cnt, void *stream);
 
 /* Pass 1 (xpg/integrate_kernels.py:287-365): pixel geometry, masks, robust background, summation, centroids,

@@ -1240,7 +1240,7 @@ __global__ void k_gather(XiFrames F, XiGatherRows G, float* __restrict__ arena, 
 }
 
 __global__ void k_decode_bins(XiGatherRows G, float* __restrict__ arena, const int32_t* __restrict__ cnt) {
-    const int row = blockIdx.x;
+    const int row = G.order ? G.order[blockIdx.x] : blockIdx.x;
     if (G.cnt_off[row] < 0) return;
     const int Dz = G.Dz[row], bx = G.bx[row], fb = G.fb[row];
     const int P = bx * bx;
@@ -1513,7 +1513,9 @@ int xi_gather(const XiFrames* F, const XiGatherRows* G, float* arena, int32_t* c
 int xi_decode_bins(const XiGatherRows* G, float* arena, const int32_t* cnt, void* stream) {
     if (!G || !arena || !cnt) return fail(XI_E_ARG, "xi_decode_bins: null argument");
     if (G->n == 0) return XI_OK;
-    k_decode_bins<<<G->n, 256, 0, (cudaStream_t)stream>>>(*G, arena, cnt);
+    const int nblk = G->order ? G->n_order : G->n;
+    if (nblk <= 0) return XI_OK;
+    k_decode_bins<<<nblk, 256, 0, (cudaStream_t)stream>>>(*G, arena, cnt);
     return cuda_check("xi_decode_bins");
 }
 

@@ -353,7 +353,29 @@ def gather(frames_s, grows: GatherRows, order, arena, cnt, stream=None):
                 "xi_gather")
 
 
-def decode_bins(grows: GatherRows, arena, cnt, stream=None):
+def decode_bins(grows: GatherRows, arena, cnt, stream=None, order=None):
+    """Decode the binned rows (all, or the device int32 `order` subset)."""
     lib = N.load()
+    g = grows.s if order is None else grows.view(order)
     with TIMER.span("decode_bins"):
-        N.check(lib.xi_decode_bins(C.byref(grows.s), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")
+        N.check(lib.xi_decode_bins(C.byref(g), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")
+
+
+def host_groups(rows: RowSet, idx):
+    """Launch groups (as RowSet.groups: one shape each, largest first) of the local rows idx, as host int32 arrays."""
+    idx = np.asarray(idx, np.int64)
+    if idx.size == 0:
+        return []
+    key = rows.bx[idx] * 128 + rows.Dz[idx]
+    o = np.argsort(key, kind="stable")
+    ks = key[o]
+    uk, start = np.unique(ks, return_index=True)
+    stop = np.append(start[1:], o.size)
+    out = [(int(k // 128), int(k % 128), idx[o[a:e]].astype(np.int32)) for k, a, e in zip(uk, start, stop)]
+    out.sort(key=lambda g: -g[0] * g[0] * g[1])
+    return out
+
+
+def subset_groups(rows: RowSet, idx):
+    """Launch groups of the local rows idx, with device order tensors."""
+    return [(b, dz, h2d(r, None, rows.device)) for b, dz, r in host_groups(rows, idx)]

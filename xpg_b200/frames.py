@@ -16,6 +16,35 @@ import numpy as np
 import torch
 
 
+class _Uploads:
+    """Wedge transfers on a copy stream of their own: a wedge's upload overlaps the kernels of the wedges before it.
+    The compute stream waits for each wedge's copy before its gathers; at most `depth` wedges are in flight (device
+    memory)."""
+
+    def __init__(self, depth=4):
+        self.stream = None
+        self.inflight = []
+        self.depth = depth
+
+    def upload(self, h, device):
+        cur = torch.cuda.current_stream()
+        if self.stream is None:
+            self.stream = torch.cuda.Stream()
+        while len(self.inflight) >= self.depth:
+            self.inflight.pop(0).synchronize()
+        with torch.cuda.stream(self.stream):
+            d = h.to(device, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        cur.wait_event(ev)
+        d.record_stream(cur)                 # the compute stream reads it: no reuse before its kernels ran
+        self.inflight.append(ev)
+        return d, ev
+
+
+_UPLOADS = _Uploads()
+
+
 class _PinnedRing:
     """Two pinned staging buffers used alternately; a buffer is refilled only after its last upload finished."""
 
@@ -36,9 +65,7 @@ class _PinnedRing:
         return k, self.bufs[k][:n]
 
     def upload(self, k, h, device):
-        d = h.to(device, non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
+        d, ev = _UPLOADS.upload(h, device)
         self.events[k] = ev
         return d
 
@@ -54,6 +81,7 @@ class U32Frames:
         self.min_valid = int(min_valid)
         self.device = device
         self.on_device = torch.is_tensor(data) and data.is_cuda
+        self.resident = self.on_device          # frames already in device memory: nothing to transfer
         self._ring = _PinnedRing(torch.int32)
 
     def _host_slice(self, a, b):
@@ -66,7 +94,9 @@ class U32Frames:
         src = self._host_slice(f_a, f_b)
         if torch.is_tensor(src):
             h = src if src.dtype == torch.int32 else src.view(torch.int32)
-            return h.to(self.device, non_blocking=True), False
+            if not h.is_pinned():
+                return h.to(self.device), False
+            return _UPLOADS.upload(h, self.device)[0], False
         n = src.shape[0]
         k, buf = self._ring.take(n * self.ny * self.nx)
         h = buf.view(n, self.ny, self.nx)
@@ -84,6 +114,7 @@ class ImageSetFrames:
         self.overload = None
         self.min_valid = 0
         self.device = device
+        self.resident = False
         self._ring = _PinnedRing(torch.float32)
 
     def wedge(self, f_a, f_b, ok=None, stream=None):

@@ -29,6 +29,7 @@ from .plan import DZ_BUCKETS, IntegrationModel, plan_integration
 PROFILE_GRID = 41
 MAX_DZ = max(DZ_BUCKETS)
 WEDGE_FRAMES = 32                     # frames per upload / gather launch
+EARLY_PASS1_ROWS = 16384              # completed rows worth an early pass-1 launch (uploaded frames)
 OUT_F64 = ("bg", "isum", "vsum", "vsum0", "iprf", "vprf", "vprf0", "corr", "xo", "yo", "zo", "p_valid", "p_total",
            "frac_rec", "rho", "m_d", "m_m", "p_fg")
 
@@ -82,10 +83,49 @@ class _Block:
         self.span = (int(srt[0]), int(srt[-1]) + 1) if srt.size and srt[-1] - srt[0] + 1 == srt.size else None
         self.z_lo = p.iz0[rows].astype(np.int64)
         self.z_hi = self.z_lo + self.grows.span - 1      # last frame index a row's box can take
+        self.comp_hi = self.z_hi                          # last frame a row receives (set by schedule())
+        self.p1 = None                                    # pass-1 buffers and constants, made at the first pass 1
+        self.c1 = None
+        self.p1_done = np.zeros(rows.size, bool)
 
     def rows_in(self, fi_a, fi_b):
         """Local rows whose box frame range meets [fi_a, fi_b]."""
         return np.flatnonzero((self.z_lo <= fi_b) & (self.z_hi >= fi_a)).astype(np.int32)
+
+    def schedule(self, wedges, eff_hi, early_rows, device):
+        """The block's per-wedge index lists, computed at block open and uploaded in one copy: the rows each wedge
+        gathers into, and (early_rows > 0) the launch groups of the rows whose last frame arrives with a wedge, batched
+        to at least early_rows rows. One upload before the frame transfers: a small copy issued later would wait in
+        the copy engine behind every frame wedge already queued."""
+        self.comp_hi = np.minimum(self.z_hi, eff_hi)
+        parts, off = [], 0
+
+        def add(a):
+            nonlocal off
+            parts.append(np.asarray(a, np.int32))
+            o = off
+            off += parts[-1].size
+            return o, parts[-1].size
+        self.w_gather, self.w_early = {}, {}
+        acc = np.zeros(0, np.int64)
+        for w, (fa, fb) in enumerate(wedges):
+            fi_a, fi_b = fa - 1, fb - 1
+            if eff_hi >= fi_a:
+                loc = self.rows_in(fi_a, min(fi_b, eff_hi))
+                if loc.size:
+                    self.w_gather[w] = add(loc)
+            if early_rows:
+                acc = np.concatenate([acc, np.flatnonzero((self.comp_hi <= fi_b) & (self.comp_hi >= fi_a))])
+                if acc.size >= early_rows:
+                    groups = [(bx, dz, add(o)) for bx, dz, o in D.host_groups(self.rowset, acc)]
+                    binned = acc[self.grows.binned[acc]]
+                    self.w_early[w] = (acc, groups, add(binned) if binned.size else None)
+                    acc = np.zeros(0, np.int64)
+        self.sched_t = D.h2d(np.concatenate(parts) if parts else np.zeros(1, np.int32), None, device)
+
+    def sched(self, o_n):
+        o, n = o_n
+        return self.sched_t[o:o + n]
 
 
 def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dmax=1e9, frames=None, mask=None,
@@ -145,23 +185,51 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     if mask is not None and not np.asarray(mask).all():
         mask_t = torch.as_tensor(np.asarray(mask, np.uint8)).to(device)
 
-    def process(b, blk: _Block):
-        nonlocal t_dev
-        tg = time.time()
-        sd_b = state["sd"] if adaptive else sd
-        sm_b, rcw_b = (state["sm"], state["rcw"]) if adaptive else (sm, A.rc_default_weights())
-        g = exp_blocks[b].geom
+    def detector(g):
         key = (id(g), id(bkg_template))
         if key not in det_cache:
             det_cache.clear()
             det_cache[key] = D.DeviceDetector(g, bkg_template, device)
-        det = det_cache[key]
+        return det_cache[key]
+
+    def widths():
+        sd_b = state["sd"] if adaptive else sd
+        sm_b, rcw_b = (state["sm"], state["rcw"]) if adaptive else (sm, A.rc_default_weights())
+        return sd_b, sm_b, rcw_b
+
+    def block_pass1_consts(b, blk: _Block):
+        """The block's pass-1 constants from the current widths (those adapted by every block processed before it),
+        made once; allocated with the buffers before any frame transfer of the block is queued."""
+        if blk.p1 is None:
+            sd_b, sm_b, rcw_b = widths()
+            blk.c1 = (sd_b, sm_b, rcw_b) + D.block_consts(exp_blocks[b].geom, sd_b, sm_b, model.gain, rcw_b, device)
+            blk.p1 = D.Pass1Buffers(blk.rowset)
+
+    def pass1_rows(b, blk: _Block, idx, groups=None, binned_t=None):
+        """Bin decode and pass 1 of the block's local rows idx, whose frames have all been gathered (launch groups
+        and binned rows on the device when given, else made here)."""
+        block_pass1_consts(b, blk)
+        if binned_t is None:
+            binned = idx[blk.grows.binned[idx]]
+            binned_t = D.h2d(binned.astype(np.int32), None, device) if binned.size else None
+        if binned_t is not None:
+            D.decode_bins(blk.grows, blk.arena, blk.cnt, order=binned_t)
+        if groups is None and idx.size != blk.rowset.n:
+            groups = D.subset_groups(blk.rowset, idx)
+        D.pass1(detector(exp_blocks[b].geom), blk.rowset, blk.c1[3], blk.arena, blk.p1, groups=groups)
+        blk.p1_done[idx] = True
+
+    def process(b, blk: _Block):
+        nonlocal t_dev
+        tg = time.time()
+        g = exp_blocks[b].geom
+        det = detector(g)
         rs = blk.rowset
-        if blk.grows.any_binned:
-            D.decode_bins(blk.grows, blk.arena, blk.cnt)
-        c1, k1 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
-        p1 = D.Pass1Buffers(rs)
-        D.pass1(det, rs, c1, blk.arena, p1)
+        rem = np.flatnonzero(~blk.p1_done)
+        if rem.size:
+            pass1_rows(b, blk, rem)
+        sd_b, sm_b, rcw_b = blk.c1[:3]
+        p1 = blk.p1
         num = torch.zeros((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float64, device=device)
         den = torch.zeros_like(num)
         if learn_profiles:
@@ -197,36 +265,63 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
             fz_out[rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
         t_dev += time.time() - tg
 
+    def next_block(extra=None):
+        """The unprocessed block that completes first (the order blocks are processed in); `extra`: a block being
+        opened (after the open ones)."""
+        cand = [(eff_hi[b], 0, open_order.index(b), b) for b in opened]
+        if extra is not None:
+            cand.append((eff_hi[extra], 0, len(open_order), extra))
+        cand += [(eff_hi[b], 1, k, b) for k, b in enumerate(pending)]
+        return min(cand)[3] if cand else None
+
     # ---- frame loop: wedges of consecutive frame numbers --------------------------------------------------------
+    # When frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1 at
+    # once: it overlaps the transfer of the later wedges (their widths are fixed: every block before it has been
+    # processed). Resident frames have no transfer to hide: their blocks run pass 1 whole, in the fewest launches.
     W = max(int(wedge_frames), 1)
-    f = f_first
-    while f <= f_last:
-        f_b = min(f + W - 1, f_last)
+    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, W)]
+    oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in wedges]
+    ok_parts = [ok.astype(np.uint8) for ok in oks if not ok.all()]
+    ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
+    early_rows = 0 if getattr(src, "resident", False) else EARLY_PASS1_ROWS
+    ok_off = 0
+    for w, (f, f_b) in enumerate(wedges):
         fi_a, fi_b = f - 1, f_b - 1
         while pending and plan.need_lo[pending[0]] <= fi_b:
             b = pending.pop(0)
-            opened[b] = _Block(b, blocks_rows[b], plan, device)
+            blk = _Block(b, blocks_rows[b], plan, device)
+            blk.schedule(wedges, eff_hi[b], early_rows, device)
+            if early_rows and next_block(extra=b) == b:
+                block_pass1_consts(b, blk)
+            opened[b] = blk
             open_order.append(b)
-        ok = np.array([(g_ not in excl) for g_ in range(f, f_b + 1)], bool)
+        ok = oks[w]
+        ok_t = None
+        if not ok.all():
+            ok_t = ok_dev[ok_off:ok_off + ok.size]
+            ok_off += ok.size
         if ok.any() and opened:
             data, is_f = src.wedge(f, f_b, ok)
-            ok_t = D.h2d(ok.astype(np.uint8), None, device) if not ok.all() else None
             for b in open_order:
                 blk = opened.get(b)
-                if blk is None or eff_hi[b] < fi_a:
+                if blk is None or w not in blk.w_gather:
                     continue
                 nf = min(fi_b, eff_hi[b]) - fi_a + 1
-                loc = blk.rows_in(fi_a, fi_a + nf - 1)
-                if loc.size == 0:
-                    continue
                 fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
                                      mask_t, ok_t[:nf] if ok_t is not None else None)
-                D.gather(fs, blk.grows, D.h2d(loc, None, device), blk.arena, blk.cnt)
+                D.gather(fs, blk.grows, blk.sched(blk.w_gather[w]), blk.arena, blk.cnt)
         done = sorted((b for b in open_order if b in opened and eff_hi[b] <= fi_b),
                       key=lambda b: (eff_hi[b], open_order.index(b)))
         for b in done:
             process(b, opened.pop(b))
-        f = f_b + 1
+        nxt = next_block()
+        if nxt is not None and nxt in opened and w in opened[nxt].w_early:
+            blk = opened[nxt]
+            idx, groups, bin_on = blk.w_early[w]
+            idx = idx[~blk.p1_done[idx]]
+            if idx.size == blk.w_early[w][0].size:          # none of them done yet: the precomputed launches apply
+                pass1_rows(nxt, blk, idx, [(bx, dz, blk.sched(o)) for bx, dz, o in groups],
+                           blk.sched(bin_on) if bin_on is not None else None)
     for b in open_order:
         if b in opened:
             process(b, opened.pop(b))
