@@ -106,6 +106,26 @@ def test_results_independent_of_wedge_size():
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
 
 
+@pytest.mark.parametrize("case", ["binned", "adaptive"])
+def test_results_independent_of_schedule(case, monkeypatch):
+    """Pass 1 of completed rows between wedge uploads (forced for every wedge), and resident frames gathered in one
+    wedge, give the same results as the default schedule; "adaptive" has two blocks whose widths carry over."""
+    import sys
+
+    import torch
+    from xpg_b200 import frames as FR
+    I = sys.modules["xpg_b200.integrate"]              # the module (the package exports the function of that name)
+    spec = G.case_inputs(case)[0]
+    a = _run(case).refl
+    resident = FR.U32Frames(torch.as_tensor(G.frames_of(case).view(np.int32)).cuda(), first=1, overload=spec.overload)
+    b = _run(case, images=resident).refl
+    monkeypatch.setattr(I, "EARLY_PASS1_ROWS", 1)
+    c = _run(case, wedge_frames=3).refl
+    for k in CHECK_F + ("n_over", "n_fg_masked"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), ("resident", k)
+        assert np.array_equal(np.asarray(a[k]), np.asarray(c[k]), equal_nan=True), ("early pass 1", k)
+
+
 def test_estimate_sigmas_matches_reference():
     from xpg_b200 import frames as FR
     from xpg_b200.integrate import estimate_sigmas

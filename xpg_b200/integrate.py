@@ -278,12 +278,13 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     # When frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1 at
     # once: it overlaps the transfer of the later wedges (their widths are fixed: every block before it has been
     # processed). Resident frames have no transfer to hide: their blocks run pass 1 whole, in the fewest launches.
-    W = max(int(wedge_frames), 1)
-    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, W)]
+    resident = bool(getattr(src, "resident", False))
+    W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
+    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
     oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in wedges]
     ok_parts = [ok.astype(np.uint8) for ok in oks if not ok.all()]
     ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
-    early_rows = 0 if getattr(src, "resident", False) else EARLY_PASS1_ROWS
+    early_rows = 0 if resident else EARLY_PASS1_ROWS
     ok_off = 0
     for w, (f, f_b) in enumerate(wedges):
         fi_a, fi_b = f - 1, f_b - 1
