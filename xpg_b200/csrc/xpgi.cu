@@ -302,6 +302,7 @@ __device__ void stage_wait(bool tma, unsigned long long* bar, float* stage, cons
 constexpr int kClipCand = 1024;     // background voxels above the lowest clip threshold kept per CTA
 constexpr int kFgList = 2048;       // foreground pixels listed per CTA (pass C iterates them densely)
 constexpr int kZBatch = 8;          // voxels of a pixel column loaded together (memory-level parallelism)
+constexpr int kGatherBatch = 8;     // frames of a box pixel read together by the gather
 
 // Dynamic shared memory: nblo (8P) | geometry scratch e1s/e2s (8P), then brefs (4P) + nbhi (4P) | flags (P) |
 // img2 counts (P, padded to 16) | staged shoebox (4V, when STAGED).
@@ -1188,6 +1189,13 @@ __device__ __forceinline__ float prepared_pixel(const XiFrames& F, const void* f
     return v;
 }
 
+// the raw value of a pixel known to be inside the frame, encoded as XPG's readers deliver it (mask applied later)
+__device__ __forceinline__ float encode_raw(const XiFrames& F, uint32_t r) {
+    if (r == 0xFFFFFFFFu || r < F.min_valid) return -1.0f;
+    if (r >= F.overload) return -2.0f;
+    return (float)r;
+}
+
 __device__ __forceinline__ float box_value(const XiFrames& F, const void* frame, int sy, int sx, int s) {
     if (s == 1) return prepared_pixel(F, frame, sy, sx);
     // s x s super-pixel (xpg/integrate.py:682-699): incomplete super-pixels at the far edges are masked
@@ -1214,6 +1222,38 @@ __global__ void k_gather(XiFrames F, XiGatherRows G, float* __restrict__ arena, 
     const int w0 = max(0, iz0 - F.first_fi), w1 = min(F.n_frames, iz0 + span - F.first_fi);
     float* dst = arena + G.sb_off[row];
     const size_t fstride = (size_t)F.ny * F.nx * (F.is_float ? sizeof(float) : sizeof(uint32_t));
+    if (fb == 1 && s == 1) {
+        // plain rows: a thread owns box pixels and reads a pixel's frames kGatherBatch at a time (independent loads
+        // in flight); the pixel's bounds and mask are looked up once
+        const size_t fpix = (size_t)F.ny * F.nx;
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            const int y = iy0 + p / bx, x = ix0 + p % bx;
+            const bool inside = y >= 0 && y < F.ny && x >= 0 && x < F.nx;
+            const size_t idx = inside ? (size_t)y * F.nx + x : 0;
+            const bool masked = inside && F.mask && F.mask[idx] == 0;
+            const int k0 = F.first_fi - iz0;                  // box frame of wedge frame 0
+            for (int w = w0; w < w1; w += kGatherBatch) {
+                float vv[kGatherBatch];
+#pragma unroll
+                for (int u = 0; u < kGatherBatch; ++u) {
+                    vv[u] = -1.0f;
+                    const int ww = w + u;
+                    if (inside && ww < w1) {
+                        const size_t o = (size_t)ww * fpix + idx;
+                        vv[u] = F.is_float ? ((const float*)F.data)[o] : encode_raw(F, ((const uint32_t*)F.data)[o]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kGatherBatch; ++u) {
+                    const int ww = w + u;
+                    if (ww >= w1 || (F.frame_ok && !F.frame_ok[ww])) continue;
+                    const float v = masked ? fminf(vv[u], -1.0f) : vv[u];
+                    dst[(size_t)(k0 + ww) * P + p] = v + kSbOff;
+                }
+            }
+        }
+        return;
+    }
     for (int w = w0; w < w1; ++w) {
         if (F.frame_ok && !F.frame_ok[w]) continue;
         const int fi = F.first_fi + w;
