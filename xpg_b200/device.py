@@ -72,6 +72,15 @@ def h2d(a, dtype=None, device="cuda"):
     return t.pin_memory().to(device, non_blocking=True)
 
 
+def d2h(t):
+    """Device tensor -> host numpy array through pinned memory (the array keeps its pinned block alive)."""
+    if t.numel() == 0:
+        return t.cpu().numpy()
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t)
+    return h.numpy()
+
+
 def _dev(a, dtype, device):
     if torch.is_tensor(a):                  # already a tensor (the planner's device columns): convert in place
         return a.to(device=device, dtype=dtype).contiguous()

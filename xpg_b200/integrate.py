@@ -42,16 +42,6 @@ class IntegrationResult:
     timing: dict = field(default_factory=dict)
 
 
-def _reference_row_order(rows, bucket, bxs, pxs, has_partner):
-    """The block's rows in XPG's kernel-call order (`xpg/integrate.py:375-381`): depth bucket, then box side, then
-    super-pixel side (all ascending), partners first within a group, block-row order otherwise (a stable sort on
-    one combined key)."""
-    if rows.size == 0:
-        return rows
-    key = ((bucket[rows].astype(np.int64) * 1024 + bxs[rows]) * 64 + pxs[rows]) * 2 + (~has_partner[rows]).astype(np.int64)
-    return rows[np.argsort(key, kind="stable")]
-
-
 class _Block:
     """Device state of one open phi block."""
 
@@ -65,7 +55,7 @@ class _Block:
         pj = dv["nbj"][:, 0].long().index_select(0, rt)   # nearest neighbour: the partner where there is one
         rad = lambda phi: (phi * (np.pi / 180.0)).float()  # numpy's radians, then float32
         nb = {k: sel(dv["nb" + k]) for k in ("x", "y", "z", "sx", "sz")}
-        if nb["x"].shape[1] != p.nb["x"].shape[1]:        # foreign-spot columns were added on the host
+        if nb["x"].shape[1] != p.nb_columns:              # foreign-spot columns were added on the host
             nb = {k: v[rows] for k, v in p.nb.items()}
         ix0, iy0, iz0, fb, pxs = (sel(dv[k]) for k in ("ix0", "iy0", "iz0", "fb", "pxs"))
         self.rowset = D.RowSet(
@@ -77,8 +67,9 @@ class _Block:
         self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
         order = np.argsort(rows, kind="stable")            # local rows by global row: outputs leave in plan order
-        self.perm_t = D.h2d(order, None, device)
-        self.rows_sorted = rows[order]
+        ident = bool((order == np.arange(order.size)).all())
+        self.perm_t = None if ident else D.h2d(order, None, device)
+        self.rows_sorted = rows if ident else rows[order]
         srt = self.rows_sorted
         self.span = (int(srt[0]), int(srt[-1]) + 1) if srt.size and srt[-1] - srt[0] + 1 == srt.size else None
         self.z_lo = p.iz0[rows].astype(np.int64)
@@ -154,7 +145,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         log(f"  INTEGRATE: {plan.info['n_predicted']} predicted reflections, box {plan.box}x{plan.box} px, sigma_D "
             f"{model.sigma_d:.4f} sigma_M {model.sigma_m:.4f} deg; {plan.info['n_wide']} wide in phi (> {MAX_DZ} "
             f"frames): integrated in bins, {plan.info['n_trunc']} of them still truncated")
-    out = {k: np.full(n, np.nan, np.float64) for k in OUT_F64}
+    out = {k: np.empty(n, np.float64) for k in OUT_F64}           # every processed block fills its rows
     out["n_over"] = np.zeros(n, np.int32)
     out["n_fg_masked"] = np.zeros(n, np.int32)
     keep_fz = not learn_profiles
@@ -166,8 +157,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     block_params, prof_by_block = {}, {}
     t_dev = 0.0
     nblocks = len(exp_blocks)
-    blocks_rows = [_reference_row_order(r, plan.Dz, plan.bx, plan.pxs, plan.has_partner) if r.size else r
-                   for r in plan.blocks_refl]
+    blocks_rows = plan.blocks_refl                     # plan order (a launch groups its rows by shape itself)
     excl = set(int(f) for f in exclude_frames)
     read = [f for f in range(f_first, f_last + 1) if f not in excl]
     read_fi = np.array([f - 1 for f in read], np.int64)
@@ -219,9 +209,12 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         D.pass1(detector(exp_blocks[b].geom), blk.rowset, blk.c1[3], blk.arena, blk.p1, groups=groups)
         blk.p1_done[idx] = True
 
+    processed = []
+
     def process(b, blk: _Block):
         nonlocal t_dev
         tg = time.time()
+        processed.append(b)
         g = exp_blocks[b].geom
         det = detector(g)
         rs = blk.rowset
@@ -327,6 +320,14 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
         if b in opened:
             process(b, opened.pop(b))
 
+    unfilled = np.ones(n, bool)                       # rows of blocks never processed: NaN, as XPG leaves them
+    for b in processed:
+        unfilled[plan.blocks_refl[b]] = False
+    for k in OUT_F64:
+        if moments_only and k not in P1_OUT:         # pass 2 did not run
+            out[k][:] = np.nan
+        else:
+            out[k][unfilled] = np.nan
     refl.update(out)
     refl["overlap"] = plan.overlap
     if fz_out is not None:
@@ -360,7 +361,7 @@ def _host_rows(t, keys, perm=None):
         st = torch.stack([t[k] for k in ks])
         if perm is not None:
             st = st.index_select(1, perm)
-        st = st.cpu().numpy()
+        st = D.d2h(st)
         out.update({k: st[i] for i, k in enumerate(ks)})
     return out
 

@@ -90,8 +90,32 @@ class Plan:
     dev: dict = field(default_factory=dict)      # device copies of the per-row columns (torch tensors)
 
     @property
+    def nb_columns(self):
+        return self.nb.columns if isinstance(self.nb, LazyHost) else int(self.nb["x"].shape[1])
+
+    @property
     def n(self):
         return int(self.refl["x"].size)
+
+
+class LazyHost(dict):
+    """Host copies of device columns, made on first access (the integration itself reads them from the device)."""
+
+    def __init__(self, dev, columns):
+        super().__init__()
+        self._dev = dev
+        self.columns = columns
+
+    def __missing__(self, k):
+        v = self._dev[k].cpu().numpy()
+        self[k] = v
+        return v
+
+    def items(self):
+        return [(k, self[k]) for k in self._dev]
+
+    def keys(self):
+        return self._dev.keys()
 
 
 def _segments(g):
@@ -323,10 +347,11 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
     refl = {k: v.cpu().numpy() for k, v in pred.items()}
     h = {k: v.cpu().numpy().astype(np.int64) for k, v in bcols.items() if k in BOX_I32}
     refl["coverage"] = bcols["coverage"].cpu().numpy()
-    nbh = {k: v.cpu().numpy() for k, v in nb.items()}
+    nbh = LazyHost(nb, K)
     hp = has_partner.cpu().numpy()
     partner = nbj[:, 0].cpu().numpy().astype(np.int64) if n else np.zeros(0, np.int64)
     if foreign_spots is not None and len(foreign_spots[0]) and n:
+        nbh = {k: nbh[k] for k in ("x", "y", "z", "sx", "sz")}
         _add_foreign(nbh, refl, foreign_spots, n_foreign, sxm, szm)
     blk = refl["block"]
     nblocks = len(exp_blocks)
