@@ -196,9 +196,10 @@ int xi_pass2(const XiDetector *det, const XiRows *rows, const XiBlock *blk, cons
 /* Detector of the planner (xpg/geometry.py:246-410; the panel maps of xpg/detector.py:79-90). Panel record k:
  * P0[3] Bx[3] By[3] n[3] u1[3] u2[3] un[3] P0.n Bx.Bx By.By x1 x2 y1 y2 with n = Bx x By, u1 = Bx / qx,
  * u2 = By / qy, un = u1 x u2 and the panel's inclusive 1-based pixel rectangle. Device pointers. */
+#define XI_PANELS_INLINE 4         /* panel records a detector may carry inline (no device copy) */
 typedef struct {
     int n_panels;
-    const double *panels;           /* (n_panels, XI_PANEL_F64) */
+    const double *panels;           /* (n_panels, XI_PANEL_F64); NULL: the records are in panel_inline */
     int segmented;                  /* panel rectangles bound the hits; pixel_to_lab looks the panel up in segmap */
     const int16_t *segmap;          /* (seg_ny, seg_nx) panel of each pixel, -1 in gaps */
     int seg_nx, seg_ny;
@@ -212,6 +213,7 @@ typedef struct {
     double pol_n[3], pol_main[3];   /* polarisation plane normal and its in-plane partner (lp_factor) */
     double pol_f;                   /* polarisation fraction */
     double nx, ny;                  /* detector size in pixels (acceptance test, regions) */
+    double panel_inline[XI_PANELS_INLINE * XI_PANEL_F64];   /* used when panels is NULL (n_panels <= 4) */
 } XiPlanDetector;
 
 /* Predictions of one phi block (xpg/geometry.py:468-545 and the acceptance test of xpg/integrate.py:101-122). */

@@ -108,8 +108,9 @@ def test_results_independent_of_wedge_size():
 
 @pytest.mark.parametrize("case", ["binned", "adaptive"])
 def test_results_independent_of_schedule(case, monkeypatch):
-    """Pass 1 of completed rows between wedge uploads (forced for every wedge), and resident frames gathered in one
-    wedge, give the same results as the default schedule; "adaptive" has two blocks whose widths carry over."""
+    """Pass 1 of completed rows between wedge uploads (forced for every wedge), resident frames gathered in one
+    wedge, and pinned host frames streamed by the transfer thread give the same results as the default schedule;
+    "adaptive" has two blocks whose widths carry over."""
     import sys
 
     import torch
@@ -119,11 +120,16 @@ def test_results_independent_of_schedule(case, monkeypatch):
     a = _run(case).refl
     resident = FR.U32Frames(torch.as_tensor(G.frames_of(case).view(np.int32)).cuda(), first=1, overload=spec.overload)
     b = _run(case, images=resident).refl
+    pinned = torch.as_tensor(G.frames_of(case).view(np.int32)).pin_memory()
+    d = _run(case, images=FR.U32Frames(pinned, first=1, overload=spec.overload), wedge_frames=4).refl
     monkeypatch.setattr(I, "EARLY_PASS1_ROWS", 1)
     c = _run(case, wedge_frames=3).refl
+    e = _run(case, images=FR.U32Frames(pinned, first=1, overload=spec.overload), wedge_frames=3).refl
     for k in CHECK_F + ("n_over", "n_fg_masked"):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), ("resident", k)
         assert np.array_equal(np.asarray(a[k]), np.asarray(c[k]), equal_nan=True), ("early pass 1", k)
+        assert np.array_equal(np.asarray(a[k]), np.asarray(d[k]), equal_nan=True), ("transfer thread", k)
+        assert np.array_equal(np.asarray(a[k]), np.asarray(e[k]), equal_nan=True), ("thread + early pass 1", k)
 
 
 def test_estimate_sigmas_matches_reference():

@@ -29,6 +29,11 @@ constexpr int64_t kMaxCells = 1 << 22;   // cell grid of the neighbour search
 enum { PR_P0 = 0, PR_BX = 3, PR_BY = 6, PR_N = 9, PR_U1 = 12, PR_U2 = 15, PR_UN = 18, PR_P0N = 21, PR_BXBX = 22,
        PR_BYBY = 23, PR_X1 = 24, PR_X2 = 25, PR_Y1 = 26, PR_Y2 = 27 };
 
+// panel record k: device array, or the records carried in the argument itself
+__device__ __forceinline__ const double* panel_rec(const XiPlanDetector& D, int k) {
+    return D.panels ? D.panels + (size_t)k * XI_PANEL_F64 : D.panel_inline + k * XI_PANEL_F64;
+}
+
 __device__ __forceinline__ double dot3(const double* a, const double* b) {
     return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
 }
@@ -114,7 +119,7 @@ __device__ void pixel_to_lab(const XiPlanDetector& D, double x, double y, double
     }
     int k = segment_of(D, x, y);
     k = k < 0 ? 0 : k;
-    const double* pr = D.panels + (size_t)k * XI_PANEL_F64;
+    const double* pr = panel_rec(D, k);
     double xc = x, yc = y;
     if (D.geo_x) {
         xc = x + bilinear(D.geo_x, D.geo_ny, D.geo_nx, x, y);
@@ -139,7 +144,7 @@ __device__ void pixel_to_lab(const XiPlanDetector& D, double x, double y, double
 __device__ void s_to_pixel(const XiPlanDetector& D, const double* S, double* px, double* py) {
     double x = CUDART_NAN, y = CUDART_NAN;
     for (int k = 0; k < D.n_panels; ++k) {
-        const double* pr = D.panels + (size_t)k * XI_PANEL_F64;
+        const double* pr = panel_rec(D, k);
         const double t = pr[PR_P0N] / dot3(S, pr + PR_N);
         double P[3];
         for (int c = 0; c < 3; ++c) P[c] = t * S[c] - pr[PR_P0 + c];
@@ -367,7 +372,8 @@ PredictWs predict_ws(const XiPredict* P, void* base) {
 
 int predict_check(const XiPredict* P, const XiPlanDetector* D) {
     if (!P || !D) return xi_fail(XI_E_ARG, "predict: null argument");
-    if (D->n_panels < 1 || !D->panels) return xi_fail(XI_E_ARG, "predict: no detector panels");
+    if (D->n_panels < 1 || (!D->panels && D->n_panels > XI_PANELS_INLINE))
+        return xi_fail(XI_E_ARG, "predict: no detector panels");
     if (D->segmented && (!D->segmap || D->seg_nx < 1 || D->seg_ny < 1)) return xi_fail(XI_E_ARG, "predict: segmap");
     if (D->geo_x && (!D->geo_y || D->geo_nx < 1 || D->geo_ny < 1)) return xi_fail(XI_E_ARG, "predict: geo tables");
     if (P->hkl ? P->n_hkl < 0 : (P->hmax[0] < 0 || P->hmax[1] < 0 || P->hmax[2] < 0))
@@ -527,6 +533,13 @@ KnnWs knn_ws(const XiKnn* q, const KnnGrid& g, void* base) {
     w.cub = take(w.cub_bytes);
     w.bytes = o;
     return w;
+}
+
+__global__ void k_zero2(int* __restrict__ a, int* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        a[i] = 0;
+        b[i] = 0;
+    }
 }
 
 __device__ __forceinline__ int cell_axis(double v, double lo, double cs, int dim) {
@@ -727,7 +740,8 @@ int xi_plan_boxes(const XiBoxRules* B, const XiPlanDetector* D, const XiBoxOut* 
     if (B->n < 0) return xi_fail(XI_E_ARG, "xi_plan_boxes: negative size");
     if (B->n_xyb < 1 || B->n_xyb > 16) return xi_fail(XI_E_ARG, "xi_plan_boxes: side buckets");
     if (B->n_regions_xy < 1) return xi_fail(XI_E_ARG, "xi_plan_boxes: regions");
-    if (D->n_panels < 1 || !D->panels) return xi_fail(XI_E_ARG, "xi_plan_boxes: no detector panels");
+    if (D->n_panels < 1 || (!D->panels && D->n_panels > XI_PANELS_INLINE))
+        return xi_fail(XI_E_ARG, "xi_plan_boxes: no detector panels");
     if (D->segmented && !D->segmap) return xi_fail(XI_E_ARG, "xi_plan_boxes: segmap");
     if (B->n == 0) return XI_OK;
     const unsigned nb = (unsigned)((B->n + 255) / 256);
@@ -751,8 +765,9 @@ int xi_knn(const XiKnn* q, void* ws, size_t ws_bytes, int32_t* nbj, double* nbd,
     if (!nbj || !nbd) return xi_fail(XI_E_ARG, "xi_knn: null output");
     cudaStream_t s = (cudaStream_t)stream;
     const unsigned nb = (unsigned)((q->n + 255) / 256);
-    cudaMemsetAsync(w.count, 0, sizeof(int) * g.n_cells, s);
-    cudaMemsetAsync(w.fill, 0, sizeof(int) * g.n_cells, s);
+    // counters zeroed by a kernel: a memset could queue behind host-to-device transfers in the copy engine
+    const int64_t zb = (g.n_cells + 255) / 256;
+    k_zero2<<<(unsigned)(zb < 4096 ? zb : 4096), 256, 0, s>>>(w.count, w.fill, g.n_cells);
     k_knn_bin<<<nb, 256, 0, s>>>(*q, g, w.count, w.cell_of);
     size_t cb = w.cub_bytes;
     if (cub::DeviceScan::ExclusiveSum(w.cub, cb, w.count, w.start, (int)g.n_cells, s) != cudaSuccess)

@@ -12,6 +12,10 @@ neither read nor uploaded.
 """
 from __future__ import annotations
 
+import collections
+import threading
+import time
+
 import numpy as np
 import torch
 
@@ -43,6 +47,87 @@ class _Uploads:
 
 
 _UPLOADS = _Uploads()
+
+
+class _Feeder:
+    """Transfers the wedges of a run from pinned host memory ahead of the integration, from a thread of its own, on
+    a copy stream, starting before the plan is made. Each wedge goes in copies of `chunk` frames with at most `queued`
+    copies waiting in the copy engine (it serves copies in submission order, across streams), so a small copy the
+    integration issues meanwhile waits for little; at most `depth` wedges are held on the device."""
+
+    def __init__(self, host, first, wedges, oks, device, depth=4, chunk=2, queued=4):
+        self.host, self.first = host, first
+        self.wedges, self.oks = wedges, oks
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.ready = [threading.Event() for _ in wedges]
+        self.out = [None] * len(wedges)
+        self.held = [False] * len(wedges)   # the wedge took a slot
+        self.slots = threading.Semaphore(depth)
+        self.chunk, self.queued = chunk, queued
+        self.error = None
+        self.stopping = False
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _run(self):
+        try:
+            torch.cuda.set_device(self.device)
+            pend = collections.deque()
+            with torch.cuda.stream(self.stream):
+                for w, (fa, fb) in enumerate(self.wedges):
+                    if not self.oks[w].any():
+                        self.ready[w].set()
+                        continue
+                    self.slots.acquire()
+                    if self.stopping:
+                        break
+                    self.held[w] = True
+                    h = self.host[fa - self.first:fb - self.first + 1]
+                    d = torch.empty(h.shape, dtype=h.dtype, device=self.device)
+                    for c0 in range(0, h.shape[0], self.chunk):
+                        while len(pend) >= self.queued:
+                            ev0 = pend.popleft()
+                            while not ev0.query():       # polling lets the integration's thread run meanwhile
+                                time.sleep(2e-4)
+                        d[c0:c0 + self.chunk].copy_(h[c0:c0 + self.chunk], non_blocking=True)
+                        ev = torch.cuda.Event()
+                        ev.record(self.stream)
+                        pend.append(ev)
+                    self.out[w] = (d, pend[-1])
+                    self.ready[w].set()
+        except BaseException as e:          # surfaced by get()
+            self.error = e
+            for r in self.ready:
+                r.set()
+
+    def get(self, w):
+        """Wedge w on the device, ordered before the current stream's next work."""
+        self.ready[w].wait()
+        if self.error is not None:
+            raise RuntimeError("frame transfer failed") from self.error
+        d, ev = self.out[w]
+        self.out[w] = None
+        cur = torch.cuda.current_stream()
+        cur.wait_event(ev)
+        d.record_stream(cur)                 # no reuse of its memory before the current stream's kernels ran
+        return d
+
+    def done_with(self, w):
+        """The wedge's kernels are queued (or it was not needed): its slot may take the next wedge."""
+        self.ready[w].wait()
+        self.out[w] = None
+        if self.held[w]:
+            self.held[w] = False
+            self.slots.release()
+
+    def close(self):
+        self.stopping = True
+        for _ in range(len(self.wedges) + 1):
+            self.slots.release()
+        self.thread.join()
 
 
 class _PinnedRing:
@@ -86,6 +171,14 @@ class U32Frames:
 
     def _host_slice(self, a, b):
         return self.data[a - self.first:b - self.first + 1]
+
+    def feeder(self, wedges, oks):
+        """A transfer thread for the run's wedges when the frames are a pinned host tensor (None otherwise)."""
+        d = self.data
+        if self.on_device or not torch.is_tensor(d) or not d.is_pinned():
+            return None
+        h = d if d.dtype == torch.int32 else d.view(torch.int32)
+        return _Feeder(h, self.first, wedges, oks, self.device)
 
     def wedge(self, f_a, f_b, ok=None, stream=None):
         if self.on_device:

@@ -137,6 +137,26 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     if frames is None:
         frames = (src.first, src.last)
     f_first, f_last = int(frames[0]), int(frames[1])
+    excl = set(int(f) for f in exclude_frames)
+    # wedges of the run; frames in pinned host memory start moving to the device now, under the planning
+    resident = bool(getattr(src, "resident", False))
+    W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
+    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
+    oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in wedges]
+    feeder = src.feeder(wedges, oks) if (hasattr(src, "feeder") and not resident) else None
+    try:
+        return _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, block_edges, model, dmin,
+                          dmax, f_first, f_last, excl, mask, minimum_zeta, verbose, log, n_regions_xy,
+                          learn_profiles, adaptive, deconvolve_overlaps, bkg_template, foreign_spots, n_foreign,
+                          moments_only, device, allowed)
+    finally:
+        if feeder is not None:
+            feeder.close()
+
+
+def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, block_edges, model, dmin, dmax,
+               f_first, f_last, excl, mask, minimum_zeta, verbose, log, n_regions_xy, learn_profiles, adaptive,
+               deconvolve_overlaps, bkg_template, foreign_spots, n_foreign, moments_only, device, allowed):
     plan = plan_integration(exp_blocks, block_edges, model, dmin, dmax, (f_first, f_last), minimum_zeta,
                             n_regions_xy, adaptive, deconvolve_overlaps, lattice_of, foreign_spots, n_foreign, allowed)
     refl = plan.refl
@@ -158,7 +178,6 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     t_dev = 0.0
     nblocks = len(exp_blocks)
     blocks_rows = plan.blocks_refl                     # plan order (a launch groups its rows by shape itself)
-    excl = set(int(f) for f in exclude_frames)
     read = [f for f in range(f_first, f_last + 1) if f not in excl]
     read_fi = np.array([f - 1 for f in read], np.int64)
     # a block takes every frame read up to the first frame read at or after its last needed frame
@@ -271,10 +290,6 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
     # When frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1 at
     # once: it overlaps the transfer of the later wedges (their widths are fixed: every block before it has been
     # processed). Resident frames have no transfer to hide: their blocks run pass 1 whole, in the fewest launches.
-    resident = bool(getattr(src, "resident", False))
-    W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
-    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
-    oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in wedges]
     ok_parts = [ok.astype(np.uint8) for ok in oks if not ok.all()]
     ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
     early_rows = 0 if resident else EARLY_PASS1_ROWS
@@ -295,7 +310,7 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
             ok_t = ok_dev[ok_off:ok_off + ok.size]
             ok_off += ok.size
         if ok.any() and opened:
-            data, is_f = src.wedge(f, f_b, ok)
+            data, is_f = (feeder.get(w), False) if feeder is not None else src.wedge(f, f_b, ok)
             for b in open_order:
                 blk = opened.get(b)
                 if blk is None or w not in blk.w_gather:
@@ -304,6 +319,8 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
                 fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
                                      mask_t, ok_t[:nf] if ok_t is not None else None)
                 D.gather(fs, blk.grows, blk.sched(blk.w_gather[w]), blk.arena, blk.cnt)
+        if feeder is not None:
+            feeder.done_with(w)
         done = sorted((b for b in open_order if b in opened and eff_hi[b] <= fi_b),
                       key=lambda b: (eff_hi[b], open_order.index(b)))
         for b in done:

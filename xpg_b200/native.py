@@ -77,6 +77,7 @@ class XiSynthBackground(C.Structure):
 
 
 XI_PANEL_F64 = 28
+XI_PANELS_INLINE = 4
 XI_KNN_MAX = 16
 XI_KNN_NOALLOC_MAX_POINTS, XI_KNN_NOALLOC_MAX_CELLS = 1 << 19, 1 << 18
 _d3 = C.c_double * 3
@@ -88,7 +89,8 @@ class XiPlanDetector(C.Structure):
                 ("geo_ny", C.c_int), ("parallax", C.c_int), ("tsens", C.c_double), ("mu", C.c_double),
                 ("orgx", C.c_double), ("orgy", C.c_double), ("qx", C.c_double), ("qy", C.c_double),
                 ("distance", C.c_double), ("ed1", _d3), ("ed2", _d3), ("ed3", _d3), ("beam", _d3), ("pol_n", _d3),
-                ("pol_main", _d3), ("pol_f", C.c_double), ("nx", C.c_double), ("ny", C.c_double)]
+                ("pol_main", _d3), ("pol_f", C.c_double), ("nx", C.c_double), ("ny", C.c_double),
+                ("panel_inline", C.c_double * (4 * 28))]
 
 
 class XiPredict(C.Structure):

@@ -139,10 +139,15 @@ def plan_detector(g, device="cuda"):
         rec[k, 21], rec[k, 22], rec[k, 23] = P0[k] @ n, Bx[k] @ Bx[k], By[k] @ By[k]
         s = segs[min(k, len(segs) - 1)]
         rec[k, 24:28] = (s.x1, s.x2, s.y1, s.y2)
-    keep = {"panels": h2d(rec, None, device)}
     d = N.XiPlanDetector()
     d.n_panels = K
-    d.panels = N.ptr(keep["panels"])
+    keep = {}
+    if K <= N.XI_PANELS_INLINE:                 # carried in the kernel argument: no device copy
+        d.panel_inline[:K * N.XI_PANEL_F64] = [float(v) for v in rec.reshape(-1)]
+        d.panels = None
+    else:
+        keep["panels"] = h2d(rec, None, device)
+        d.panels = N.ptr(keep["panels"])
     if getattr(g, "segmented", False):
         m = np.asarray(g.segmap(), np.int16)
         keep["segmap"] = torch.as_tensor(m).to(device)
