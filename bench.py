@@ -340,21 +340,30 @@ def run(args):
         dist.destroy_process_group()
 
 
-def _ref_worker(args_tuple):
-    """Oracle work of one chunk of rows (spawned process): gather, pass 1, pass 2 from prepared frame crops."""
-    (prep, a, wz, payload, spec_d, nreg, origin) = args_tuple
+_REF = {}
+
+
+def _ref_init(prep, a, wz, spec_d, nreg, origin):
+    """Worker set-up (spawned process, once per pool): the prepared frame crops and the block constants."""
     from oracle import kernels as OK
-    from oracle import pipeline as OP
     from xpg_b200 import synth
     spec = synth.SweepSpec(**spec_d)
     g = spec.geometry()
-    det = OK.detector_consts(g, None)
     prof = np.repeat(OK.gaussian_profile()[None], nreg, 0)
-    prof = prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2)
-    OP.integrate_rows(prep, list(range(a, a + wz)), payload, det, g.s0.astype(np.float32), g.axis.astype(np.float32),
-                      np.float32(np.radians(g.z_to_phi(0.0))), np.float32(np.radians(g.osc)),
-                      np.radians(spec.sigma_d), np.radians(spec.sigma_m), 1.0, OK.rc_default_weights(), prof,
-                      origin=origin)
+    _REF.update(prep=prep, a=a, wz=wz, spec=spec, g=g, det=OK.detector_consts(g, None), origin=origin,
+                prof=prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2))
+
+
+def _ref_worker(payload):
+    """Oracle work of one chunk of rows: gather, pass 1, pass 2 from the worker's prepared frame crops."""
+    from oracle import kernels as OK
+    from oracle import pipeline as OP
+    r = _REF
+    g, spec = r["g"], r["spec"]
+    OP.integrate_rows(r["prep"], list(range(r["a"], r["a"] + r["wz"])), payload, r["det"], g.s0.astype(np.float32),
+                      g.axis.astype(np.float32), np.float32(np.radians(g.z_to_phi(0.0))), np.float32(np.radians(g.osc)),
+                      np.radians(spec.sigma_d), np.radians(spec.sigma_m), 1.0, OK.rc_default_weights(), r["prof"],
+                      origin=r["origin"])
     return len(payload)
 
 
@@ -390,18 +399,18 @@ def reference_arm(args):
     else:
         raw = synth.render_frames(spec, range(a + 1, a + wz + 1), table)
     prep = OP.prepared_frames(raw[:, y0:y0 + c, x0:x0 + c], a, spec.overload, [1])
-    per_step = max(cores * 4, 16)
+    per_step = max(cores * 24, 48)
     sd = asdict(spec)
     sd.pop("U", None)
     ctx = mp.get_context("spawn")
     n_done, t_all = 0, 0.0
-    with ctx.Pool(cores) as pool:
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(prep, a, wz, sd, p.nreg, (y0, x0))) as pool:
         def step(k):
             lo = (k * per_step) % max(rows_all.size - per_step, 1)
             rows = rows_all[lo:lo + per_step]
             chunks = [OP.row_payload(p, rows[i::cores]) for i in range(cores)]
             t0 = time.perf_counter()
-            n = sum(pool.map(_ref_worker, [(prep, a, wz, ch, sd, p.nreg, (y0, x0)) for ch in chunks if ch]))
+            n = sum(pool.map(_ref_worker, [ch for ch in chunks if ch]))
             t_rows = time.perf_counter() - t0
             t_prep = _frame_prep_seconds(raw[:1], spec.overload)
             return n, t_rows + t_prep * n_frames / p.n * n / cores
