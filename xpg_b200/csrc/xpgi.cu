@@ -71,19 +71,21 @@ __device__ __forceinline__ NbTab nb_tab(unsigned char* base, int K, int max_bx, 
 __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const float* xs, const float* ys,
                                 const float* zzs, bool skip_first, NbShared& nb, const NbTab& tb) {
     const int K = R.K;
-    if (threadIdx.x == 0) {
-        int n = 0;
-        for (int k = 0; k < K; ++k) {
-            if (k == 0 && skip_first) continue;
+    if (threadIdx.x < 32) {                  // warp 0: lane k tests neighbour column k, then the passing columns are
+        const int k = threadIdx.x;           // listed in column order
+        bool on = false;
+        if (k < K && !(k == 0 && skip_first)) {
             float nx_ = R.nbx[(size_t)row * K + k], ny_ = R.nby[(size_t)row * K + k];
             float nz_ = R.nbz[(size_t)row * K + k];
             float sx = R.nbsx[(size_t)row * K + k], sz = R.nbsz[(size_t)row * K + k];
             float mx = (fminf(fmaxf(nx_, xs[0]), xs[bx - 1]) - nx_) / sx;
             float my = (fminf(fmaxf(ny_, ys[0]), ys[bx - 1]) - ny_) / sx;
             float mz = (fminf(fmaxf(nz_, zzs[0]), zzs[Dz - 1]) - nz_) / sz;
-            if ((mx * mx + my * my) + mz * mz < 1.0f) nb.act[n++] = k;
+            on = (mx * mx + my * my) + mz * mz < 1.0f;
         }
-        nb.nact = n;
+        const unsigned ball = __ballot_sync(0xffffffffu, on);
+        if (on) nb.act[__popc(ball & ((1u << k) - 1u))] = k;
+        if (k == 0) nb.nact = __popc(ball);
     }
     __syncthreads();
     for (int a = 0; a < nb.nact; ++a) {
@@ -103,11 +105,28 @@ __device__ void neighbour_setup(const XiRows& R, int row, int Dz, int bx, const 
         }
     }
     __syncthreads();
-    for (int a = threadIdx.x; a < nb.nact; a += blockDim.x) {
-        int zm = 0;
-        for (int z = 1; z < Dz; ++z)
-            if (tb.z2(a)[z] < tb.z2(a)[zm]) zm = z;
-        nb.zmin[a] = zm;
+    // frame of each neighbour's smallest dz^2 (the first such frame): one warp per neighbour
+    {
+        const int lane = threadIdx.x & 31;
+        for (int a = threadIdx.x >> 5; a < nb.nact; a += blockDim.x >> 5) {
+            const float* d2 = tb.z2(a);
+            float best = d2[0];
+            int bz = 0;
+            for (int z = lane; z < Dz; z += 32)
+                if (d2[z] < best || (z < bz && d2[z] == best)) {
+                    best = d2[z];
+                    bz = z;
+                }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oz = __shfl_down_sync(0xffffffffu, bz, o);
+                if (ov < best || (ov == best && oz < bz)) {
+                    best = ov;
+                    bz = oz;
+                }
+            }
+            if (lane == 0) nb.zmin[a] = bz;
+        }
     }
     __syncthreads();
 }
@@ -437,17 +456,20 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         }
         if (threadIdx.x == 0) s_nfgl = base;
     }
-    // foreground frames: R >= 1e-3 * Rmax + 1e-6
-    if (threadIdx.x == 0) {
+    // foreground frames: R >= 1e-3 * Rmax + 1e-6 (warp 0: max by shuffles, the mask by ballots)
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         float Rmax = fR[0];
-        for (int z = 1; z < Dz; ++z) Rmax = fmaxf(Rmax, fR[z]);
+        for (int z = lane; z < Dz; z += 32) Rmax = fmaxf(Rmax, fR[z]);
+        for (int o = 16; o > 0; o >>= 1) Rmax = fmaxf(Rmax, __shfl_xor_sync(0xffffffffu, Rmax, o));
         const float thr = 1e-3f * Rmax + 1e-6f;
-        Mask65 m;
-        m.clear();
-        for (int z = 0; z < Dz; ++z)
-            if (fR[z] >= thr) m.set(z);
-        s_fgz_lo = m.lo;
-        s_fgz_hi = m.hi;
+        const unsigned w0 = __ballot_sync(0xffffffffu, lane < Dz && fR[lane] >= thr);
+        const unsigned w1 = __ballot_sync(0xffffffffu, lane + 32 < Dz && fR[lane + 32] >= thr);
+        const unsigned w2 = __ballot_sync(0xffffffffu, lane + 64 < Dz && fR[lane + 64] >= thr);
+        if (lane == 0) {
+            s_fgz_lo = (unsigned long long)w0 | ((unsigned long long)w1 << 32);
+            s_fgz_hi = w2 & 1u;
+        }
     }
     neighbour_setup(R, row, Dz, bx, xs, ys, fzz, false, nb, tb);     // ends with a barrier
     pixel_tables(det, nb, tb, bx, Dz, xs, ys, nblo, nbhi, brefs);
