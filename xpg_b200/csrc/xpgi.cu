@@ -261,7 +261,7 @@ __device__ void pixel_tables(const XiDetector& det, const NbShared& nb, const Nb
         const int i = p % bx, j = p / bx;
         const Mask65 m = neighbour_frames(nb, tb, i, j, Dz);
         nblo[p] = m.lo;
-        nbhi[p] = m.hi;
+        if (nbhi) nbhi[p] = m.hi;
         brefs[p] = bkg_ref(det, xs[i], ys[j]);
     }
     __syncthreads();
@@ -794,10 +794,17 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
 // pass 2
 // ==================================================================================================================
 // Dynamic shared memory: nblo (8P, first the partner's eps1 / eps2) | P2s (4P) | P2ps (4P) | brefs (4P, first the
-// partner's J) | nbhi (4P) | staged net counts of the fitted voxels (4V, when STAGED).
-__host__ __device__ inline size_t pass2_pix_bytes(int P) { return ((size_t)24 * P + 15) / 16 * 16; }
-__host__ __device__ inline size_t pass2_stage_offset(int P, int cap) {
-    return (pass2_pix_bytes(P) + (size_t)8 * cap + 15) / 16 * 16;
+// partner's J) | nbhi (4P; only when boxes reach frame 64, whose bit it holds) | fit list (8 x cap, first the
+// rocking-curve terms) | staged net counts of the fitted voxels (4V, when STAGED).
+__host__ __device__ inline size_t pass2_pix_bytes(int P, int max_dz) {
+    return ((size_t)(max_dz > 64 ? 24 : 20) * P + 15) / 16 * 16;
+}
+__host__ __device__ inline size_t pass2_list_bytes(int cap) {
+    const size_t b = (size_t)8 * cap, t = (size_t)XI_MAX_DZ * XI_RC_K * sizeof(float);
+    return ((b > t ? b : t) + 15) / 16 * 16;
+}
+__host__ __device__ inline size_t pass2_stage_offset(int P, int max_dz, int cap) {
+    return pass2_pix_bytes(P, max_dz) + pass2_list_bytes(cap);
 }
 
 template <int NT, bool STAGED>
@@ -811,7 +818,6 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     __shared__ int s_nlist;
     __shared__ float xs[XI_MAX_BX], ys[XI_MAX_BX];
     __shared__ float fR[XI_MAX_DZ], fRp[XI_MAX_DZ], fzz[XI_MAX_DZ];
-    __shared__ float terms[XI_MAX_DZ * XI_RC_K];
     __shared__ NbShared nb;
     __shared__ float s_e1[3], s_e2[3], s_S[3], s_zetap, s_seffp;
     __shared__ float s_I, s_Ip, s_pmax, s_ppmax;
@@ -836,11 +842,12 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     float* P2ps = P2s + Pm;
     float* brefs = P2ps + Pm;
     float* Jps = brefs;                                   // partner J, before brefs is written
-    unsigned* nbhi = reinterpret_cast<unsigned*>(brefs + Pm);
-    float* ul_v = reinterpret_cast<float*>(dyn2 + pass2_pix_bytes(Pm));      // fit list: net counts
+    unsigned* nbhi = max_dz > 64 ? reinterpret_cast<unsigned*>(brefs + Pm) : nullptr;   // frame 64's bit
+    float* ul_v = reinterpret_cast<float*>(dyn2 + pass2_pix_bytes(Pm, max_dz));      // fit list: net counts
+    float* terms = ul_v;                                  // rocking-curve terms, before the fit list is written
     unsigned* ul_i = reinterpret_cast<unsigned*>(ul_v + cap);                 // fit list: z << 16 | pixel
-    float* stage = reinterpret_cast<float*>(dyn2 + pass2_stage_offset(Pm, cap));   // 16-byte aligned
-    const NbTab tb = nb_tab(dyn2 + pass2_stage_offset(Pm, cap) + (STAGED ? ((size_t)Pm * max_dz * 4 + 15) / 16 * 16 : 0),
+    float* stage = reinterpret_cast<float*>(dyn2 + pass2_stage_offset(Pm, max_dz, cap));   // 16-byte aligned
+    const NbTab tb = nb_tab(dyn2 + pass2_stage_offset(Pm, max_dz, cap) + (STAGED ? ((size_t)Pm * max_dz * 4 + 15) / 16 * 16 : 0),
                             R.K, max_bx, max_dz);
     const int pxs = R.pxs ? R.pxs[row] : 1;
     const int ix0 = R.ix0[row], iy0 = R.iy0[row], iz0 = R.iz0[row];
@@ -981,7 +988,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                 const unsigned long long nl = nblo[p];
                 nbw[0] = (unsigned)nl;
                 nbw[1] = (unsigned)(nl >> 32);
-                nbw[2] = nbhi[p];
+                nbw[2] = nbhi ? nbhi[p] : 0u;
             }
             const float bpix = bg * bref;
             const float iv0 = __frcp_rn(gain * fmaxf(bpix, kVarFloor));
@@ -1046,7 +1053,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                 if (fg2) a8[4] += (double)P2 * r_fg;
                 if (STAGED) {                    // the neighbour mask is not needed any more: keep the fit mask
                     nblo[p] = (unsigned long long)umw[0] | ((unsigned long long)umw[1] << 32);
-                    nbhi[p] = umw[2];
+                    if (nbhi) nbhi[p] = umw[2];
                 }
             }
         }
@@ -1082,7 +1089,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
             const float P2 = P2s[p], P2p = P2ps[p];
             Mask65 nbm;
             nbm.lo = nblo[p];
-            nbm.hi = nbhi[p];
+            nbm.hi = nbhi ? nbhi[p] : 0u;
             for (int z = 0; z < Dz; ++z) {
                 if (STAGED) {
                     if (!nbm.get(z)) continue;   // fit mask
@@ -1448,7 +1455,7 @@ template <int NT, bool STAGED>
 int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, const float* prof,
                  const XiPass2In* in, XiPass2Out* O, cudaStream_t s, int nblk, int cap) {
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    size_t sm = pass2_stage_offset((int)P, cap) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0) +
+    size_t sm = pass2_stage_offset((int)P, R->max_dz, cap) + (STAGED ? (P * R->max_dz * sizeof(float) + 15) / 16 * 16 : 0) +
                 nb_bytes(R->K, R->max_bx, R->max_dz);
     cudaFuncSetAttribute(k_pass2<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     cudaFuncSetAttribute(k_pass2<NT, STAGED>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1541,16 +1548,16 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     cudaStream_t s = (cudaStream_t)stream;
     const size_t P = (size_t)R->max_bx * R->max_bx;
     const size_t V = P * R->max_dz;
-    if (pass2_pix_bytes((int)P) > kStageBudget)
-        return fail(XI_E_LIMIT, "xi_pass2: box side above 89 pixels (per-pixel tables exceed shared memory)");
+    if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > kStageBudget)
+        return fail(XI_E_LIMIT, "xi_pass2: box too large (per-pixel tables exceed shared memory)");
     // the fit list holds up to every voxel of small boxes and 2048 fitted voxels of large ones; the box itself is
     // staged only when small (it is read once: staging buys the copy's overlap with the set-up, not re-reads)
     // (the list shrinks to what shared memory leaves beside the tables; rows whose list overflows fit from the box)
-    const size_t fit = (kStageBudget - pass2_pix_bytes((int)P)) / 8 / 4 * 4;
+    const size_t fit = (kStageBudget - pass2_pix_bytes((int)P, R->max_dz)) / 8 / 4 * 4;
     size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
     if (capz > fit) capz = fit;
     const int cap = (int)capz;
-    const size_t base = pass2_stage_offset((int)P, cap);
+    const size_t base = pass2_stage_offset((int)P, R->max_dz, cap);
     if (base > kStageBudget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
     const bool staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= kStageBudget;
     if (staged) {
