@@ -10,7 +10,9 @@ stack (~34 GB) is far larger than L2, so no flush is needed between steps.
 
   value  reflections integrated per second with the frames resident in HBM (device-timed, CUDA events, max over
          ranks), whole job over all ranks;
-  e2e    the same with the frames in pinned host memory, uploaded inside every step;
+  e2e    the same with the frames in pinned host memory, uploaded inside every step (the transfer thread sends
+         each 2-frame chunk raw or packed to one byte a pixel on the host's cores, whichever keeps the link busy;
+         h2d_bytes_per_step counts the bytes that crossed);
   roofline  of the dominant kernel (largest share of device time): algorithmic bytes per launch / live CUDA-event
          launch duration, against the measured HBM copy bandwidth;
   cpu_baseline  the oracle (numpy restatement of the reference's CPU path) on a bounded sample of the same block.
@@ -308,6 +310,7 @@ def run(args):
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         k2 = max(1, min(args.steps, args.e2e_steps))
+        moved0 = dict(hsrc.transfer)
         f0.record()
         for _ in range(k2):
             res = blk.integrate(hsrc)
@@ -315,8 +318,12 @@ def run(args):
         torch.cuda.synchronize()
         te, _ = reduce_over_ranks(f0.elapsed_time(f1) * 1e-3, 0, dist)
         n_out = sum(v.nbytes for v in res.refl.values() if isinstance(v, np.ndarray))
+        moved = {k: (hsrc.transfer.get(k, 0) - moved0.get(k, 0)) / k2 for k in ("h2d_bytes", "chunks_raw",
+                                                                                 "chunks_packed")}
         e2e = {"value": round(blk.n_refl * world * k2 / te, 1), "unit": UNIT,
-               "h2d_bytes_per_step": int(host.numel() * 4), "d2h_bytes_per_step": int(n_out), "steps": k2}
+               "h2d_bytes_per_step": int(moved["h2d_bytes"]), "d2h_bytes_per_step": int(n_out), "steps": k2,
+               "frame_bytes_per_step": int(host.numel() * 4),
+               "chunks_per_step": {"raw": moved["chunks_raw"], "packed": moved["chunks_packed"]}}
         del host
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

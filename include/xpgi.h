@@ -337,6 +337,27 @@ int xi_rocking_gram(const XiRocking *q, double sm, void *ws, size_t ws_bytes, do
 #define XI_KNN_NOALLOC_MAX_CELLS (1 << 18)
 int xi_knn_noalloc(const XiKnn *q, int32_t *nbj, double *nbd, void *stream);
 
+/* ---- Transfer encoding of uint32 frames --------------------------------------------------------------------------
+ * No counterpart in XPG, which reads and decodes frames on the host (xpg/io/images.py:72-102). Raw uint32 frames
+ * (Eiger-style: 0xFFFFFFFF flagged) are mostly small counts, so they cross the host-device link as one byte per
+ * pixel plus exceptions and are widened back on the device, bit for bit:
+ *   plane[i] = v for v < XI_PACK_ESCAPE, XI_PACK_FLAGGED for v = 0xFFFFFFFF, XI_PACK_ESCAPE otherwise;
+ *   exc = (index, value) uint32 pairs of every pixel coded XI_PACK_ESCAPE, in increasing index order. */
+#define XI_PACK_ESCAPE 254u
+#define XI_PACK_FLAGGED 255u
+#define XI_PACK_MAX_PIXELS 0xFFFFFFFFll   /* pixels per packed run (exception indices are uint32) */
+
+/* Host function (no CUDA call): packs n pixels of host memory src into plane (n bytes) and exc (room for exc_cap
+ * pairs), on `threads` host threads (0: the library's choice) of a pool kept by the library; *n_exc gets the number
+ * of pairs. Fails with XI_E_LIMIT when more than exc_cap pixels need an exception (plane and exc then hold partial
+ * output; send the run unpacked). Calls from several host threads are serialised. */
+int xi_pack_u8(const uint32_t *src, int64_t n, uint8_t *plane, uint32_t *exc, int64_t exc_cap, int threads,
+               int64_t *n_exc);
+
+/* Widens a packed run on the device: out[i] (n uint32) from plane (n bytes) and the n_exc pairs at exc (all three
+ * device memory; plane and out 16-byte aligned). */
+int xi_unpack_u8(const uint8_t *plane, int64_t n, const uint32_t *exc, int64_t n_exc, uint32_t *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

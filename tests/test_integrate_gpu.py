@@ -132,6 +132,40 @@ def test_results_independent_of_schedule(case, monkeypatch):
         assert np.array_equal(np.asarray(a[k]), np.asarray(e[k]), equal_nan=True), ("thread + early pass 1", k)
 
 
+@pytest.mark.parametrize("mode", ["packed", "exceptions_overflow"])
+def test_packed_transfer_identical(mode, monkeypatch):
+    """Frames uploaded packed to one byte a pixel (xi_pack_u8 on the host, xi_unpack_u8 on the device) give the
+    results of the same frames resident in device memory, bit for bit: with counts planted at and around the byte
+    codes' limits (253-256, 2^16, the overload threshold, 0xFFFFFFFE, flagged), and with a chunk holding more
+    exception pixels than the exception list takes (that chunk is sent raw)."""
+    import torch
+    from xpg_b200 import frames as FR
+    case = "binned"
+    spec = G.case_inputs(case)[0]
+    raw = G.frames_of(case).copy()
+    rng = np.random.default_rng(7)
+    n_f, ny, nx = raw.shape
+    fixed = np.array([253, 254, 255, 256, 1 << 16, spec.overload - 1, spec.overload, 0xFFFFFFFE, 0xFFFFFFFF],
+                     np.uint32)
+    for f in range(n_f):
+        iy, ix = rng.integers(0, ny, 40), rng.integers(0, nx, 40)
+        raw[f, iy, ix] = np.where(raw[f, iy, ix] == 0xFFFFFFFF, raw[f, iy, ix], rng.choice(fixed, 40))
+    if mode == "exceptions_overflow":
+        iy, ix = rng.integers(0, ny, 4000), rng.integers(0, nx, 4000)
+        raw[1, iy, ix] = np.where(raw[1, iy, ix] == 0xFFFFFFFF, raw[1, iy, ix], 300)
+        monkeypatch.setattr(FR, "PACK_EXC_PER_PIXEL", 0.0)       # the list takes 1024 pairs per chunk
+    monkeypatch.setattr(FR, "PACK_MIN_BACKLOG", 0.0)              # pack every chunk the list allows
+    resident = FR.U32Frames(torch.as_tensor(raw.view(np.int32)).cuda(), first=1, overload=spec.overload)
+    a = _run(case, images=resident).refl
+    src = FR.U32Frames(torch.as_tensor(raw.view(np.int32)).pin_memory(), first=1, overload=spec.overload)
+    b = _run(case, images=src, wedge_frames=5).refl
+    assert src.transfer["chunks_packed"] > 0
+    if mode == "exceptions_overflow":
+        assert src.transfer["chunks_raw"] > 0
+    for k in CHECK_F + ("n_over", "n_fg_masked"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), (mode, k)
+
+
 def test_estimate_sigmas_matches_reference():
     from xpg_b200 import frames as FR
     from xpg_b200.integrate import estimate_sigmas

@@ -1,0 +1,69 @@
+// Device side of the frames' transfer encoding (include/xpgi.h, "Transfer encoding"): one byte per pixel widened to
+// uint32, then the exception pairs written over the escaped pixels. A CTA widens a span of kSpan pixels with 16-byte
+// loads and stores, then writes the exceptions inside its span (found by a binary search of the sorted indices), so
+// every pixel is written by one CTA, the exceptions after the byte codes.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpgi.h"
+#include "xpgi_internal.h"
+
+namespace {
+
+constexpr int kNT = 256;
+constexpr int64_t kSpan = (int64_t)kNT * 16 * 4;   // pixels per CTA: four 16-byte plane loads per thread
+
+__device__ __forceinline__ uint32_t widen(uint32_t b) { return b == XI_PACK_FLAGGED ? 0xFFFFFFFFu : b; }
+
+__global__ void __launch_bounds__(kNT) k_unpack_u8(const uint8_t* __restrict__ plane, int64_t n,
+                                                   const uint32_t* __restrict__ exc, int64_t n_exc,
+                                                   uint32_t* __restrict__ out) {
+    const int64_t a = (int64_t)blockIdx.x * kSpan;
+    const int64_t b = a + kSpan < n ? a + kSpan : n;
+    for (int64_t p = a + (int64_t)threadIdx.x * 16; p < b; p += (int64_t)kNT * 16) {
+        if (p + 16 <= b) {
+            const uint4 v = *reinterpret_cast<const uint4*>(plane + p);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+            uint4* o = reinterpret_cast<uint4*>(out + p);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                o[q] = make_uint4(widen(w[q] & 0xFFu), widen((w[q] >> 8) & 0xFFu), widen((w[q] >> 16) & 0xFFu),
+                                  widen(w[q] >> 24));
+        } else {
+            for (int64_t i = p; i < b; ++i) out[i] = widen(plane[i]);
+        }
+    }
+    if (n_exc == 0) return;
+    __syncthreads();                         // the byte codes of the span are written before the exceptions
+    __shared__ int64_t s_lo;
+    if (threadIdx.x == 0) {                  // first exception with index >= a
+        int64_t lo = 0, hi = n_exc;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((int64_t)exc[2 * mid] < a) lo = mid + 1;
+            else hi = mid;
+        }
+        s_lo = lo;
+    }
+    __syncthreads();
+    for (int64_t k = s_lo + threadIdx.x; k < n_exc; k += kNT) {
+        const int64_t i = exc[2 * k];
+        if (i >= b) break;
+        out[i] = exc[2 * k + 1];
+    }
+}
+
+}  // namespace
+
+extern "C" int xi_unpack_u8(const uint8_t* plane, int64_t n, const uint32_t* exc, int64_t n_exc, uint32_t* out,
+                            void* stream) {
+    if (n < 0 || n_exc < 0 || (n && (!plane || !out)) || (n_exc && !exc))
+        return xi_fail(XI_E_ARG, "xi_unpack_u8: null pointer or negative size");
+    if (n > XI_PACK_MAX_PIXELS) return xi_fail(XI_E_LIMIT, "xi_unpack_u8: more than XI_PACK_MAX_PIXELS pixels");
+    if (((uintptr_t)plane & 15) || ((uintptr_t)out & 15) || ((uintptr_t)exc & 3))
+        return xi_fail(XI_E_ARG, "xi_unpack_u8: plane and out must be 16-byte aligned");
+    if (n == 0) return XI_OK;
+    const int64_t grid = (n + kSpan - 1) / kSpan;
+    k_unpack_u8<<<(unsigned)grid, kNT, 0, (cudaStream_t)stream>>>(plane, n, exc, n_exc, out);
+    return xi_cuda_check("xi_unpack_u8");
+}
