@@ -358,6 +358,13 @@ int xi_pack_u8(const uint32_t *src, int64_t n, uint8_t *plane, uint32_t *exc, in
  * device memory; plane and out 16-byte aligned). */
 int xi_unpack_u8(const uint8_t *plane, int64_t n, const uint32_t *exc, int64_t n_exc, uint32_t *out, void *stream);
 
+/* Copies `bytes` from page-locked host memory (cudaHostAlloc / cudaHostRegister, mapped into the device's address
+ * space) to device memory with a kernel that reads the host memory over the link: unlike cudaMemcpyAsync it does not
+ * queue behind the copies already waiting in the copy engine (the frame chunks), so a small upload is not delayed by
+ * them. Fails with XI_E_ARG when src is not mapped page-locked host memory (checked with cudaPointerGetAttributes
+ * before any launch). No counterpart in XPG (its arrays stay on the host). */
+int xi_upload(const void *src, void *dst, int64_t bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -154,16 +154,23 @@ def test_packed_transfer_identical(mode, monkeypatch):
         iy, ix = rng.integers(0, ny, 4000), rng.integers(0, nx, 4000)
         raw[1, iy, ix] = np.where(raw[1, iy, ix] == 0xFFFFFFFF, raw[1, iy, ix], 300)
         monkeypatch.setattr(FR, "PACK_EXC_PER_PIXEL", 0.0)       # the list takes 1024 pairs per chunk
-    monkeypatch.setattr(FR, "PACK_MIN_BACKLOG", 0.0)              # pack every chunk the list allows
     resident = FR.U32Frames(torch.as_tensor(raw.view(np.int32)).cuda(), first=1, overload=spec.overload)
     a = _run(case, images=resident).refl
-    src = FR.U32Frames(torch.as_tensor(raw.view(np.int32)).pin_memory(), first=1, overload=spec.overload)
-    b = _run(case, images=src, wedge_frames=5).refl
+    pinned = torch.as_tensor(raw.view(np.int32)).pin_memory()
+    src = FR.U32Frames(pinned, first=1, overload=spec.overload)
+    b = _run(case, images=src, wedge_frames=5).refl                # both transfer threads
     assert src.transfer["chunks_packed"] > 0
+    monkeypatch.setattr(FR, "RAW_THREAD", False)                  # pack every chunk the exception list allows
+    only = FR.U32Frames(pinned, first=1, overload=spec.overload)
+    c = _run(case, images=only, wedge_frames=5).refl
+    n_chunks = only.transfer["chunks_packed"] + only.transfer["chunks_raw"]
     if mode == "exceptions_overflow":
-        assert src.transfer["chunks_raw"] > 0
+        assert only.transfer["chunks_raw"] == 1 and only.transfer["chunks_packed"] == n_chunks - 1
+    else:
+        assert only.transfer["chunks_raw"] == 0 and n_chunks > 0
     for k in CHECK_F + ("n_over", "n_fg_masked"):
-        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), (mode, k)
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), (mode, "two threads", k)
+        assert np.array_equal(np.asarray(a[k]), np.asarray(c[k]), equal_nan=True), (mode, "packed", k)
 
 
 def test_estimate_sigmas_matches_reference():

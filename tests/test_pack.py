@@ -83,3 +83,41 @@ def test_unpack_round_trip(n):
     native.check(rc, "xi_unpack_u8")
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy().view(np.uint32), src)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,off", [(1, 0), (15, 1), (16, 0), (4099, 3), (1 << 20, 0), (3 * (1 << 20) + 7, 5)])
+def test_upload_round_trip(n, off):
+    """xi_upload copies from page-locked host memory at any offset and length, bit for bit."""
+    import torch
+    lib = native.load()
+    host = torch.randint(0, 256, (n + off,), dtype=torch.uint8).pin_memory()
+    out = torch.zeros(n + 16, dtype=torch.uint8, device="cuda")
+    rc = lib.xi_upload(C.c_void_p(host.data_ptr() + off), C.c_void_p(out.data_ptr() + (off & 1)), n,
+                       native.stream_handle())
+    native.check(rc, "xi_upload")
+    torch.cuda.synchronize()
+    assert torch.equal(out[(off & 1):(off & 1) + n].cpu(), host[off:off + n])
+
+
+@pytest.mark.gpu
+def test_upload_rejects_pageable_memory():
+    import torch
+    lib = native.load()
+    src = np.arange(64, dtype=np.uint8)                     # pageable: refused before any launch
+    out = torch.zeros(64, dtype=torch.uint8, device="cuda")
+    assert lib.xi_upload(src.ctypes.data, native.ptr(out), 64, native.stream_handle()) == native.XI_E_ARG
+
+
+@pytest.mark.gpu
+def test_h2d_ring_wraps():
+    """The upload ring gives every upload its own bytes while regions are reused (more than the ring's size in
+    flight across a run of uploads)."""
+    import torch
+    from xpg_b200 import device as D
+    rng = np.random.default_rng(5)
+    arrays = [rng.integers(0, 1 << 30, size=int(rng.integers(1, 3 << 20)), dtype=np.int64) for _ in range(40)]
+    outs = [D.h2d(a) for a in arrays]
+    torch.cuda.synchronize()
+    for a, o in zip(arrays, outs):
+        assert np.array_equal(o.cpu().numpy(), a)

@@ -57,16 +57,17 @@ def fit_rocking_width(sel_fit, g, sm_guess, lo_fac=0.2, hi_fac=3.0):
     sel_fit: list of (fz (n, 65), iz0, phi (deg), zeta) with fz a host array or a device tensor."""
     import torch
     from . import native as N
-    from .device import TIMER
+    from .device import TIMER, h2d
     Fs = [torch.as_tensor(s[0], dtype=torch.float64) for s in sel_fit]
     dev = next((f.device for f in Fs if f.is_cuda), torch.device("cuda"))
-    F = torch.cat([f.to(dev) for f in Fs]) if Fs else torch.zeros((0, MAX_DZ), dtype=torch.float64, device=dev)
+    F = (torch.cat([f if f.is_cuda else h2d(f.numpy(), None, dev) for f in Fs]) if Fs
+         else torch.zeros((0, MAX_DZ), dtype=torch.float64, device=dev))
     iz0 = np.concatenate([s[1] for s in sel_fit]) if sel_fit else np.zeros(0, np.int32)
     phi = np.concatenate([s[2] for s in sel_fit]) if sel_fit else np.zeros(0)
     zeta = np.concatenate([s[3] for s in sel_fit]) if sel_fit else np.zeros(0)
     grid = sm_guess * np.exp(np.linspace(np.log(lo_fac), np.log(hi_fac), 61))
     q, keep = _rocking_struct(F, iz0, phi, zeta, g)
-    grid_t = torch.as_tensor(grid, dtype=torch.float64).to(dev)
+    grid_t = h2d(np.asarray(grid, np.float64), None, dev)
     cost_t = torch.empty(len(grid), dtype=torch.float64, device=dev)
     lib = N.load()
     with TIMER.span("adapt"):

@@ -1,4 +1,6 @@
-// Device side of the frames' transfer encoding (include/xpgi.h, "Transfer encoding"): one byte per pixel widened to
+// Device side of the frames' transfer encoding (include/xpgi.h, "Transfer encoding"), and xi_upload (small uploads
+// read by a kernel from mapped page-locked host memory).
+// The unpacking: one byte per pixel widened to
 // uint32, then the exception pairs written over the escaped pixels. A CTA widens a span of kSpan pixels with 16-byte
 // loads and stores, then writes the exceptions inside its span (found by a binary search of the sorted indices), so
 // every pixel is written by one CTA, the exceptions after the byte codes.
@@ -53,7 +55,40 @@ __global__ void __launch_bounds__(kNT) k_unpack_u8(const uint8_t* __restrict__ p
     }
 }
 
+// byte copy from mapped host memory; the 16-byte body when both ends are 16-byte aligned, bytes otherwise
+__global__ void __launch_bounds__(kNT) k_upload(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
+                                                int64_t bytes, int vec) {
+    const int64_t stride = (int64_t)gridDim.x * kNT;
+    const int64_t t0 = (int64_t)blockIdx.x * kNT + threadIdx.x;
+    int64_t done = 0;
+    if (vec) {
+        const int64_t n16 = bytes >> 4;
+        for (int64_t i = t0; i < n16; i += stride)
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+        done = n16 << 4;
+    }
+    for (int64_t i = done + t0; i < bytes; i += stride) dst[i] = src[i];
+}
+
 }  // namespace
+
+extern "C" int xi_upload(const void* src, void* dst, int64_t bytes, void* stream) {
+    if (bytes < 0 || (bytes && (!src || !dst))) return xi_fail(XI_E_ARG, "xi_upload: null pointer or negative size");
+    if (bytes == 0) return XI_OK;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, src) != cudaSuccess) {
+        cudaGetLastError();
+        return xi_fail(XI_E_ARG, "xi_upload: src is not page-locked host memory");
+    }
+    if (at.type != cudaMemoryTypeHost || !at.devicePointer)
+        return xi_fail(XI_E_ARG, "xi_upload: src is not mapped page-locked host memory");
+    const uint8_t* s = static_cast<const uint8_t*>(at.devicePointer);
+    const int vec = !((uintptr_t)s & 15) && !((uintptr_t)dst & 15);
+    int64_t grid = (bytes / (vec ? 16 : 1) + kNT - 1) / kNT;
+    grid = grid < 1 ? 1 : (grid > 1184 ? 1184 : grid);          // 8 CTAs per SM at most
+    k_upload<<<(unsigned)grid, kNT, 0, (cudaStream_t)stream>>>(s, static_cast<uint8_t*>(dst), bytes, vec);
+    return xi_cuda_check("xi_upload");
+}
 
 extern "C" int xi_unpack_u8(const uint8_t* plane, int64_t n, const uint32_t* exc, int64_t n_exc, uint32_t* out,
                             void* stream) {

@@ -2,6 +2,7 @@
 // plus (index, value) exceptions, on a pool of host threads. The work is a streaming read of the frames, so the pool
 // splits a run into slices of kSlice pixels handed out in order; each slice records which of its kBlock-pixel
 // blocks hold an exception, and the calling thread lists those blocks' exceptions afterwards, in pixel order.
+#include <immintrin.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -33,6 +34,19 @@ uint32_t pack_block(const uint32_t* __restrict__ s, uint8_t* __restrict__ d, int
         esc |= big & (flagged ^ 1u);
     }
     return esc;
+}
+
+// a block's codes go through a cache-resident buffer to the plane with streaming stores: the plane is read next by
+// the copy engine, not by this core, so its cache lines are not fetched first (32-byte aligned, whole blocks only)
+__attribute__((target("avx2"))) void stream_copy(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, int64_t m) {
+    for (int64_t i = 0; i < m; i += 32)
+        _mm256_stream_si256(reinterpret_cast<__m256i*>(d + i),
+                            _mm256_load_si256(reinterpret_cast<const __m256i*>(s + i)));
+}
+
+bool have_avx2() {
+    static const bool ok = __builtin_cpu_supports("avx2");
+    return ok;
 }
 
 class Pool {
@@ -117,8 +131,10 @@ Pool& pool() {
 }
 
 int default_threads() {
+    // the packing is bound by the host's memory bandwidth well before every core is busy: leave cores to the
+    // threads that launch the kernels and issue the raw copies
     const unsigned hc = std::thread::hardware_concurrency();
-    return hc > 2 ? (int)hc - 2 : 1;      // leave a core to the thread that launches the kernels
+    return hc > 5 ? (int)hc - 4 : 1;
 }
 
 }  // namespace
@@ -136,10 +152,18 @@ extern "C" int xi_pack_u8(const uint32_t* src, int64_t n, uint8_t* plane, uint32
     const int64_t n_items = (n + kSlice - 1) / kSlice;
     pool().run(n_items, threads, [&](int64_t it) {
         const int64_t a = it * kSlice, b = std::min(n, a + kSlice);
+        alignas(64) uint8_t buf[kBlock];
+        const bool stream = have_avx2() && ((uintptr_t)plane & 31) == 0;
         for (int64_t p = a; p < b; p += kBlock) {
             const int64_t m = std::min(kBlock, b - p);
-            flag[(size_t)(p / kBlock)] = (uint8_t)pack_block(src + p, plane + p, m);
+            if (stream && m == kBlock) {
+                flag[(size_t)(p / kBlock)] = (uint8_t)pack_block(src + p, buf, m);
+                stream_copy(plane + p, buf, m);
+            } else {
+                flag[(size_t)(p / kBlock)] = (uint8_t)pack_block(src + p, plane + p, m);
+            }
         }
+        _mm_sfence();                     // the streaming stores are visible before the call returns
     });
     int64_t k = 0;
     for (int64_t blk = 0; blk < n_blocks; ++blk) {

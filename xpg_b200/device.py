@@ -5,7 +5,9 @@ Every buffer is a torch CUDA tensor (torch is the allocator and the stream); the
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
+import threading
 
 import numpy as np
 import torch
@@ -62,14 +64,66 @@ class _Span:
 TIMER = KernelTimer()
 
 
+class _UploadRing:
+    """Page-locked staging ring of the uploads, allocated once per process. An upload is copied into the ring and
+    read from there by a kernel on the current stream (xi_upload), not by the copy engine: that serves copies in
+    submission order, so a small upload would otherwise wait behind every frame chunk already queued. A region is
+    rewritten only after the kernel that read it has run (regions are taken in ring order, so the ones a new region
+    overlaps are the oldest in flight); while they have not run, the upload takes the copy engine instead, so the
+    host never waits for the device here."""
+
+    SIZE = 256 << 20
+
+    def __init__(self):
+        self.buf = None
+        self.head = 0
+        self.inflight = collections.deque()      # (start, end, event), oldest first
+        self.lock = threading.Lock()
+
+    def upload(self, t, out, stream):
+        """Copies CPU tensor t into device tensor out on `stream`; False when t does not fit or the ring's memory is
+        not mapped into the device (the caller copies another way)."""
+        n = t.numel() * t.element_size()
+        size = (n + 255) // 256 * 256
+        if size > self.SIZE // 4:
+            return False
+        with self.lock:
+            if self.buf is None:
+                self.buf = torch.empty(self.SIZE, dtype=torch.uint8, pin_memory=True)
+            a = self.head if self.head + size <= self.SIZE else 0
+            b = a + size
+            while self.inflight and self.inflight[0][0] < b and self.inflight[0][1] > a:
+                if not self.inflight[0][2].query():
+                    return False
+                self.inflight.popleft()
+            base = self.buf.data_ptr()
+            C.memmove(base + a, t.data_ptr(), n)
+            rc = N.load().xi_upload(C.c_void_p(base + a), C.c_void_p(out.data_ptr()), n, C.c_void_p(stream.cuda_stream))
+            if rc != N.XI_OK:
+                return False
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            self.inflight.append((a, b, ev))
+            self.head = b
+            return True
+
+
+_RING = _UploadRing()
+
+
 def h2d(a, dtype=None, device="cuda"):
-    """Host array -> device tensor without blocking the host: staged through pinned memory (torch's caching host
-    allocator keeps the staging block until the copy has run), copied on the current stream. A pageable copy would
+    """Host array -> device tensor on the current stream without blocking the host: staged through the upload ring
+    and read by a kernel (large arrays: through torch's pinned staging and the copy engine). A pageable copy would
     wait for every kernel queued before it."""
     t = torch.as_tensor(np.ascontiguousarray(a), dtype=dtype)
     if t.numel() == 0:
         return t.to(device)
-    return t.pin_memory().to(device, non_blocking=True)
+    t = t.contiguous()
+    out = torch.empty(t.shape, dtype=t.dtype, device=device)
+    if _RING.upload(t, out, torch.cuda.current_stream(out.device)):
+        return out
+    out.copy_(t.pin_memory(), non_blocking=True)
+    return out
 
 
 def d2h(t):

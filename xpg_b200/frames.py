@@ -22,12 +22,12 @@ import numpy as np
 import torch
 
 
-# transfer thread: a chunk is packed while at least this many raw chunks' worth of copies are queued ...
-PACK_MIN_BACKLOG = 1.0
-# ... and goes raw when more than this fraction of its pixels need an exception pair
+# transfers: a chunk goes raw when more than this fraction of its pixels need an exception pair
 PACK_EXC_PER_PIXEL = 1.0 / 64
-# raw chunks' worth of copies the transfer thread keeps queued at most
-QUEUED_CHUNKS = 4
+# raw chunks' worth of copies kept queued in the copy engine at most
+QUEUED_CHUNKS = 3
+# a second transfer thread copies chunks raw from the back of each wedge while the first packs from its front
+RAW_THREAD = True
 
 
 class _Uploads:
@@ -92,151 +92,237 @@ class _HostSlots:
 _HOST_SLOTS = _HostSlots()
 
 
-class _Feeder:
-    """Transfers the wedges of a run from pinned host memory ahead of the integration, from a thread of its own,
-    starting before the plan is made, in copies of `chunk` frames on a copy stream (the copy engine serves copies in
-    submission order, across streams, so at most `queued` raw chunks' worth of bytes wait in it and a small copy the
-    integration issues meanwhile waits for little); at most `depth` wedges are held on the device.
+_STREAMS = {}
 
-    A chunk goes raw (4 bytes a pixel) or packed by xi_pack_u8 on the host's cores (1 byte a pixel plus exceptions,
-    widened back on the device by xi_unpack_u8 on a second stream). The thread packs the next chunk while at least
-    `min_backlog` raw chunks' worth of copies are queued, and sends it raw otherwise, so that the link never waits
-    for the packing: the split adapts to the link's and the host's speeds. The device frames are the same either way,
-    bit for bit."""
+
+def _transfer_streams(device):
+    """Streams of the transfer threads, one set per device for the whole process (the caching allocator reuses a
+    stream's freed blocks only for that stream): raw copies, packed copies, and the unpacks (high priority, so that
+    the widening of a chunk does not wait behind the integration's kernels)."""
+    key = device.index
+    if key not in _STREAMS:
+        _STREAMS[key] = (torch.cuda.Stream(device=device), torch.cuda.Stream(device=device),
+                         torch.cuda.Stream(device=device, priority=-1))
+    return _STREAMS[key]
+
+
+class _Job:
+    """One wedge in transfer: chunks [lo, hi) are not yet taken; `left` are not yet issued."""
+
+    def __init__(self, w, h, d, n_chunks):
+        self.w, self.h, self.d = w, h, d
+        self.lo, self.hi, self.left = 0, n_chunks, n_chunks
+
+
+class _Feeder:
+    """Transfers the wedges of a run from pinned host memory ahead of the integration, starting before the plan is
+    made, in chunks of `chunk` frames; at most `depth` wedges are held on the device.
+
+    Two threads share each wedge. The packing thread takes chunks from its front, packs each on the host's cores
+    (xi_pack_u8: 1 byte a pixel plus exceptions) and uploads it, to be widened on the device (xi_unpack_u8); the raw
+    thread takes chunks from its back and copies them as they are (4 bytes a pixel), keeping `queued` raw chunks'
+    worth of copies waiting in the copy engine (it serves copies in submission order, across streams, so a small
+    copy the integration issues meanwhile waits for little). Both stay busy until they meet, so the split between
+    the link and the host's cores follows their speeds. Without packing one thread copies every chunk raw. The
+    device frames are the same either way, bit for bit."""
 
     HOST_SLOTS = 8
-    DEV_SLOTS = 3
+    DEV_SLOTS = 6
 
-    def __init__(self, host, first, wedges, oks, device, depth=4, chunk=2, queued=4, pack=True,
-                 min_backlog=PACK_MIN_BACKLOG, exc_per_pixel=PACK_EXC_PER_PIXEL, threads=0, stats=None):
+    def __init__(self, host, first, wedges, oks, device, depth=4, chunk=2, queued=4, pack=True, raw_thread=True,
+                 exc_per_pixel=PACK_EXC_PER_PIXEL, threads=0, stats=None):
         self.host, self.first = host, first
         self.wedges, self.oks = wedges, oks
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
-        self.stream = torch.cuda.Stream(device=self.device)
-        self.unpack_stream = torch.cuda.Stream(device=self.device) if pack else None
+        self.s_raw, self.s_pk, self.s_un = _transfer_streams(self.device)
         self.ready = [threading.Event() for _ in wedges]
         self.out = [None] * len(wedges)
         self.held = [False] * len(wedges)   # the wedge took a slot
         self.slots = threading.Semaphore(depth)
         self.chunk, self.queued = chunk, queued
-        self.pack, self.min_backlog = pack, min_backlog
-        self.exc_per_pixel, self.threads = exc_per_pixel, threads
+        self.pack, self.exc_per_pixel, self.threads = pack, exc_per_pixel, threads
         self.stats = stats if stats is not None else {}
         for k in ("h2d_bytes", "chunks_raw", "chunks_packed"):
             self.stats.setdefault(k, 0)
+        self.cv = threading.Condition()
+        self.jobs = []                      # wedges in transfer, in order
+        self.owner_done = False
+        self.pend = collections.deque()     # (copy event, raw chunks' worth of bytes), in submission order
         self.error = None
         self.stopping = False
-        self.thread = threading.Thread(target=self._run, daemon=True)
-        self.thread.start()
+        self.px_chunk = chunk * int(host.shape[1]) * int(host.shape[2])
+        self.threads_ = [threading.Thread(target=self._guard, args=(self._owner,), daemon=True)]
+        if pack and raw_thread:
+            self.threads_.append(threading.Thread(target=self._guard, args=(self._raw_from_back,), daemon=True))
+        for t in self.threads_:
+            t.start()
 
-    def _run(self):
+    def _guard(self, fn):
         try:
             torch.cuda.set_device(self.device)
-            self._transfer()
+            fn()
         except BaseException as e:          # surfaced by get()
-            self.error = e
+            with self.cv:
+                self.error = self.error or e
+                self.stopping = True
+                self.cv.notify_all()
             for r in self.ready:
                 r.set()
 
-    def _transfer(self):
+    # ---- the copy engine's queue
+    def _backlog(self):
+        with self.cv:
+            while self.pend and self.pend[0][0].query():
+                self.pend.popleft()
+            return sum(u for _, u in self.pend)
+
+    def _wait_backlog(self):
+        while self._backlog() >= self.queued and not self.stopping:
+            time.sleep(2e-4)                # polling lets the integration's thread run meanwhile
+
+    # ---- one chunk
+    def _raw(self, job, c):
+        hc, dc = job.h[c * self.chunk:(c + 1) * self.chunk], job.d[c * self.chunk:(c + 1) * self.chunk]
+        with torch.cuda.stream(self.s_raw):
+            dc.copy_(hc, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.s_raw)
+        with self.cv:
+            self.pend.append((ev, hc.numel() / self.px_chunk))
+            self.stats["h2d_bytes"] += 4 * hc.numel()
+            self.stats["chunks_raw"] += 1
+
+    def _packed(self, job, c, st):
+        """Packs and uploads chunk c; False when it needs more exception pairs than a slot holds (send it raw)."""
         import ctypes as C
         from . import native
-        lib = native.load() if self.pack else None
-        s1, s2 = self.stream, self.unpack_stream
-        ny, nx = int(self.host.shape[1]), int(self.host.shape[2])
-        px_chunk = self.chunk * ny * nx
-        plane_bytes = (px_chunk + 15) // 16 * 16
-        cap = max(1024, int(px_chunk * self.exc_per_pixel))
-        slot_bytes = plane_bytes + 8 * cap
-        dev_slots, dev_events = [], []
+        hc, dc = job.h[c * self.chunk:(c + 1) * self.chunk], job.d[c * self.chunk:(c + 1) * self.chunk]
+        if dc.data_ptr() % 16:
+            return False
+        n = hc.numel()
+        hk, hbuf = _HOST_SLOTS.take(st["slot_bytes"], self.HOST_SLOTS)
+        hp = hbuf.data_ptr()
+        rc = st["lib"].xi_pack_u8(C.c_void_p(hc.data_ptr()), n, C.c_void_p(hp), C.c_void_p(hp + st["plane"]),
+                                  st["cap"], self.threads, C.byref(st["n_exc"]))
+        if rc == native.XI_E_LIMIT:
+            return False
+        native.check(rc, "xi_pack_u8")
+        ne = st["n_exc"].value
+        nbytes = st["plane"] + 8 * ne
+        dk = st["dk"]
+        st["dk"] = (dk + 1) % self.DEV_SLOTS
+        dbuf = st["dev"][dk]
+        if st["dev_ev"][dk] is not None:
+            self.s_pk.wait_event(st["dev_ev"][dk])      # its last unpack has read it
+        with torch.cuda.stream(self.s_pk):
+            dbuf[:nbytes].copy_(hbuf[:nbytes], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.s_pk)
+        _HOST_SLOTS.events[hk] = ev
+        self.s_un.wait_event(ev)
+        dp = dbuf.data_ptr()
+        native.check(st["lib"].xi_unpack_u8(C.c_void_p(dp), n, C.c_void_p(dp + st["plane"]), ne,
+                                            C.c_void_p(dc.data_ptr()), C.c_void_p(self.s_un.cuda_stream)),
+                     "xi_unpack_u8")
+        ue = torch.cuda.Event()
+        ue.record(self.s_un)
+        st["dev_ev"][dk] = ue
+        with self.cv:
+            self.pend.append((ev, nbytes / (4.0 * self.px_chunk)))
+            self.stats["h2d_bytes"] += nbytes
+            self.stats["chunks_packed"] += 1
+        return True
+
+    def _issued(self, job):
+        """One chunk of the job issued; after its last one the wedge's ready event follows every copy and unpack."""
+        with self.cv:
+            job.left -= 1
+            if job.left:
+                return
+            ev = torch.cuda.Event()
+            ev.record(self.s_raw)
+            self.s_un.wait_event(ev)
+            ready = torch.cuda.Event()
+            ready.record(self.s_un)
+            self.out[job.w] = (job.d, ready)
+            self.ready[job.w].set()
+
+    def _take(self, job, front):
+        with self.cv:
+            if job.lo >= job.hi:
+                return None
+            if front:
+                job.lo += 1
+                return job.lo - 1
+            job.hi -= 1
+            return job.hi
+
+    # ---- the threads
+    def _owner(self):
+        """Opens the wedges in order and works on each from its front (packing, or raw copies without packing)."""
+        st = None
         if self.pack:
-            with torch.cuda.stream(s1):
-                dev_slots = [torch.empty(slot_bytes, dtype=torch.uint8, device=self.device)
+            import ctypes as C
+            from . import native
+            plane = (self.px_chunk + 15) // 16 * 16
+            cap = max(1024, int(self.px_chunk * self.exc_per_pixel))
+            st = {"lib": native.load(), "plane": plane, "cap": cap, "slot_bytes": plane + 8 * cap,
+                  "n_exc": C.c_int64(), "dk": 0, "dev_ev": [None] * self.DEV_SLOTS}
+            with torch.cuda.stream(self.s_pk):
+                st["dev"] = [torch.empty(plane + 8 * cap, dtype=torch.uint8, device=self.device)
                              for _ in range(self.DEV_SLOTS)]
-            for t in dev_slots:
-                t.record_stream(s2)
-            dev_events = [None] * self.DEV_SLOTS
-        dk = 0
-        n_exc = C.c_int64() if self.pack else None
-        pend = collections.deque()            # (copy event on s1, raw chunks' worth of bytes)
+            for t in st["dev"]:
+                t.record_stream(self.s_un)
+        try:
+            for w, (fa, fb) in enumerate(self.wedges):
+                if not self.oks[w].any():
+                    self.ready[w].set()
+                    continue
+                self.slots.acquire()
+                if self.stopping:
+                    break
+                self.held[w] = True
+                h = self.host[fa - self.first:fb - self.first + 1]
+                with torch.cuda.stream(self.s_raw):
+                    d = torch.empty(h.shape, dtype=h.dtype, device=self.device)
+                d.record_stream(self.s_un)       # unpacks write it from their own stream
+                job = _Job(w, h, d, (h.shape[0] + self.chunk - 1) // self.chunk)
+                with self.cv:
+                    self.jobs.append(job)
+                    self.cv.notify_all()
+                while not self.stopping:
+                    c = self._take(job, True)
+                    if c is None:
+                        break
+                    if not (self.pack and self._packed(job, c, st)):
+                        if not self.pack:
+                            self._wait_backlog()
+                        self._raw(job, c)
+                    self._issued(job)
+        finally:
+            with self.cv:
+                self.owner_done = True
+                self.cv.notify_all()
 
-        def backlog():
-            while pend and pend[0][0].query():
-                pend.popleft()
-            return sum(u for _, u in pend)
-
-        for w, (fa, fb) in enumerate(self.wedges):
-            if not self.oks[w].any():
-                self.ready[w].set()
+    def _raw_from_back(self):
+        """Raw copies from the back of the earliest wedge with chunks left, while the copy engine has room."""
+        k = 0
+        while True:
+            with self.cv:
+                while k >= len(self.jobs) and not self.owner_done and not self.stopping:
+                    self.cv.wait(0.05)
+                if self.stopping or k >= len(self.jobs):
+                    return
+                job = self.jobs[k]
+            self._wait_backlog()
+            c = self._take(job, False)
+            if c is None:
+                k += 1
                 continue
-            self.slots.acquire()
-            if self.stopping:
-                break
-            self.held[w] = True
-            h = self.host[fa - self.first:fb - self.first + 1]
-            with torch.cuda.stream(s1):
-                d = torch.empty(h.shape, dtype=h.dtype, device=self.device)
-            if self.pack:
-                d.record_stream(s2)              # unpacks write it from the second stream
-            last = None
-            for c0 in range(0, h.shape[0], self.chunk):
-                hc, dc = h[c0:c0 + self.chunk], d[c0:c0 + self.chunk]
-                n = hc.numel()
-                units = n / px_chunk
-                q = backlog()
-                while q >= self.queued:
-                    time.sleep(2e-4)            # polling lets the integration's thread run meanwhile
-                    q = backlog()
-                packed = False
-                if self.pack and q >= self.min_backlog and dc.data_ptr() % 16 == 0:
-                    hk, hbuf = _HOST_SLOTS.take(slot_bytes, self.HOST_SLOTS)
-                    hp = hbuf.data_ptr()
-                    rc = lib.xi_pack_u8(C.c_void_p(hc.data_ptr()), n, C.c_void_p(hp),
-                                        C.c_void_p(hp + plane_bytes), cap, self.threads, C.byref(n_exc))
-                    if rc == native.XI_OK:
-                        packed = True
-                    elif rc != native.XI_E_LIMIT:   # too many exceptions: this chunk goes raw
-                        native.check(rc, "xi_pack_u8")
-                if packed:
-                    ne = n_exc.value
-                    nbytes = plane_bytes + 8 * ne
-                    dbuf = dev_slots[dk]
-                    if dev_events[dk] is not None:
-                        s1.wait_event(dev_events[dk])   # its last unpack has read it
-                    with torch.cuda.stream(s1):
-                        dbuf[:nbytes].copy_(hbuf[:nbytes], non_blocking=True)
-                    ev = torch.cuda.Event()
-                    ev.record(s1)
-                    _HOST_SLOTS.events[hk] = ev
-                    s2.wait_event(ev)
-                    dp = dbuf.data_ptr()
-                    native.check(lib.xi_unpack_u8(C.c_void_p(dp), n, C.c_void_p(dp + plane_bytes), ne,
-                                                  C.c_void_p(dc.data_ptr()), C.c_void_p(s2.cuda_stream)),
-                                 "xi_unpack_u8")
-                    ue = torch.cuda.Event()
-                    ue.record(s2)
-                    dev_events[dk] = ue
-                    dk = (dk + 1) % self.DEV_SLOTS
-                    pend.append((ev, nbytes / (4.0 * px_chunk)))
-                    self.stats["h2d_bytes"] += nbytes
-                    self.stats["chunks_packed"] += 1
-                else:
-                    with torch.cuda.stream(s1):
-                        dc.copy_(hc, non_blocking=True)
-                    ev = torch.cuda.Event()
-                    ev.record(s1)
-                    pend.append((ev, units))
-                    self.stats["h2d_bytes"] += 4 * n
-                    self.stats["chunks_raw"] += 1
-                last = ev
-            if self.pack:                        # the wedge is ready when its raw copies and its unpacks are done
-                s2.wait_event(last)
-                last = torch.cuda.Event()
-                last.record(s2)
-            self.out[w] = (d, last)
-            self.ready[w].set()
+            self._raw(job, c)
+            self._issued(job)
 
     def get(self, w):
         """Wedge w on the device, ordered before the current stream's next work."""
@@ -259,10 +345,13 @@ class _Feeder:
             self.slots.release()
 
     def close(self):
-        self.stopping = True
+        with self.cv:
+            self.stopping = True
+            self.cv.notify_all()
         for _ in range(len(self.wedges) + 1):
             self.slots.release()
-        self.thread.join()
+        for t in self.threads_:
+            t.join()
 
 
 class _PinnedRing:
@@ -315,8 +404,18 @@ class U32Frames:
         if self.on_device or not torch.is_tensor(d) or not d.is_pinned():
             return None
         h = d if d.dtype == torch.int32 else d.view(torch.int32)
-        return _Feeder(h, self.first, wedges, oks, self.device, queued=QUEUED_CHUNKS, pack=self.pack,
-                       min_backlog=PACK_MIN_BACKLOG, exc_per_pixel=PACK_EXC_PER_PIXEL, stats=self.transfer)
+        return _Feeder(h, self.first, wedges, oks, self.device, depth=self._depth(wedges), queued=QUEUED_CHUNKS,
+                       pack=self.pack, raw_thread=RAW_THREAD, exc_per_pixel=PACK_EXC_PER_PIXEL, stats=self.transfer)
+
+    def _depth(self, wedges):
+        """Wedges the transfer may hold on the device at once: as many as half the free device memory takes (at
+        least 4), so that the transfer runs ahead of an integration that is still planning."""
+        dev = torch.device(self.device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        free = torch.cuda.mem_get_info(dev)[0] + torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+        per = max(fb - fa + 1 for fa, fb in wedges) * self.ny * self.nx * 4 if wedges else 1
+        return max(4, min(len(wedges), int(0.5 * free // per)))
 
     def wedge(self, f_a, f_b, ok=None, stream=None):
         if self.on_device:

@@ -192,7 +192,7 @@ def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, b
     det_cache = {}
     mask_t = None
     if mask is not None and not np.asarray(mask).all():
-        mask_t = torch.as_tensor(np.asarray(mask, np.uint8)).to(device)
+        mask_t = D.h2d(np.asarray(mask, np.uint8), None, device)
 
     def detector(g):
         key = (id(g), id(bkg_template))
