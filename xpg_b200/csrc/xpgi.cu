@@ -1018,24 +1018,23 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                   float vv[kZBatch];
 #pragma unroll
                   for (int u = 0; u < kZBatch; ++u) vv[u] = have && t0 + u < zn ? col[(size_t)(t0 + u) * P] : 0.0f;
+                  unsigned ub = 0u;                      // fitted voxels of this batch
 #pragma unroll
                   for (int u = 0; u < kZBatch; ++u) {
                     const int t = t0 + u;
                     if (t >= zn) break;
                     const int z = 32 * w + t;
-                    bool use = false;
-                    float net = 0.0f;
                     if (have) {
                         const float v = vv[u] - R.sb_bias;
                         const float pv = P2 * fR[z];
                         const float ppv = (P2p * fRp[z]) * hp;
                         const bool clean = v >= 0.0f && !((nw >> t) & 1u);
                         if (!clean) lost += fR[z];
-                        use = clean && (pv > pthr || ppv > ppthr);
-                        net = v - bpix;
+                        const bool use = clean && (pv > pthr || ppv > ppthr);
+                        const float net = v - bpix;
                         if (STAGED) stage[(size_t)z * P + p] = use ? net : __int_as_float(0x7fc00000);
                         if (use) {
-                            uw |= 1u << t;
+                            ub |= 1u << u;
                             a8[0] += (double)net;
                             a8[1] += (double)(pv + ppv);
                             a8[5] += (double)((pv * pv) * iv0);
@@ -1043,18 +1042,32 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                             a8[7] += 1.0;
                         }
                     }
-                    // warp-aggregated append to the fit list
-                    const unsigned ball = __ballot_sync(0xffffffffu, use);
-                    if (ball) {
-                        int base = 0;
-                        if (lane == 0) base = atomicAdd(&s_nlist, __popc(ball));
-                        base = __shfl_sync(0xffffffffu, base, 0);
-                        const int k = base + __popc(ball & ((1u << lane) - 1u));
-                        if (use && k < cap) {
-                            ul_v[k] = net;
-                            ul_i[k] = ((unsigned)z << 16) | (unsigned)p;
-                        }
-                    }
+                  }
+                  uw |= ub << t0;
+                  // warp-aggregated append of the batch's fitted voxels to the fit list: a lane's entries follow
+                  // the entries of the lanes before it (one scan and one atomic per warp and batch)
+                  const int c = __popc(ub);
+                  int incl = c;
+#pragma unroll
+                  for (int o = 1; o < 32; o <<= 1) {
+                      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                      if (lane >= o) incl += y;
+                  }
+                  const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+                  if (wtot) {
+                      int base = 0;
+                      if (lane == 31) base = atomicAdd(&s_nlist, wtot);
+                      base = __shfl_sync(0xffffffffu, base, 31);
+                      int k = base + incl - c;
+#pragma unroll
+                      for (int u = 0; u < kZBatch; ++u) {
+                          if (!((ub >> u) & 1u)) continue;
+                          if (k < cap) {
+                              ul_v[k] = (vv[u] - R.sb_bias) - bpix;
+                              ul_i[k] = ((unsigned)(32 * w + t0 + u) << 16) | (unsigned)p;
+                          }
+                          ++k;
+                      }
                   }
                 }
                 umw[w] = uw;

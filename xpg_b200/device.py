@@ -191,6 +191,14 @@ def block_consts(g, sd, sm, gain, rcw, device="cuda"):
     return b, rc
 
 
+def _offsets(sizes):
+    """Exclusive prefix sum (int64): where each row's block starts."""
+    out = np.zeros(sizes.size, np.int64)
+    if sizes.size > 1:
+        np.cumsum(sizes[:-1], out=out[1:])
+    return out
+
+
 class RowSet:
     """Per-reflection inputs of a set of rows (any mix of shoebox shapes), packed on the device with their arena
     offsets: `sb_off` (shoebox voxels), `pix_off` (per-pixel outputs), `frm_off` (per-frame outputs)."""
@@ -201,16 +209,14 @@ class RowSet:
         self.n = n
         self.Dz = np.asarray(Dz, np.int64)
         self.bx = np.asarray(bx, np.int64)
-        V = self.Dz * self.bx * self.bx
-        self.vox = V
-        Vp = (V + 3) // 4 * 4 if sb_bias == 3.0 else V     # arena rows start on 16 bytes (bulk copies)
-        self.sb_off = np.concatenate([[0], np.cumsum(Vp)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
         P = self.bx * self.bx
-        self.pix_off = np.concatenate([[0], np.cumsum(P)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
-        self.frm_off = np.concatenate([[0], np.cumsum(self.Dz)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
-        self.n_vox = int(Vp.sum()) + 4
-        self.n_pix = int(P.sum())
-        self.n_frm = int(self.Dz.sum())
+        V = self.Dz * P
+        self.vox = V
+        Vp = (V + 3) & ~3 if sb_bias == 3.0 else V          # arena rows start on 16 bytes (bulk copies)
+        self.sb_off, self.pix_off, self.frm_off = _offsets(Vp), _offsets(P), _offsets(self.Dz)
+        self.n_vox = int(self.sb_off[-1] + Vp[-1]) + 4 if n else 4
+        self.n_pix = int(self.pix_off[-1] + P[-1]) if n else 0
+        self.n_frm = int(self.frm_off[-1] + self.Dz[-1]) if n else 0
         K = int(nb["x"].shape[1]) if n else 0
         if K > N.XI_MAX_K:
             raise ValueError(f"{K} neighbour columns > {N.XI_MAX_K}")

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import native as N
-from .device import TIMER, h2d
+from .device import TIMER, d2h, h2d
 from .geometry import centring_allowed, generate_hkl, unit
 
 N_FG = 3.0
@@ -221,6 +221,20 @@ PRED_F64 = ("phi", "x", "y", "z", "zeta", "polarization", "zeta_k")
 BOX_I32 = ("iz0", "dz", "fb", "Dz", "bx", "pxs", "ix0", "iy0", "region", "zstart", "zend")
 
 
+def _host_cols(cols):
+    """Device columns -> host numpy arrays: the columns of one dtype and size go in one stacked copy through pinned
+    memory (each column a contiguous row of it) instead of one synchronising copy each."""
+    groups = {}
+    for k, v in cols.items():
+        groups.setdefault((v.dtype, v.numel()), []).append(k)
+    out = {}
+    for ks in groups.values():
+        st = d2h(torch.stack([cols[k].reshape(-1) for k in ks]))
+        for i, k in enumerate(ks):
+            out[k] = st[i].reshape(tuple(cols[k].shape))
+    return out
+
+
 def _columns(n, names, dtype, device, width=None):
     return {k: torch.empty((n,) if not width or k not in width else (n, width[k]), dtype=dtype, device=device)
             for k in names}
@@ -349,12 +363,14 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
               z=f32(torch.where(has, pred["z"][jl], -1e6)), sx=f32(torch.where(has, bcols["sx_px"][jl], 1.0)),
               sz=f32(torch.where(has, bcols["sz_f"][jl], 1.0)))
     # host copies
-    refl = {k: v.cpu().numpy() for k, v in pred.items()}
-    h = {k: v.cpu().numpy().astype(np.int64) for k, v in bcols.items() if k in BOX_I32}
-    refl["coverage"] = bcols["coverage"].cpu().numpy()
+    hc = _host_cols(dict(pred, **{"box_" + k: bcols[k] for k in BOX_I32}, coverage=bcols["coverage"],
+                         has_partner=has_partner, partner=nbj[:, 0].contiguous()))
+    refl = {k: hc[k] for k in pred}
+    h = {k: hc["box_" + k].astype(np.int64) for k in BOX_I32}
+    refl["coverage"] = hc["coverage"]
     nbh = LazyHost(nb, K)
-    hp = has_partner.cpu().numpy()
-    partner = nbj[:, 0].cpu().numpy().astype(np.int64) if n else np.zeros(0, np.int64)
+    hp = hc["has_partner"]
+    partner = hc["partner"].astype(np.int64) if n else np.zeros(0, np.int64)
     if foreign_spots is not None and len(foreign_spots[0]) and n:
         nbh = {k: nbh[k] for k in ("x", "y", "z", "sx", "sz")}
         _add_foreign(nbh, refl, foreign_spots, n_foreign, sxm, szm)
