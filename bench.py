@@ -23,6 +23,7 @@ independent; weak scaling). `--impl reference` times the CPU restatement of the 
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -56,9 +57,10 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons: started before the warm-up (its start-up load stays out
+    of the timed steps), summarised over the samples taken between mark() and stop() (the timed region)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
@@ -66,6 +68,10 @@ class Clocks:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.gpu = gpu_index
         self.p = None
+        self.t0 = None
+
+    def mark(self):
+        self.t0 = time.time()
 
     def start(self):
         try:
@@ -78,10 +84,20 @@ class Clocks:
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t1 = time.time()
         self.p.terminate()
         self.p.wait(5)
         self.f.flush()
         rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        timed = []
+        for r in rows:
+            try:
+                ts = datetime.datetime.strptime(r[0].strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except (ValueError, IndexError):
+                continue
+            if self.t0 is None or self.t0 <= ts <= t1:
+                timed.append(r)
+        rows = timed or rows
         sm, smax, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for r in rows:
@@ -245,8 +261,6 @@ def run(args):
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import datetime
-
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from xpg_b200 import device as D
@@ -255,15 +269,16 @@ def run(args):
         build.build()
     blk = Block(args.workload, seed_offset=rank)
     src = blk.source()
+    clocks = Clocks(local)
+    clocks.start()                # before the warm-up: nvidia-smi's start-up load stays out of the timed steps
     for _ in range(args.warmup):
         blk.integrate(src)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    clocks = Clocks(local)
-    clocks.start()
     D.TIMER.reset()
     D.TIMER.enabled = True
+    clocks.mark()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -296,7 +311,8 @@ def run(args):
                 "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_unit": "GB per launch",
                 "algorithmic": round(per_launch / 1e9, 3), "peak_kind": peak_kind,
                 "launches": n_l, "ms_per_launch": round(t_k / n_l * 1e3, 4),
-                "share": {k: round(v[1] / max(sum(x[1] for x in ksum.values()), 1e-12), 4) for k, v in ksum.items()}}
+                "share": {k: round(v[1] / max(sum(x[1] for x in ksum.values()), 1e-12), 4) for k, v in ksum.items()},
+                "ms_per_step": {k: round(v[1] / args.steps * 1e3, 2) for k, v in ksum.items()}}
     # end to end: frames from pinned host memory, uploaded inside every step; results read back by the API
     e2e = None
     if not args.no_e2e:

@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import functools
 import threading
 
 import numpy as np
@@ -209,26 +210,27 @@ class RowSet:
         self.n = n
         self.Dz = np.asarray(Dz, np.int64)
         self.bx = np.asarray(bx, np.int64)
+        self.sb_bias = sb_bias
         P = self.bx * self.bx
-        V = self.Dz * P
-        self.vox = V
-        Vp = (V + 3) & ~3 if sb_bias == 3.0 else V          # arena rows start on 16 bytes (bulk copies)
-        self.sb_off, self.pix_off, self.frm_off = _offsets(Vp), _offsets(P), _offsets(self.Dz)
-        self.n_vox = int(self.sb_off[-1] + Vp[-1]) + 4 if n else 4
-        self.n_pix = int(self.pix_off[-1] + P[-1]) if n else 0
-        self.n_frm = int(self.frm_off[-1] + self.Dz[-1]) if n else 0
+        self.n_vox = int(self._vp(self.Dz * P).sum()) + 4
+        self.n_pix = int(P.sum())
+        self.n_frm = int(self.Dz.sum())
         K = int(nb["x"].shape[1]) if n else 0
         if K > N.XI_MAX_K:
             raise ValueError(f"{K} neighbour columns > {N.XI_MAX_K}")
         d = device
+        dzbx = _dev(np.stack([self.Dz, self.bx]), torch.int32, d)      # one upload for both
+        dz64, bx64 = dzbx[0].long(), dzbx[1].long()
+        p64 = bx64 * bx64
+        vp64 = self._vp(dz64 * p64)
         self.t = dict(
             S=_dev(S, F32, d).reshape(n, 3), phi=_dev(phi, F32, d),
             ix0=_dev(ix0, torch.int32, d), iy0=_dev(iy0, torch.int32, d), iz0=_dev(iz0, torch.int32, d),
             fb=_dev(fb, F32, d), region=_dev(region, torch.int32, d),
             has_p=_dev(has_p, F32, d), pS=_dev(pS, F32, d).reshape(n, 3),
-            pphi=_dev(pphi, F32, d), pxs=_dev(pxs, torch.int32, d), Dz=_dev(self.Dz, torch.int32, d),
-            bx=_dev(self.bx, torch.int32, d), sb_off=_dev(self.sb_off, torch.int64, d),
-            pix_off=_dev(self.pix_off, torch.int64, d), frm_off=_dev(self.frm_off, torch.int64, d))
+            pphi=_dev(pphi, F32, d), pxs=_dev(pxs, torch.int32, d), Dz=dzbx[0], bx=dzbx[1],
+            sb_off=torch.cumsum(vp64, 0) - vp64, pix_off=torch.cumsum(p64, 0) - p64,
+            frm_off=torch.cumsum(dz64, 0) - dz64)
         for k in ("x", "y", "z", "sx", "sz"):
             self.t["nb" + k] = _dev(nb[k], F32, d).reshape(n, K)
         r = N.XiRows()
@@ -244,6 +246,26 @@ class RowSet:
         r.sb_bias = float(sb_bias)
         self.s = r
         self.device = device
+
+    def _vp(self, v):
+        """Arena floats of rows of v voxels: with the +3 encoding every row starts on 16 bytes (bulk copies)."""
+        return (v + 3) & ~3 if self.sb_bias == 3.0 else v
+
+    @functools.cached_property
+    def vox(self):
+        return self.Dz * self.bx * self.bx
+
+    @functools.cached_property
+    def sb_off(self):
+        return _offsets(self._vp(self.vox))
+
+    @functools.cached_property
+    def pix_off(self):
+        return _offsets(self.bx * self.bx)
+
+    @functools.cached_property
+    def frm_off(self):
+        return _offsets(self.Dz)
 
     def groups(self):
         """Launch groups: rows of one shoebox shape (side, depth), so that each launch sizes its shared memory
@@ -373,14 +395,19 @@ class GatherRows:
         n = rows.n
         fb = np.asarray(fb, np.int64)
         binned = fb > 1
-        cnt_len = np.where(binned, rows.Dz, 0)
-        cnt_off = np.where(binned, np.concatenate([[0], np.cumsum(cnt_len)[:-1]]) if n else 0, -1).astype(np.int64)
-        self.n_cnt = int(cnt_len.sum())
         self.any_binned = bool(binned.any())
+        self.n_cnt = int(rows.Dz[binned].sum()) if self.any_binned else 0
         d = device
+        fb_t = _dev(fb, torch.int32, d)
+        if self.any_binned:                  # bin counters of binned rows, packed in row order; -1 elsewhere
+            bin_t = fb_t > 1
+            cl = torch.where(bin_t, rows.t["Dz"].long(), 0)
+            cnt_off = torch.where(bin_t, torch.cumsum(cl, 0) - cl, -1)
+        else:
+            cnt_off = torch.full((n,), -1, dtype=torch.int64, device=d)
         self.t = dict(ix0=_dev(ix0, torch.int32, d), iy0=_dev(iy0, torch.int32, d), iz0=_dev(iz0, torch.int32, d),
-                      fb=_dev(fb, torch.int32, d), Dz=rows.t["Dz"], bx=rows.t["bx"], pxs=_dev(pxs, torch.int32, d),
-                      sb_off=rows.t["sb_off"], cnt_off=_dev(cnt_off, torch.int64, d))
+                      fb=fb_t, Dz=rows.t["Dz"], bx=rows.t["bx"], pxs=_dev(pxs, torch.int32, d),
+                      sb_off=rows.t["sb_off"], cnt_off=cnt_off)
         g = N.XiGatherRows()
         g.n = n
         for k, v in self.t.items():

@@ -66,8 +66,8 @@ class _Block:
         self.grows = D.GatherRows(self.rowset, ix0, iy0, iz0, p.fb[rows], pxs, device)
         self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
-        order = np.argsort(rows, kind="stable")            # local rows by global row: outputs leave in plan order
-        ident = bool((order == np.arange(order.size)).all())
+        ident = bool((rows[1:] > rows[:-1]).all())         # local rows by global row: outputs leave in plan order
+        order = None if ident else np.argsort(rows, kind="stable")
         self.perm_t = None if ident else D.h2d(order, None, device)
         self.rows_sorted = rows if ident else rows[order]
         srt = self.rows_sorted

@@ -363,10 +363,10 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
               z=f32(torch.where(has, pred["z"][jl], -1e6)), sx=f32(torch.where(has, bcols["sx_px"][jl], 1.0)),
               sz=f32(torch.where(has, bcols["sz_f"][jl], 1.0)))
     # host copies
-    hc = _host_cols(dict(pred, **{"box_" + k: bcols[k] for k in BOX_I32}, coverage=bcols["coverage"],
+    hc = _host_cols(dict(pred, **{"box_" + k: bcols[k].long() for k in BOX_I32}, coverage=bcols["coverage"],
                          has_partner=has_partner, partner=nbj[:, 0].contiguous()))
     refl = {k: hc[k] for k in pred}
-    h = {k: hc["box_" + k].astype(np.int64) for k in BOX_I32}
+    h = {k: hc["box_" + k] for k in BOX_I32}
     refl["coverage"] = hc["coverage"]
     nbh = LazyHost(nb, K)
     hp = hc["has_partner"]
