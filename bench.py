@@ -57,8 +57,8 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons: started before the warm-up (its start-up load stays out
-    of the timed steps), summarised over the samples taken between mark() and stop() (the timed region)."""
+    """nvidia-smi sampling of SM clocks and throttle reasons: started before the workload's set-up (its start-up load
+    stays out of the timed steps), summarised over the samples taken between mark() and stop() (the timed region)."""
 
     Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -267,12 +267,13 @@ def run(args):
     from xpg_b200.csrc import build
     if build.stale():
         build.build()
+    clocks = Clocks(local)
+    clocks.start()                # before the set-up: nvidia-smi's start-up load stays out of the timed steps
     blk = Block(args.workload, seed_offset=rank)
     src = blk.source()
-    clocks = Clocks(local)
-    clocks.start()                # before the warm-up: nvidia-smi's start-up load stays out of the timed steps
-    for _ in range(args.warmup):
-        blk.integrate(src)
+    res = None
+    for _ in range(args.warmup):  # results held across calls as in the timed loop: the pinned result buffers that
+        res = blk.integrate(src)  # two live results need are allocated here, not in a timed step
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -284,14 +285,18 @@ def run(args):
     torch.cuda.synchronize()
     e0.record()
     n_ok = 0
+    marks = []
     for _ in range(args.steps):
         res = blk.integrate(src)
         n_ok += int(np.isfinite(res.refl["iprf"]).sum())
+        marks.append(torch.cuda.Event(enable_timing=True))
+        marks[-1].record()
     e1.record()
     torch.cuda.synchronize()
     D.TIMER.enabled = False
     clk = clocks.stop()
     t = e0.elapsed_time(e1) * 1e-3
+    step_ms = [round(a.elapsed_time(b), 1) for a, b in zip([e0] + marks[:-1], marks)]
     ksum = D.TIMER.summary()
     launches = D.TIMER.launches
     t_max, n_total = reduce_over_ranks(t, blk.n_refl * args.steps, dist)
@@ -319,7 +324,8 @@ def run(args):
         host = torch.empty(blk.frames.shape, dtype=torch.int32, pin_memory=True)
         host.copy_(blk.frames)
         hsrc = blk.source(host)
-        blk.integrate(hsrc)
+        res = blk.integrate(hsrc)
+        res = blk.integrate(hsrc)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
@@ -348,7 +354,8 @@ def run(args):
         dist.barrier()
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 3), "higher_is_better": True,
+                "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 3), "step_ms": step_ms,
+                "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulation)",
                 "data": "synthetic: seeded 16M-pixel frames rendered on the device (spec in xpg_b200/synth.py)",
                 "config": {"workload": args.workload, "reflections_per_step": blk.n_refl,

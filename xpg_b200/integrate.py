@@ -50,9 +50,13 @@ class _Block:
         self.rows = rows                                  # global row indices, reference kernel-call order
         p = plan
         dv = p.dev                                        # the planner's device columns
-        rt = D.h2d(rows, None, device)
-        sel = lambda t: t.index_select(0, rt)
-        pj = dv["nbj"][:, 0].long().index_select(0, rt)   # nearest neighbour: the partner where there is one
+        if rows.size and rows[-1] - rows[0] + 1 == rows.size and (rows[1:] > rows[:-1]).all():
+            a, e = int(rows[0]), int(rows[-1]) + 1        # a range of plan rows (the planner's block order): views
+            sel = lambda t: t[a:e]
+        else:
+            rt = D.h2d(rows, None, device)
+            sel = lambda t: t.index_select(0, rt)
+        pj = sel(dv["nbj"][:, 0]).long()                  # nearest neighbour: the partner where there is one
         rad = lambda phi: (phi * (np.pi / 180.0)).float()  # numpy's radians, then float32
         nb = {k: sel(dv["nb" + k]) for k in ("x", "y", "z", "sx", "sz")}
         if nb["x"].shape[1] != p.nb_columns:              # foreign-spot columns were added on the host

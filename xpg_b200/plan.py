@@ -376,8 +376,12 @@ def plan_integration(exp_blocks, block_edges, model, dmin, dmax=1e9, frames=(1, 
         _add_foreign(nbh, refl, foreign_spots, n_foreign, sxm, szm)
     blk = refl["block"]
     nblocks = len(exp_blocks)
-    order = np.argsort(blk, kind="stable")
-    blocks_refl = [order[blk[order] == b] for b in range(nblocks)]
+    if (blk[1:] >= blk[:-1]).all():        # predictions leave the planner in block order: ranges of rows
+        bounds = np.searchsorted(blk, np.arange(nblocks + 1), side="left")
+        blocks_refl = [np.arange(bounds[b], bounds[b + 1], dtype=np.int64) for b in range(nblocks)]
+    else:
+        order = np.argsort(blk, kind="stable")
+        blocks_refl = [order[blk[order] == b] for b in range(nblocks)]
     zstart, zend = h["zstart"], h["zend"]
     need_lo = [int(zstart[r].min()) if r.size else 10 ** 9 for r in blocks_refl]
     need_hi = [int(zend[r].max()) if r.size else -1 for r in blocks_refl]
