@@ -320,7 +320,6 @@ __device__ void stage_wait(bool tma, unsigned long long* bar, float* stage, cons
 // ==================================================================================================================
 constexpr int kClipCand = 1024;     // background voxels above the lowest clip threshold kept per CTA
 constexpr int kFgList = 2048;       // foreground pixels listed per CTA (pass C iterates them densely)
-constexpr int kFgRounds = 40;       // rounds of NT pixels whose foreground counts are kept (>= 97^2 / 256)
 constexpr int kZBatch = 8;          // voxels of a pixel column loaded together (memory-level parallelism)
 constexpr int kGatherBatch = 8;     // frames of a box pixel read together by the gather
 
@@ -357,7 +356,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
     __shared__ int s_ncand;
     __shared__ unsigned short fgl[kFgList];
     __shared__ int s_nfgl;
-    __shared__ int wcnt[kFgRounds * (NT / 32)];
+    __shared__ int wcnt[NT / 32];
     __shared__ double s_base[2];
 
     const int row = order ? order[blockIdx.x] : blockIdx.x;
@@ -426,14 +425,13 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         float S[3] = {s_S[0], s_S[1], s_S[2]};
         box_geometry(det, S, e1, e2, bx, xs, ys, B.sd, e1s, e2s, O.J + po, nullptr, &s_seff);
     }
-    // u1 / u2 out, foreground / background-ring flags per pixel, and the foreground pixels listed in pixel order:
-    // warps count their foreground pixels per round of NT pixels, one scan of the counts gives every warp's offset
-    // per round, then the list is written (the same order on every run)
+    // u1 / u2 out, foreground / background-ring flags per pixel, and the foreground pixels listed in pixel order
+    // (a block-wide ballot scan: the list, and so every later sum over it, is the same on every run)
     {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        const int rounds = (P + NT - 1) / NT;
-        for (int q = 0; q < rounds; ++q) {
-            const int p = q * NT + threadIdx.x;
+        int base = 0;
+        for (int q0 = 0; q0 < P; q0 += NT) {
+            const int p = q0 + threadIdx.x;
             bool f = false;
             if (p < P) {
                 const float u1 = e1s[p], u2 = e2s[p];
@@ -444,30 +442,19 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
                 flags[p] = (f ? 1 : 0) | (r2 >= kBgR2 ? 2 : 0);
             }
             const unsigned ball = __ballot_sync(0xffffffffu, f);
-            if (lane == 0 && q < kFgRounds) wcnt[q * (NT / 32) + wid] = __popc(ball);
-        }
-        __syncthreads();
-        if (rounds <= kFgRounds) {
-            if (threadIdx.x == 0) {              // exclusive scan of the (round, warp) counts, round-major
-                int run = 0;
-                for (int i = 0; i < rounds * (NT / 32); ++i) {
-                    const int c = wcnt[i];
-                    wcnt[i] = run;
-                    run += c;
-                }
-                s_nfgl = run;
-            }
+            if (lane == 0) wcnt[wid] = __popc(ball);
             __syncthreads();
-            for (int q = 0; q < rounds; ++q) {
-                const int p = q * NT + threadIdx.x;
-                const bool f = p < P && (flags[p] & 1);
-                const unsigned ball = __ballot_sync(0xffffffffu, f);
-                const int k = wcnt[q * (NT / 32) + wid] + __popc(ball & ((1u << lane) - 1u));
-                if (f && k < kFgList) fgl[k] = (unsigned short)p;
+            int off = base, all = 0;
+            for (int w = 0; w < NT / 32; ++w) {
+                off += w < wid ? wcnt[w] : 0;
+                all += wcnt[w];
             }
-        } else if (threadIdx.x == 0) {
-            s_nfgl = kFgList + 1;                // more rounds than counted: pass C scans every pixel
+            const int k = off + __popc(ball & ((1u << lane) - 1u));
+            if (f && k < kFgList) fgl[k] = (unsigned short)p;
+            base += all;
+            __syncthreads();
         }
+        if (threadIdx.x == 0) s_nfgl = base;
     }
     // foreground frames: R >= 1e-3 * Rmax + 1e-6 (warp 0: max by shuffles, the mask by ballots)
     if (threadIdx.x < 32) {
