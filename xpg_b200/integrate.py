@@ -399,11 +399,16 @@ def _fz_rows(p1: D.Pass1Buffers, rs: D.RowSet, rows):
 
 
 def _adapt_rows(h1, plan, rows):
-    """Strong rows of the per-block adaptation (`xpg/integrate.py:411-414`), float64 on the float32 outputs."""
-    isum = h1["isum"].astype(np.float64)
-    vs = h1["vsum"].astype(np.float64)
-    return (isum > 0) & (isum / np.sqrt(np.maximum(vs, 1e-6)) > 15) & (h1["n_over"] == 0) & \
-        (h1["frac_rec"].astype(np.float64) > 0.98) & (plan.fb[rows] == 1)
+    """Strong rows of the per-block adaptation (`xpg/integrate.py:411-414`), float64 on the float32 outputs. The
+    integer tests go first; the float64 ratio is evaluated on the rows that pass them only (same arithmetic per row)."""
+    fb = plan.fb[rows[0]:rows[-1] + 1] if rows.size and rows[-1] - rows[0] + 1 == rows.size else plan.fb[rows]
+    cand = np.flatnonzero((h1["n_over"] == 0) & (fb == 1) & (h1["isum"] > 0))
+    isum = h1["isum"][cand].astype(np.float64)
+    vs = h1["vsum"][cand].astype(np.float64)
+    ok = (isum / np.sqrt(np.maximum(vs, 1e-6)) > 15) & (h1["frac_rec"][cand].astype(np.float64) > 0.98)
+    st = np.zeros(rows.size, bool)
+    st[cand[ok]] = True
+    return st
 
 
 def estimate_sigmas(images, exp, model0: IntegrationModel, dmin, frames, n_sample_frames=30, verbose=True, log=print,
