@@ -465,6 +465,72 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def decode_bench(args):
+    """The bitshuffle-LZ4 frame decode (Eiger chunks): the LZ4 stage on the host's cores (xi_bslz4_lz4_stage) and the
+    bit unshuffle on the device (xi_bitunshuffle), each timed alone, printed as one JSON line. The chunk is the
+    committed fixture tests/golden/bslz4_band.bin (a 256 x 4148 band of a config-2 frame: Poisson background 0.2,
+    seed 11, flagged columns; made by tests/golden/make_bslz4_band.py); the band is regenerated here from its seed and
+    the decode checked against it before timing. The unshuffle runs on full 4148 x 4362 frames."""
+    import ctypes as C
+
+    import torch
+    from xpg_b200 import native
+    from xpg_b200.csrc import build
+    if build.stale():
+        build.build()
+    lib = native.load()
+    ny, nx = 256, 4148
+    rng = np.random.default_rng(11)
+    band = rng.poisson(0.2, (ny, nx)).astype(np.uint32)
+    band[:, ::259] = 0xFFFFFFFF
+    chunk = np.fromfile(ROOT / "tests" / "golden" / "bslz4_band.bin", np.uint8)
+    out = torch.empty(band.nbytes, dtype=torch.uint8).pin_memory()
+    nb, be = C.c_int64(), C.c_int64()
+    call = lambda: lib.xi_bslz4_lz4_stage(chunk.ctypes.data, chunk.size, 4, C.c_void_p(out.data_ptr()), band.nbytes,
+                                          0, C.byref(nb), C.byref(be))
+    native.check(call(), "xi_bslz4_lz4_stage")
+    n = 4148 * 4362
+    dev_in = out.cuda()
+    chk = torch.empty(band.size, dtype=torch.int32, device="cuda")
+    native.check(lib.xi_bitunshuffle(native.ptr(dev_in), band.size, 4, be.value, native.ptr(chk),
+                                     native.stream_handle()), "xi_bitunshuffle")
+    if not np.array_equal(chk.cpu().numpy().view(np.uint32), band.reshape(-1)):
+        raise RuntimeError("decoded band differs from the band")
+    k = max(args.steps, 1) * 40
+    t0 = time.perf_counter()
+    for _ in range(k):
+        call()
+    th = (time.perf_counter() - t0) / k
+    staged = torch.randint(0, 256, (n * 4,), dtype=torch.uint8, device="cuda")
+    frame = torch.empty(n, dtype=torch.int32, device="cuda")
+    st = native.stream_handle()
+    go = lambda: lib.xi_bitunshuffle(native.ptr(staged), n, 4, 2048, native.ptr(frame), st)
+    for _ in range(max(args.warmup, 3)):
+        native.check(go(), "xi_bitunshuffle")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kd = max(args.steps, 1) * 4
+    e0.record()
+    for _ in range(kd):
+        go()
+    e1.record()
+    torch.cuda.synchronize()
+    td = e0.elapsed_time(e1) * 1e-3 / kd
+    peak, peak_kind = _peaks()
+    dev_gbs = 8.0 * n / td / 1e9
+    print(json.dumps({
+        "metric": "bitshuffle-LZ4 frame decode (Eiger chunks)", "unit": "GB/s of uint32 frame bytes",
+        "compression_ratio": round(band.nbytes / chunk.size, 2),
+        "host_lz4_stage": {"value": round(band.nbytes / th / 1e9, 2),
+                           "frames_per_s_16M": round(band.nbytes / th / (4 * n), 1),
+                           "cores": len(os.sched_getaffinity(0)),
+                           "sample": f"{ny} x {nx} uint32 band, {chunk.size} B chunk, {k} calls"},
+        "device_unshuffle": {"value": round(4.0 * n / td / 1e9, 1), "ms_per_16M_frame": round(td * 1e3, 3),
+                             "roofline": {"bound": "hbm", "achieved": round(dev_gbs, 1), "peak": peak, "unit": "GB/s",
+                                          "frac": round(dev_gbs / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                                          "algorithmic": "4 B read + 4 B written per pixel"}},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,8 +541,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--decode", action="store_true", help="time the bitshuffle-LZ4 frame decode instead")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.decode:
+        decode_bench(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         run(args)

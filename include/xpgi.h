@@ -358,6 +358,24 @@ int xi_pack_u8(const uint32_t *src, int64_t n, uint8_t *plane, uint32_t *exc, in
  * device memory; plane and out 16-byte aligned). */
 int xi_unpack_u8(const uint8_t *plane, int64_t n, const uint32_t *exc, int64_t n_exc, uint32_t *out, void *stream);
 
+/* ---- Bitshuffle-LZ4 frames (Eiger chunks, HDF5 filter 32008) ----------------------------------------------------
+ * XPG's split of the decode (xpg/io/bslz4.py): the LZ4 stage on the host (`lz4_stage`, :35-64), the bit unshuffle on
+ * the device (`unshuffle_frame_torch`, :85-121). Chunk: 8-byte big-endian uncompressed size, 4-byte big-endian block
+ * size in bytes (0: 8192), per block a 4-byte big-endian compressed size and an LZ4 block; a last partial block's
+ * n % 8 elements follow as they are. */
+
+/* Host function (no CUDA call): the LZ4 stage of one chunk of esize-byte elements (2 or 4) into out (out_bytes >= the
+ * chunk's uncompressed size), still bit-shuffled; *n_bytes gets that size, *block_elems the block size in elements
+ * (a multiple of 8). Blocks decompress on `threads` threads of the library's pool (0: its choice). XI_E_ARG on a
+ * malformed chunk (out then holds partial output). */
+int xi_bslz4_lz4_stage(const uint8_t *chunk, int64_t chunk_bytes, int esize, uint8_t *out, int64_t out_bytes,
+                       int threads, int64_t *n_bytes, int64_t *block_elems);
+
+/* The bit unshuffle of a chunk's LZ4-stage output `in` (device) into n_elem uint32 values at out (device, 4-byte
+ * aligned; 16-byte aligned stores when it is): 4-byte elements as they are, 2-byte elements widened with their all-ones value to 0xFFFFFFFF (the flag
+ * of the uint32 frame path). */
+int xi_bitunshuffle(const uint8_t *in, int64_t n_elem, int esize, int64_t block_elems, uint32_t *out, void *stream);
+
 /* Copies `bytes` from page-locked host memory (cudaHostAlloc / cudaHostRegister, mapped into the device's address
  * space) to device memory with a kernel that reads the host memory over the link: unlike cudaMemcpyAsync it does not
  * queue behind the copies already waiting in the copy engine (the frame chunks), so a small upload is not delayed by

@@ -184,3 +184,114 @@ extern "C" int xi_pack_u8(const uint32_t* src, int64_t n, uint8_t* plane, uint32
     *n_exc = k;
     return XI_OK;
 }
+
+// ---- bitshuffle-LZ4 chunks: the LZ4 stage ----------------------------------------------------------------------
+// Chunk layout (HDF5 filter 32008): 8-byte big-endian uncompressed size, 4-byte big-endian block size (0: 8192), then
+// per block a 4-byte big-endian compressed size and an LZ4 block; a last partial block's n % 8 elements follow as
+// they are. The block headers are walked once on the calling thread, then the blocks decompress on the pool.
+namespace {
+
+uint64_t be(const uint8_t* p, int n) {
+    uint64_t v = 0;
+    for (int i = 0; i < n; ++i) v = (v << 8) | p[i];
+    return v;
+}
+
+// one LZ4 block (the published block format) into exactly n_out bytes; false on a malformed block
+bool lz4_block(const uint8_t* src, int64_t n, uint8_t* dst, int64_t n_out) {
+    int64_t ip = 0, op = 0;
+    for (;;) {
+        if (ip >= n) return false;
+        const unsigned token = src[ip++];
+        int64_t lit = token >> 4;
+        if (lit == 15) {
+            unsigned b;
+            do {
+                if (ip >= n) return false;
+                b = src[ip++];
+                lit += b;
+            } while (b == 255);
+        }
+        if (lit > n - ip || lit > n_out - op) return false;
+        memcpy(dst + op, src + ip, (size_t)lit);
+        ip += lit;
+        op += lit;
+        if (ip == n) break;                          // the last sequence: literals only
+        if (n - ip < 2) return false;
+        const int64_t off = (int64_t)src[ip] | ((int64_t)src[ip + 1] << 8);
+        ip += 2;
+        int64_t ml = token & 15;
+        if (ml == 15) {
+            unsigned b;
+            do {
+                if (ip >= n) return false;
+                b = src[ip++];
+                ml += b;
+            } while (b == 255);
+        }
+        ml += 4;
+        if (off == 0 || off > op || ml > n_out - op) return false;
+        uint8_t* d = dst + op;
+        for (int64_t k = 0; k < ml;) {               // pieces of at most `off` bytes never overlap their source
+            const int64_t c = std::min(off, ml - k);
+            memcpy(d + k, d + k - off, (size_t)c);
+            k += c;
+        }
+        op += ml;
+    }
+    return op == n_out;
+}
+
+struct Lz4Block {
+    int64_t src, csize, dst, bytes;
+};
+
+}  // namespace
+
+extern "C" int xi_bslz4_lz4_stage(const uint8_t* chunk, int64_t chunk_bytes, int esize, uint8_t* out, int64_t out_bytes,
+                                  int threads, int64_t* n_bytes, int64_t* block_elems) {
+    if (!chunk || !out || !n_bytes || !block_elems || chunk_bytes < 0 || out_bytes < 0)
+        return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: null pointer or negative size");
+    if (esize != 2 && esize != 4) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: element size must be 2 or 4");
+    if (chunk_bytes < 12) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: chunk shorter than its header");
+    const uint64_t total = be(chunk, 8);
+    const uint64_t bsize = be(chunk + 8, 4) ? be(chunk + 8, 4) : 8192;
+    if (total % (uint64_t)esize || total > (uint64_t)out_bytes)
+        return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: uncompressed size is not a whole frame of this buffer");
+    const int64_t n = (int64_t)(total / esize);
+    int64_t belem = (int64_t)(bsize / esize);
+    belem -= belem % 8;
+    if (belem <= 0) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: block smaller than 8 elements");
+    std::vector<Lz4Block> blocks;
+    blocks.reserve((size_t)(n / belem + 1));
+    int64_t pos = 12, done = 0;
+    while (done < n) {
+        const int64_t m = std::min(belem, n - done), m8 = m - m % 8;
+        if (m8) {
+            if (chunk_bytes - pos < 4) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: truncated block header");
+            const int64_t c = (int64_t)be(chunk + pos, 4);
+            pos += 4;
+            if (c > chunk_bytes - pos) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: block beyond the chunk");
+            blocks.push_back({pos, c, done * esize, m8 * esize});
+            pos += c;
+        }
+        if (m8 < m) {
+            const int64_t r = (m - m8) * esize;
+            if (r > chunk_bytes - pos) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: truncated trailing elements");
+            memcpy(out + (done + m8) * esize, chunk + pos, (size_t)r);
+            pos += r;
+        }
+        done += m;
+    }
+    std::atomic<int> bad{0};
+    if (!blocks.empty()) {
+        pool().run((int64_t)blocks.size(), threads <= 0 ? default_threads() : threads, [&](int64_t i) {
+            const Lz4Block& b = blocks[(size_t)i];
+            if (!lz4_block(chunk + b.src, b.csize, out + b.dst, b.bytes)) bad.store(1);
+        });
+    }
+    if (bad.load()) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: malformed LZ4 block");
+    *n_bytes = (int64_t)total;
+    *block_elems = belem;
+    return XI_OK;
+}

@@ -4,6 +4,8 @@
   (numpy, ideally pinned) or already on the device (torch). The kernels encode them (`xpg/io/images.py:72-102`).
   From a pinned torch tensor a transfer thread uploads them, mostly packed to one byte a pixel on the host's cores
   (`xi_pack_u8` / `xi_unpack_u8`).
+* `BSLZ4Frames`: bitshuffle-LZ4 chunks (Eiger HDF5 chunks) of uint32 / uint16 counts: the LZ4 stage on the host's
+  cores, the bit unshuffle on the device, then the uint32 path.
 * `ImageSetFrames`: any XPG-style image set (`first`, `last`, `nx`, `ny`, `get(frame)` -> float32 frame with -1
   masked / -2 overloaded, `xpg/io/images.py:59-102`); frames are stacked per wedge on the host and uploaded as
   float32.
@@ -460,9 +462,84 @@ class ImageSetFrames:
         return self._ring.upload(k, h, self.device), True
 
 
+class BSLZ4Frames:
+    """Frames as bitshuffle-LZ4 chunks (HDF5 filter 32008: Eiger data read with the filter bypassed, as XPG's
+    `read_chunk` gives them, `xpg/io/images.py:384-396`) of uint32 or uint16 counts. Each wedge: the LZ4 stage of its
+    chunks on the host's cores (xi_bslz4_lz4_stage) into pinned staging, one upload, the bit unshuffle on the device
+    (xi_bitunshuffle) into uint32 frames; from there the uint32 path (the gather encodes the counts: all-ones flagged,
+    counts >= overload overloaded), so the results are those of the same frames given raw.
+
+    chunks: a sequence (frame `first + i` at index i) or a callable frame -> chunk bytes."""
+
+    def __init__(self, chunks, ny, nx, esize=4, first=1, last=None, overload=1 << 20, min_valid=0, device="cuda"):
+        if esize not in (2, 4):
+            raise ValueError("esize: 2 or 4 bytes")
+        self.chunks = chunks
+        self.first = int(first)
+        self.last = int(last) if last is not None else self.first + len(chunks) - 1
+        self.ny, self.nx, self.esize = int(ny), int(nx), int(esize)
+        self.overload = int(overload) if overload is not None else None
+        self.min_valid = int(min_valid)
+        self.device = device
+        self.resident = False
+        self._ring = _PinnedRing(torch.uint8)
+
+    def _chunk(self, f):
+        c = self.chunks(f) if callable(self.chunks) else self.chunks[f - self.first]
+        if c is None:
+            raise RuntimeError(f"frame {f}: no chunk")
+        return np.frombuffer(c, np.uint8) if not isinstance(c, np.ndarray) else np.ascontiguousarray(c, np.uint8)
+
+    def wedge(self, f_a, f_b, ok=None, stream=None):
+        import ctypes as C
+        from . import native
+        lib = native.load()
+        n = f_b - f_a + 1
+        nel = self.ny * self.nx
+        fb = nel * self.esize
+        k, buf = self._ring.take(n * fb)
+        base = buf.data_ptr()
+        nb, be = C.c_int64(), C.c_int64()
+        belem = [0] * n
+        for w in range(n):
+            if ok is not None and not ok[w]:
+                continue                                   # excluded: never read (the gather skips the frame)
+            c = self._chunk(f_a + w)
+            native.check(lib.xi_bslz4_lz4_stage(c.ctypes.data, c.size, self.esize, C.c_void_p(base + w * fb), fb,
+                                                0, C.byref(nb), C.byref(be)), f"frame {f_a + w}: xi_bslz4_lz4_stage")
+            if nb.value != fb:
+                raise RuntimeError(f"frame {f_a + w}: chunk of {nb.value} bytes, frame of {fb}")
+            belem[w] = be.value
+        dev = self._ring.upload(k, buf, self.device)
+        d = torch.empty((n, self.ny, self.nx), dtype=torch.int32, device=dev.device)
+        st = native.stream_handle()
+        for w in range(n):
+            if belem[w]:
+                native.check(lib.xi_bitunshuffle(C.c_void_p(dev.data_ptr() + w * fb), nel, self.esize, belem[w],
+                                                 C.c_void_p(d[w].data_ptr()), st), "xi_bitunshuffle")
+        return d, False
+
+
 def as_frame_source(images, device="cuda"):
-    if isinstance(images, (U32Frames, ImageSetFrames)):
+    if isinstance(images, (U32Frames, ImageSetFrames, BSLZ4Frames)):
         return images
+    if _bitshuffled_imageset(images):
+        return BSLZ4Frames(images.read_chunk, images.ny, images.nx, esize=int(np.dtype(images.dtype).itemsize),
+                           first=images.first, last=images.last, overload=getattr(images, "overload", None),
+                           min_valid=getattr(images, "min_valid", 0), device=device)
     if hasattr(images, "get") and hasattr(images, "first"):
         return ImageSetFrames(images, device)
     raise TypeError("images: a U32Frames, ImageSetFrames or an XPG-style ImageSet (first, last, nx, ny, get)")
+
+
+def _bitshuffled_imageset(images):
+    """An XPG image set whose frames are plain bitshuffle-LZ4 chunks the device can finish (`bitshuffled_ok`,
+    `xpg/io/images.py:157-160`, `:365-382`) and whose encoding is the uint32 path's: no static pixel mask (a masked
+    pixel there reads -1 even when overloaded), no offset or dark frame."""
+    try:
+        if not (hasattr(images, "read_chunk") and images.bitshuffled_ok()):
+            return False
+    except Exception:
+        return False
+    sm = getattr(images, "static_mask", None)
+    return sm is None or bool(np.asarray(sm).all())

@@ -136,7 +136,8 @@ XI_PACK_ESCAPE, XI_PACK_FLAGGED = 254, 255
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
-           "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload")
+           "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
+           "xi_bitunshuffle")
 
 _LIB = None
 
@@ -174,6 +175,9 @@ def load(path=None):
                                C.POINTER(C.c_int64)]
     lib.xi_unpack_u8.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     lib.xi_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    lib.xi_bslz4_lz4_stage.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_int,
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.xi_bitunshuffle.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
     lib.xi_status.argtypes = [C.c_void_p]
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
