@@ -187,3 +187,66 @@ def test_accumulate_and_finalize_match_oracle():
     want = OK.finalize_profiles(num_o, den_o)
     got = prof.cpu().numpy()
     assert np.max(np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), 1e-30)) < 2.5e-7
+
+
+@pytest.mark.parametrize("with_partner", [False, True])
+def test_largest_box_matches_oracle(with_partner):
+    """The largest shoebox XPG plans (97 x 97 px, 65 frames: max(XY_BUCKETS), max(DZ_BUCKETS)) through pass 1 and
+    pass 2: a stored reflection's box pasted into a 97 x 97 x 65 box of Poisson background (with masked, unrecorded
+    and overloaded voxels), its origin moved so that the reflection stays centred, against the oracle."""
+    from xpg_b200 import device as D
+    case = "crowded" if with_partner else "config1"        # a partner (joint fit) in the crowded sweep's chunks
+    spec, tmpl, mask, excl = G.case_inputs(case)
+    g = spec.geometry()
+    det = D.DeviceDetector(g, tmpl)
+    odet = OK.detector_consts(g, tmpl)
+    i = next(k for k in G.chunks(case) if G.chunk(case, k)[4])
+    d, rc, nb, o1, o2 = G.chunk(case, i)
+    j = int(np.argmax(rc["has_p"])) if with_partner else int(np.argmin(rc["has_p"]))
+    assert (rc["has_p"][j] > 0.5) == with_partner
+    _, Dz0, Dy0, Dx0 = d["sb"].shape
+    bx, Dz = 97, 65
+    oy, ox = (bx - Dy0) // 2, (bx - Dx0) // 2
+    rng = np.random.default_rng(5)
+    sb = rng.poisson(1.5, (1, Dz, bx, bx)).astype(np.float32)
+    sb[0, :Dz0, oy:oy + Dy0, ox:ox + Dx0] = d["sb"][j]
+    flat = sb.reshape(-1)
+    flat[rng.choice(flat.size, 300, replace=False)] = -1.0
+    flat[rng.choice(flat.size, 30, replace=False)] = -2.0
+    sb[0, :, :3, :] = -3.0                                     # unrecorded rows at the box edge
+    one = {k: np.asarray(v[j:j + 1]).copy() for k, v in rc.items()}
+    one["ix0"] = one["ix0"] - ox
+    one["iy0"] = one["iy0"] - oy
+    nb1 = {k: np.asarray(v[j:j + 1]) for k, v in nb.items()}
+    rows = D.RowSet(S=one["S"], phi=one["phi"], ix0=one["ix0"], iy0=one["iy0"], iz0=one["iz0"], fb=one["fb"],
+                    region=one["region"], has_p=one["has_p"], pS=one["pS"], pphi=one["pphi"],
+                    pxs=np.ones(1, np.int32), Dz=np.full(1, Dz), bx=np.full(1, bx), nb=nb1, device="cuda",
+                    sb_bias=0.0)
+    arena = torch.as_tensor(sb.reshape(-1)).cuda()
+    blk, keep = _block(d)
+    p1 = D.Pass1Buffers(rows)
+    D.pass1(det, rows, blk, arena, p1)
+    D.status()
+    h1 = {k: v.cpu().numpy() for k, v in p1.t.items()}
+    mine = _row_out(h1, rows, 0)
+    r0 = G.row_dict(one, 0)
+    ref = OK.pass1(sb[0], r0, G.nb_row(nb1, 0), odet, d["s0"], d["axis"], d["frames_phi0"], d["osc"], d["sd"],
+                   d["sm"], d["gain"], d["rcw"])
+    for k in EXACT:
+        assert np.array_equal(np.asarray(mine[k]).astype(np.float64), np.asarray(ref[k]).astype(np.float64)), k
+    for k in ("isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "img2", "fz"):
+        ok, worst = T.within(k, mine[k], ref[k], ref, rel=1e-5)
+        assert ok, (k, worst)
+    prof = torch.as_tensor(d["prof"]).cuda()
+    blk2, keep2 = _block(d, "p2_")
+    p2 = D.Pass2Buffers(rows)
+    D.pass2(det, rows, blk2, arena, prof, p1, p2)
+    D.status()
+    got = {k: v.cpu().numpy()[0] for k, v in p2.t.items()}
+    pix = dict(zeta=mine["zeta"], J=mine["J"], u1=mine["u1"], u2=mine["u2"], seff=mine["seff"])
+    want = OK.pass2(sb[0], r0, G.nb_row(nb1, 0), odet, d["s0"], d["axis"], d["frames_phi0"], d["osc"], d["p2_sd"],
+                    d["p2_sm"], d["p2_gain"], d["prof"], mine["bg"], mine["nbg"], d["p2_rcw"], pix)
+    ctx = dict(want, vsum=mine["vsum"])
+    for k in want:
+        ok, worst = T.within(k, got[k], want[k], ctx, rel=2e-6)
+        assert ok, (k, worst, got[k], want[k])

@@ -253,15 +253,25 @@ __device__ void rocking_curve_cta(int Dz, int iz0, float fb, const XiBlock& B, c
     __syncthreads();
 }
 
-// Per-pixel neighbour frame masks and background template of a box, computed once (shared memory).
+// Per-pixel neighbour frame masks and background template of a box, computed once (shared memory). Frame 64's bit
+// (boxes of 65 frames) goes to nbhi: one word per pixel, or (hi_bits) one bit per pixel, pixel p at bit p % 32 of
+// word p / 32 (the form pass 2 uses, so that its tables fit the largest boxes).
 __device__ void pixel_tables(const XiDetector& det, const NbShared& nb, const NbTab& tb, int bx, int Dz, const float* xs,
-                             const float* ys, unsigned long long* nblo, unsigned* nbhi, float* brefs) {
+                             const float* ys, unsigned long long* nblo, unsigned* nbhi, float* brefs,
+                             bool hi_bits = false) {
     const int P = bx * bx;
+    if (nbhi && hi_bits) {
+        for (int w = threadIdx.x; w < (P + 31) / 32; w += blockDim.x) nbhi[w] = 0u;
+        __syncthreads();
+    }
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const int i = p % bx, j = p / bx;
         const Mask65 m = neighbour_frames(nb, tb, i, j, Dz);
         nblo[p] = m.lo;
-        if (nbhi) nbhi[p] = m.hi;
+        if (nbhi) {
+            if (!hi_bits) nbhi[p] = m.hi;
+            else if (m.hi & 1u) atomicOr(&nbhi[p >> 5], 1u << (p & 31));
+        }
         brefs[p] = bkg_ref(det, xs[i], ys[j]);
     }
     __syncthreads();
@@ -794,10 +804,10 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
 // pass 2
 // ==================================================================================================================
 // Dynamic shared memory: nblo (8P, first the partner's eps1 / eps2) | P2s (4P) | P2ps (4P) | brefs (4P, first the
-// partner's J) | nbhi (4P; only when boxes reach frame 64, whose bit it holds) | fit list (8 x cap, first the
-// rocking-curve terms) | staged net counts of the fitted voxels (4V, when STAGED).
+// partner's J) | nbhi (one bit per pixel, only when boxes reach frame 64, whose bit it holds) | fit list (8 x cap,
+// first the rocking-curve terms) | staged net counts of the fitted voxels (4V, when STAGED).
 __host__ __device__ inline size_t pass2_pix_bytes(int P, int max_dz) {
-    return ((size_t)(max_dz > 64 ? 24 : 20) * P + 15) / 16 * 16;
+    return ((size_t)20 * P + (max_dz > 64 ? (size_t)(P + 31) / 32 * 4 : 0) + 15) / 16 * 16;
 }
 __host__ __device__ inline size_t pass2_list_bytes(int cap) {
     const size_t b = (size_t)8 * cap, t = (size_t)XI_MAX_DZ * XI_RC_K * sizeof(float);
@@ -842,7 +852,8 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     float* P2ps = P2s + Pm;
     float* brefs = P2ps + Pm;
     float* Jps = brefs;                                   // partner J, before brefs is written
-    unsigned* nbhi = max_dz > 64 ? reinterpret_cast<unsigned*>(brefs + Pm) : nullptr;   // frame 64's bit
+    unsigned* nbhi = max_dz > 64 ? reinterpret_cast<unsigned*>(brefs + Pm) : nullptr;   // frame 64's bits
+    auto hi_bit = [&](int p) -> unsigned { return nbhi ? (nbhi[p >> 5] >> (p & 31)) & 1u : 0u; };
     float* ul_v = reinterpret_cast<float*>(dyn2 + pass2_pix_bytes(Pm, max_dz));      // fit list: net counts
     float* terms = ul_v;                                  // rocking-curve terms, before the fit list is written
     unsigned* ul_i = reinterpret_cast<unsigned*>(ul_v + cap);                 // fit list: z << 16 | pixel
@@ -941,7 +952,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
         __syncthreads();
     }
     neighbour_setup(R, row, Dz, bx, xs, ys, fzz, has_p, nb, tb);     // ends with a barrier (partner scratch free)
-    pixel_tables(det, nb, tb, bx, Dz, xs, ys, nblo, nbhi, brefs);
+    pixel_tables(det, nb, tb, bx, Dz, xs, ys, nblo, nbhi, brefs, true);
     const float pthr = 0.01f * s_pmax;
     const float ppthr = 0.01f * fmaxf(s_ppmax, 1e-12f);
 
@@ -988,7 +999,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                 const unsigned long long nl = nblo[p];
                 nbw[0] = (unsigned)nl;
                 nbw[1] = (unsigned)(nl >> 32);
-                nbw[2] = nbhi ? nbhi[p] : 0u;
+                nbw[2] = hi_bit(p);
             }
             const float bpix = bg * bref;
             const float iv0 = __frcp_rn(gain * fmaxf(bpix, kVarFloor));
@@ -1066,7 +1077,10 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
                 if (fg2) a8[4] += (double)P2 * r_fg;
                 if (STAGED) {                    // the neighbour mask is not needed any more: keep the fit mask
                     nblo[p] = (unsigned long long)umw[0] | ((unsigned long long)umw[1] << 32);
-                    if (nbhi) nbhi[p] = umw[2];
+                    if (nbhi) {                  // this pixel's bit only: other threads own the word's others
+                        if (umw[2] & 1u) atomicOr(&nbhi[p >> 5], 1u << (p & 31));
+                        else atomicAnd(&nbhi[p >> 5], ~(1u << (p & 31)));
+                    }
                 }
             }
         }
@@ -1102,7 +1116,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
             const float P2 = P2s[p], P2p = P2ps[p];
             Mask65 nbm;
             nbm.lo = nblo[p];
-            nbm.hi = nbhi ? nbhi[p] : 0u;
+            nbm.hi = hi_bit(p);
             for (int z = 0; z < Dz; ++z) {
                 if (STAGED) {
                     if (!nbm.get(z)) continue;   // fit mask
@@ -1561,18 +1575,31 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     cudaStream_t s = (cudaStream_t)stream;
     const size_t P = (size_t)R->max_bx * R->max_bx;
     const size_t V = P * R->max_dz;
-    if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > kStageBudget)
-        return fail(XI_E_LIMIT, "xi_pass2: box too large (per-pixel tables exceed shared memory)");
+    // the largest boxes (up to 97 px, 65 frames) take what the device allows a CTA beyond the kernel's static arrays
+    // and the neighbour tables, not the default budget
+    size_t budget = kStageBudget;
+    if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > budget) {
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+            cudaFuncGetAttributes(&fa, k_pass2<256, false>) != cudaSuccess)
+            return cuda_check("xi_pass2: shared memory limits");
+        const size_t fixed = fa.sharedSizeBytes + nb_bytes(R->K, R->max_bx, R->max_dz);
+        budget = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
+        if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > budget)
+            return fail(XI_E_LIMIT, "xi_pass2: box too large (per-pixel tables exceed shared memory)");
+    }
     // the fit list holds up to every voxel of small boxes and 2048 fitted voxels of large ones; the box itself is
     // staged only when small (it is read once: staging buys the copy's overlap with the set-up, not re-reads)
     // (the list shrinks to what shared memory leaves beside the tables; rows whose list overflows fit from the box)
-    const size_t fit = (kStageBudget - pass2_pix_bytes((int)P, R->max_dz)) / 8 / 4 * 4;
+    const size_t fit = (budget - pass2_pix_bytes((int)P, R->max_dz)) / 8 / 4 * 4;
     size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
     if (capz > fit) capz = fit;
     const int cap = (int)capz;
     const size_t base = pass2_stage_offset((int)P, R->max_dz, cap);
-    if (base > kStageBudget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
-    const bool staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= kStageBudget;
+    if (base > budget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
+    const bool staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= budget;
     if (staged) {
         if (P <= 96) return launch_pass2<64, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
         if (P <= 200) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
