@@ -32,7 +32,7 @@ def _worker(rank, world, port, out):
 
 def test_replicas_reduce_over_two_gloo_ranks():
     port = _free_port()
-    manager = mp.Manager()
+    manager = mp.get_context("spawn").Manager()     # no fork of a process that runs threads
     out = manager.dict()
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, start_method="spawn")
     assert out[0][:2] == (2.0, 300) and out[1][:2] == (2.0, 300)
