@@ -376,6 +376,25 @@ int xi_bslz4_lz4_stage(const uint8_t *chunk, int64_t chunk_bytes, int esize, uin
  * of the uint32 frame path). */
 int xi_bitunshuffle(const uint8_t *in, int64_t n_elem, int esize, int64_t block_elems, uint32_t *out, void *stream);
 
+/* ---- INTEGRATE.HKL records ---------------------------------------------------------------------------------------
+ * The data records of XPG's INTEGRATE.HKL (`write_integrate_hkl`, xpg/io/legacy.py:171-176), formatted in parallel. */
+typedef struct {
+    int64_t n;
+    const int64_t *hkl;             /* (n, 3) */
+    const double *I, *sig;          /* LP-corrected intensity and its sigma */
+    const double *x, *y, *zc;       /* calculated position (zc: frame coordinate kept inside its frame) */
+    const double *rlp, *peak;
+    const int64_t *corr;
+    const double *xo, *yo, *zo;     /* observed position (the calculated one where not observed) */
+    const double *alf1, *bet1;      /* diffracted beam direction: spherical angles (deg) */
+    double alf0, bet0;              /* incident beam direction */
+} XiHklRows;
+
+/* Host function: n lines " H K L I SIGMA XCAL YCAL ZCAL RLP PEAK CORR 0 XOBS YOBS ZOBS ALF0 BET0 ALF1 BET1 0.00 1"
+ * (formats %.3E for I and SIGMA, %.1f positions, %.5f RLP and PEAK, %.2f angles) into out; *n_bytes gets the text's
+ * size. XI_E_LIMIT when cap is smaller (then nothing is written and *n_bytes is the size needed). */
+int xi_format_integrate_hkl(const XiHklRows *rows, char *out, int64_t cap, int threads, int64_t *n_bytes);
+
 /* Copies `bytes` from page-locked host memory (cudaHostAlloc / cudaHostRegister, mapped into the device's address
  * space) to device memory with a kernel that reads the host memory over the link: unlike cudaMemcpyAsync it does not
  * queue behind the copies already waiting in the copy engine (the frame chunks), so a small upload is not delayed by

@@ -1,9 +1,11 @@
-// Host side of the frames' transfer encoding (include/xpgi.h, "Transfer encoding"): uint32 pixels to one byte each
-// plus (index, value) exceptions, on a pool of host threads. The work is a streaming read of the frames, so the pool
+// Host-side codecs of the library, on a pool of host threads: the frames' transfer encoding (include/xpgi.h,
+// "Transfer encoding": uint32 pixels to one byte each plus (index, value) exceptions), the LZ4 stage of
+// bitshuffle-LZ4 chunks, and the INTEGRATE.HKL records. The transfer encoding: The work is a streaming read of the frames, so the pool
 // splits a run into slices of kSlice pixels handed out in order; each slice records which of its kBlock-pixel
 // blocks hold an exception, and the calling thread lists those blocks' exceptions afterwards, in pixel order.
 #include <immintrin.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -11,6 +13,7 @@
 #include <condition_variable>
 #include <functional>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -293,5 +296,64 @@ extern "C" int xi_bslz4_lz4_stage(const uint8_t* chunk, int64_t chunk_bytes, int
     if (bad.load()) return xi_fail(XI_E_ARG, "xi_bslz4_lz4_stage: malformed LZ4 block");
     *n_bytes = (int64_t)total;
     *block_elems = belem;
+    return XI_OK;
+}
+
+// ---- INTEGRATE.HKL data records ---------------------------------------------------------------------------------
+// Rows are formatted in chunks on the pool (C's printf conversions %.3E / %.1f / %.5f / %.2f round exactly as the
+// Python format specifications of the same names), then concatenated in row order.
+#include <stdio.h>
+#include <string>
+
+namespace {
+
+void hkl_line(const XiHklRows* r, int64_t i, std::string& s) {
+    char line[512];
+    auto fmt = [&](char* buf, size_t cap) {
+        return snprintf(buf, cap,
+                        " %lld %lld %lld %.3E %.3E %.1f %.1f %.1f %.5f %.5f %lld 0 %.1f %.1f %.1f %.2f %.2f %.2f %.2f "
+                        "0.00 1\n",
+                        (long long)r->hkl[3 * i], (long long)r->hkl[3 * i + 1], (long long)r->hkl[3 * i + 2], r->I[i],
+                        r->sig[i], r->x[i], r->y[i], r->zc[i], r->rlp[i], r->peak[i], (long long)r->corr[i], r->xo[i],
+                        r->yo[i], r->zo[i], r->alf0, r->bet0, r->alf1[i], r->bet1[i]);
+    };
+    const int n = fmt(line, sizeof line);
+    if (n < 0) return;
+    if ((size_t)n < sizeof line) {
+        s.append(line, (size_t)n);
+    } else {                                        // a huge value: format again at its length
+        std::vector<char> big((size_t)n + 1);
+        fmt(big.data(), big.size());
+        s.append(big.data(), (size_t)n);
+    }
+}
+
+}  // namespace
+
+extern "C" int xi_format_integrate_hkl(const XiHklRows* r, char* out, int64_t cap, int threads, int64_t* n_bytes) {
+    if (!r || !n_bytes || r->n < 0 || cap < 0 || (cap && !out))
+        return xi_fail(XI_E_ARG, "xi_format_integrate_hkl: null pointer or negative size");
+    if (r->n && (!r->hkl || !r->I || !r->sig || !r->x || !r->y || !r->zc || !r->rlp || !r->peak || !r->corr ||
+                 !r->xo || !r->yo || !r->zo || !r->alf1 || !r->bet1))
+        return xi_fail(XI_E_ARG, "xi_format_integrate_hkl: null column");
+    const int64_t per = 4096;
+    const int64_t n_items = (r->n + per - 1) / per;
+    std::vector<std::string> parts((size_t)n_items);
+    if (n_items)
+        pool().run(n_items, threads <= 0 ? default_threads() : threads, [&](int64_t it) {
+            std::string& s = parts[(size_t)it];
+            s.reserve((size_t)per * 128);
+            const int64_t a = it * per, b = std::min(r->n, a + per);
+            for (int64_t i = a; i < b; ++i) hkl_line(r, i, s);
+        });
+    int64_t total = 0;
+    for (const auto& s : parts) total += (int64_t)s.size();
+    *n_bytes = total;
+    if (total > cap) return xi_fail(XI_E_LIMIT, "xi_format_integrate_hkl: buffer too small (size in *n_bytes)");
+    int64_t o = 0;
+    for (const auto& s : parts) {
+        memcpy(out + o, s.data(), s.size());
+        o += (int64_t)s.size();
+    }
     return XI_OK;
 }

@@ -130,6 +130,13 @@ class XiRocking(C.Structure):
                 ("osc", C.c_double), ("z_shift", C.c_double)]
 
 
+class XiHklRows(C.Structure):
+    _fields_ = [("n", C.c_int64), ("hkl", C.c_void_p), ("I", C.c_void_p), ("sig", C.c_void_p), ("x", C.c_void_p),
+                ("y", C.c_void_p), ("zc", C.c_void_p), ("rlp", C.c_void_p), ("peak", C.c_void_p),
+                ("corr", C.c_void_p), ("xo", C.c_void_p), ("yo", C.c_void_p), ("zo", C.c_void_p),
+                ("alf1", C.c_void_p), ("bet1", C.c_void_p), ("alf0", C.c_double), ("bet0", C.c_double)]
+
+
 XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP = 1, 2, 3
 XI_PACK_ESCAPE, XI_PACK_FLAGGED = 254, 255
 
@@ -137,7 +144,7 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
            "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
-           "xi_bitunshuffle")
+           "xi_bitunshuffle", "xi_format_integrate_hkl")
 
 _LIB = None
 
@@ -178,6 +185,8 @@ def load(path=None):
     lib.xi_bslz4_lz4_stage.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_int,
                                        C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.xi_bitunshuffle.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+    lib.xi_format_integrate_hkl.argtypes = [C.POINTER(XiHklRows), C.c_void_p, C.c_int64, C.c_int,
+                                            C.POINTER(C.c_int64)]
     lib.xi_status.argtypes = [C.c_void_p]
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]

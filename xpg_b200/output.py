@@ -194,13 +194,37 @@ def write_integrate_hkl(path, exp, refl, data_range, sigma_m, sigma_d, template=
     yo = np.where(np.isfinite(refl["yo"]), refl["yo"], refl["y"])
     zo = _frame_safe(np.where(np.isfinite(refl["zo"]), refl["zo"], refl["z"]))
     zc = _frame_safe(refl["z"])
-    h = np.asarray(refl["hkl"], int)
-    corr = np.nan_to_num(refl["corr"]).astype(int)
-    rows = [f" {h[i, 0]} {h[i, 1]} {h[i, 2]} {refl['I'][i]:.3E} {refl['sig'][i]:.3E} {refl['x'][i]:.1f} "
-            f"{refl['y'][i]:.1f} {zc[i]:.1f} {refl['rlp'][i]:.5f} {float(refl['peak'][i]):.5f} {corr[i]:d} 0 "
-            f"{xo[i]:.1f} {yo[i]:.1f} {zo[i]:.1f} {alf0:.2f} {bet0:.2f} {alf1[i]:.2f} {bet1[i]:.2f} 0.00 1\n"
-            for i in range(n)]
-    with open(path, "w") as f:
-        f.write("\n".join(head) + "\n")
-        f.writelines(rows)
-        f.write("!END_OF_DATA\n")
+    body = _records(n, refl, zc, xo, yo, zo, alf0, bet0, alf1, bet1)
+    with open(path, "wb") as f:
+        f.write(("\n".join(head) + "\n").encode())
+        f.write(body)
+        f.write(b"!END_OF_DATA\n")
+
+
+def _records(n, refl, zc, xo, yo, zo, alf0, bet0, alf1, bet1):
+    """The data records, formatted by the library on the host's cores (xi_format_integrate_hkl)."""
+    import ctypes as C
+    from . import native as N
+    f64 = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64), (n,)))
+    cols = dict(hkl=np.ascontiguousarray(np.asarray(refl["hkl"], np.int64).reshape(n, 3)), I=f64(refl["I"]),
+                sig=f64(refl["sig"]), x=f64(refl["x"]), y=f64(refl["y"]), zc=f64(zc), rlp=f64(refl["rlp"]),
+                peak=f64(refl["peak"]), corr=np.ascontiguousarray(np.nan_to_num(np.asarray(refl["corr"], np.float64))
+                                                                  .astype(np.int64)),
+                xo=f64(xo), yo=f64(yo), zo=f64(zo), alf1=f64(alf1), bet1=f64(bet1))
+    r = N.XiHklRows()
+    r.n = n
+    for k, v in cols.items():
+        setattr(r, k, v.ctypes.data)
+    r.alf0, r.bet0 = float(alf0), float(bet0)
+    lib = N.load()
+    need = C.c_int64()
+    cap = 160 * n
+    for _ in range(2):
+        buf = np.empty(max(cap, 1), np.uint8)
+        rc = lib.xi_format_integrate_hkl(C.byref(r), buf.ctypes.data, cap, 0, C.byref(need))
+        if rc == N.XI_OK:
+            return buf[:need.value].tobytes()
+        if rc != N.XI_E_LIMIT:
+            N.check(rc, "xi_format_integrate_hkl")
+        cap = need.value
+    N.check(rc, "xi_format_integrate_hkl")
