@@ -376,6 +376,25 @@ int xi_bslz4_lz4_stage(const uint8_t *chunk, int64_t chunk_bytes, int esize, uin
  * of the uint32 frame path). */
 int xi_bitunshuffle(const uint8_t *in, int64_t n_elem, int esize, int64_t block_elems, uint32_t *out, void *stream);
 
+/* ---- Spot finding: the strong-pixel classifier -------------------------------------------------------------------
+ * XPG's `make_finder(nbx, nby, signal_pixel, background_pixel, min_local, extended)` (xpg/spotfind.py:27-97): the
+ * dispersion test (Kabsch 2010) on a (2 nby + 1) x (2 nbx + 1) window, then (extended) the local background
+ * re-estimated over a (2 (2 nby + 1) + 1) x (2 (2 nbx + 1) + 1) window from pixels away from first-pass signal.
+ * float32 frames (negative: not valid), bit for bit with the reference. */
+#define XI_SPOT_MAX_HALF 8
+typedef struct {
+    int nbx, nby;                   /* window half-sizes, 0..XI_SPOT_MAX_HALF */
+    float signal_pixel, background_pixel;
+    int min_local;
+    int extended;                   /* 1: the second pass */
+} XiSpotParams;
+
+/* Device scratch of an extended call (bytes). */
+size_t xi_spot_workspace(int n_frames, int ny, int nx);
+/* strong (uint8 0 / 1) and mean (float32) per pixel of n_frames frames of ny x nx float32 pixels (device). */
+int xi_spot_strong(const float *img, int n_frames, int ny, int nx, float gain, const XiSpotParams *params,
+                   uint8_t *strong, float *mean, void *ws, size_t ws_bytes, void *stream);
+
 /* ---- INTEGRATE.HKL records ---------------------------------------------------------------------------------------
  * The data records of XPG's INTEGRATE.HKL (`write_integrate_hkl`, xpg/io/legacy.py:171-176), formatted in parallel. */
 typedef struct {

@@ -130,6 +130,14 @@ class XiRocking(C.Structure):
                 ("osc", C.c_double), ("z_shift", C.c_double)]
 
 
+class XiSpotParams(C.Structure):
+    _fields_ = [("nbx", C.c_int), ("nby", C.c_int), ("signal_pixel", C.c_float), ("background_pixel", C.c_float),
+                ("min_local", C.c_int), ("extended", C.c_int)]
+
+
+XI_SPOT_MAX_HALF = 8
+
+
 class XiHklRows(C.Structure):
     _fields_ = [("n", C.c_int64), ("hkl", C.c_void_p), ("I", C.c_void_p), ("sig", C.c_void_p), ("x", C.c_void_p),
                 ("y", C.c_void_p), ("zc", C.c_void_p), ("rlp", C.c_void_p), ("peak", C.c_void_p),
@@ -144,7 +152,7 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
            "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
-           "xi_bitunshuffle", "xi_format_integrate_hkl")
+           "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong", "xi_spot_workspace")
 
 _LIB = None
 
@@ -185,6 +193,10 @@ def load(path=None):
     lib.xi_bslz4_lz4_stage.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_int,
                                        C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.xi_bitunshuffle.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+    lib.xi_spot_workspace.restype = C.c_size_t
+    lib.xi_spot_workspace.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.xi_spot_strong.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(XiSpotParams),
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     lib.xi_format_integrate_hkl.argtypes = [C.POINTER(XiHklRows), C.c_void_p, C.c_int64, C.c_int,
                                             C.POINTER(C.c_int64)]
     lib.xi_status.argtypes = [C.c_void_p]
