@@ -112,9 +112,60 @@ def lp_correct(refl, g, air=True):
     return _rows(refl, lat == 0), extra
 
 
-def write_integrated_npz(path, refl):
-    """`xpg_integrated.npz`: every per-reflection array of the corrected rows but the per-frame profiles fz."""
-    np.savez_compressed(path, **{k: v for k, v in refl.items() if isinstance(v, np.ndarray) and k != "fz"})
+def write_integrated_npz(path, refl, threads=None):
+    """`xpg_integrated.npz`: every per-reflection array of the corrected rows but the per-frame profiles fz, in the
+    file numpy's `savez_compressed` writes (a zip of deflated `.npy` members, read back by `np.load`), its members
+    compressed on `threads` host threads at once (zlib releases the interpreter lock)."""
+    arrays = {k: v for k, v in refl.items() if isinstance(v, np.ndarray) and k != "fz"}
+    _write_npz_parallel(path, arrays, threads)
+
+
+def _npy_bytes(a):
+    import io
+    buf = io.BytesIO()
+    np.lib.format.write_array(buf, np.asanyarray(a), allow_pickle=False)
+    return buf.getvalue()
+
+
+def _deflate(raw):
+    import zlib
+    c = zlib.compressobj(6, zlib.DEFLATED, -15)          # raw deflate, zipfile's default level
+    return c.compress(raw) + c.flush(), zlib.crc32(raw) & 0xFFFFFFFF
+
+
+def _write_npz_parallel(path, arrays, threads=None):
+    """A zip of deflated .npy members (local headers, data, central directory: the PKWARE APPNOTE layout zipfile
+    writes); members over 4 GiB, or a file over 4 GiB, go through numpy's own writer (zip64)."""
+    import os
+    import struct
+    import time as _time
+    from concurrent.futures import ThreadPoolExecutor
+    names = list(arrays)
+    raws = [_npy_bytes(arrays[k]) for k in names]
+    if sum(len(r) for r in raws) >= 0xFFFFFFFF // 2:
+        np.savez_compressed(path, **arrays)
+        return
+    n_th = threads or max(1, min(len(raws), (os.cpu_count() or 2) - 1))
+    with ThreadPoolExecutor(n_th) as ex:
+        packed = list(ex.map(_deflate, raws))
+    t = _time.localtime()
+    dtime = (t.tm_hour << 11) | (t.tm_min << 5) | (t.tm_sec // 2)
+    ddate = ((t.tm_year - 1980) << 9) | (t.tm_mon << 5) | t.tm_mday
+    central, off = [], 0
+    with open(path, "wb") as f:
+        for k, raw, (data, crc) in zip(names, raws, packed):
+            name = (k + ".npy").encode()
+            head = struct.pack("<IHHHHHIIIHH", 0x04034B50, 20, 0, 8, dtime, ddate, crc, len(data), len(raw),
+                               len(name), 0)
+            f.write(head)
+            f.write(name)
+            f.write(data)
+            central.append(struct.pack("<IHHHHHHIIIHHHHHII", 0x02014B50, 20, 20, 0, 8, dtime, ddate, crc, len(data),
+                                       len(raw), len(name), 0, 0, 0, 0, 0o600 << 16, off) + name)
+            off += len(head) + len(name) + len(data)
+        cd = b"".join(central)
+        f.write(cd)
+        f.write(struct.pack("<IHHHHIIH", 0x06054B50, 0, 0, len(names), len(names), len(cd), off, 0))
 
 
 def _frame_safe(z):
