@@ -158,3 +158,36 @@ def test_decode_fixture_is_the_band():
     rc, got, be = _stage(chunk, 4, band.nbytes)
     assert rc == native.XI_OK
     assert np.array_equal(B.unshuffle(got, band.size, 4, be).view(np.uint32), band.reshape(-1))
+
+
+def test_imageset_adapter_takes_bitshuffled_chunks():
+    """An XPG image set whose frames are plain bitshuffle-LZ4 chunks (`bitshuffled_ok`, `read_chunk`) is read as
+    chunks; one with a static pixel mask (whose encoding differs) or without chunks goes through `get`."""
+    from xpg_b200 import frames as FR
+
+    class Images:
+        first, last, ny, nx = 1, 3, 37, 61
+        dtype = np.dtype(np.uint32)
+        overload, min_valid = 1 << 20, 0
+        static_mask = None
+
+        def bitshuffled_ok(self):
+            return True
+
+        def read_chunk(self, f):
+            return B.encode_chunk(_frame(37 * 61, f, 4), 4)
+
+        def get(self, f):
+            raise AssertionError("not used")
+
+    im = Images()
+    src = FR.as_frame_source(im, device="cpu")
+    assert isinstance(src, FR.BSLZ4Frames) and src.esize == 4 and src.overload == 1 << 20
+    assert src._chunk(2).tobytes() == im.read_chunk(2)
+    im.static_mask = np.ones((37, 61), bool)
+    assert isinstance(FR.as_frame_source(im, device="cpu"), FR.BSLZ4Frames)    # an all-True mask masks nothing
+    im.static_mask[3, 4] = False
+    assert isinstance(FR.as_frame_source(im, device="cpu"), FR.ImageSetFrames)
+    im.static_mask = None
+    im.bitshuffled_ok = lambda: False
+    assert isinstance(FR.as_frame_source(im, device="cpu"), FR.ImageSetFrames)
