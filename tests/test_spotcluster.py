@@ -1,0 +1,64 @@
+"""Clustering of strong pixels into spots (`xpg/spotcluster.py`), on the host: `cluster_spots` against XPG's own
+accumulator's spots (tests/golden/spotcluster.npz, made by tests/golden/make_spotcluster_golden.py) on the strong
+pixels of seeded runs: isolated spots, touching pairs (split at their separated peaks), and a ring of signal over every
+frame (one cluster with hundreds of peaks: the huge-cluster rules), for two pixel-count ranges. Also `find_spots`'
+glue (classifier, strong pixels read back, clustering) with the oracle's classifier on CPU tensors."""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from xpg_b200 import spotcluster as SC
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE / "golden"))
+import make_spotcluster_golden as M  # noqa: E402
+
+KEYS = ("x", "y", "z", "intensity", "npix", "zmin", "zmax")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    z = np.load(HERE / "golden" / "spotcluster.npz")
+    return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("case", M.CASES, ids=lambda c: f"case{c[0]}")
+def test_cluster_spots_matches_reference(case, gold):
+    k, y, x, v, b, ny, nx = M.strong_pixels(*case)
+    for ri, (mn, mx) in enumerate(M.RANGES):
+        got = SC.cluster_spots(k, y, x, v, b, nx, ny, mn, mx, 3.0, 2)
+        for key in KEYS:
+            assert np.array_equal(got[key], gold[f"c{case[0]}_r{ri}_{key}"]), (case[0], ri, key)
+
+
+def test_cluster_spots_empty_and_single():
+    e = np.zeros(0, np.int32)
+    got = SC.cluster_spots(e, e, e, e.astype(np.float32), e.astype(np.float32), 10, 10, 1, 100)
+    assert all(got[k].size == 0 for k in KEYS)
+    got = SC.cluster_spots([3], [4], [5], [10.0], [1.0], 10, 10, 1, 100)
+    assert got["npix"].tolist() == [1] and got["x"].tolist() == [6.0] and got["z"].tolist() == [3.5]
+
+
+def test_find_spots_glue_with_the_oracle_classifier():
+    import torch
+    from oracle import spotfind as OS
+    from xpg_b200.spotfind import find_spots
+    rng = np.random.default_rng(2)
+    img = rng.poisson(0.5, (6, 80, 90)).astype(np.float32)
+    img[2:4, 30:34, 40:44] += 60.0
+    img[1:3, 60:63, 10:13] += 40.0
+
+    def finder(t, gain):
+        s, m = OS.find(t.numpy(), gain)
+        return torch.from_numpy(s), torch.from_numpy(m)
+    got = find_spots(torch.from_numpy(img), 1.0, first_frame=10, finder=finder, min_pix=4)
+    s, m = OS.find(img, 1.0)
+    k, y, x = np.nonzero(s)
+    want = SC.cluster_spots(k + 10, y, x, img[k, y, x], m[k, y, x], 90, 80, 4, 1000000)
+    assert len(got["x"]) >= 2
+    for key in KEYS:
+        assert np.array_equal(got[key], want[key]), key

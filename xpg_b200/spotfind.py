@@ -37,3 +37,19 @@ def make_finder(nbx=3, nby=3, signal_pixel=3.0, background_pixel=2.0, min_local=
         return strong.bool().reshape(shape), mean.reshape(shape)
 
     return find
+
+
+def find_spots(img, gain=1.0, first_frame=0, finder=None, min_pix=1, max_pix=1000000, max_centroid_dist=3.0,
+               cluster_radius=2, **finder_args):
+    """Spots of a stack of frames img (n, ny, nx) float32 (negative: not valid), frame index first_frame + k for
+    img[k]: the strong pixels of the device classifier (`make_finder(**finder_args)` unless `finder` is given),
+    read back, then clustered on the host (`spotcluster.cluster_spots`, XPG's clustering all at once). Returns the
+    spot arrays x, y (pixels), z (frame coordinate), intensity, npix, zmin, zmax as XPG's `SpotList` holds them."""
+    from .spotcluster import cluster_spots
+    finder = finder or make_finder(**finder_args)
+    strong, mean = finder(img, float(gain))
+    k, y, x = torch.nonzero(strong, as_tuple=True)
+    v, b = img[k, y, x], mean[k, y, x]
+    k, y, x, v, b = (t.cpu().numpy() for t in (k, y, x, v, b))
+    return cluster_spots(k + int(first_frame), y, x, v, b, int(img.shape[2]), int(img.shape[1]), min_pix, max_pix,
+                         max_centroid_dist, cluster_radius)
