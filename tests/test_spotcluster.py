@@ -2,7 +2,7 @@
 accumulator's spots (tests/golden/spotcluster.npz, made by tests/golden/make_spotcluster_golden.py) on the strong
 pixels of seeded runs: isolated spots, touching pairs (split at their separated peaks), and a ring of signal over every
 frame (one cluster with hundreds of peaks: the huge-cluster rules), for two pixel-count ranges. Also `find_spots`'
-glue (classifier, strong pixels read back, clustering) with the oracle's classifier on CPU tensors."""
+glue for a frame stack (classifier, strong pixels read back, clustering) with the oracle's classifier on CPU tensors."""
 from __future__ import annotations
 
 import sys
@@ -43,10 +43,10 @@ def test_cluster_spots_empty_and_single():
     assert got["npix"].tolist() == [1] and got["x"].tolist() == [6.0] and got["z"].tolist() == [3.5]
 
 
-def test_find_spots_glue_with_the_oracle_classifier():
+def test_stack_glue_with_the_oracle_classifier():
     import torch
     from oracle import spotfind as OS
-    from xpg_b200.spotfind import find_spots
+    from xpg_b200.spotfind import spots_of_stack
     rng = np.random.default_rng(2)
     img = rng.poisson(0.5, (6, 80, 90)).astype(np.float32)
     img[2:4, 30:34, 40:44] += 60.0
@@ -55,10 +55,57 @@ def test_find_spots_glue_with_the_oracle_classifier():
     def finder(t, gain):
         s, m = OS.find(t.numpy(), gain)
         return torch.from_numpy(s), torch.from_numpy(m)
-    got = find_spots(torch.from_numpy(img), 1.0, first_frame=10, finder=finder, min_pix=4)
+    got = spots_of_stack(torch.from_numpy(img), 1.0, first_frame=10, finder=finder, min_pix=4)
     s, m = OS.find(img, 1.0)
     k, y, x = np.nonzero(s)
     want = SC.cluster_spots(k + 10, y, x, img[k, y, x], m[k, y, x], 90, 80, 4, 1000000)
     assert len(got["x"]) >= 2
     for key in KEYS:
         assert np.array_equal(got[key], want[key]), key
+
+
+def test_find_spots_matches_reference():
+    """The drop-in `find_spots` (XPG's signature) against XPG's own run on the same image set: batches of 4 frames, a
+    gap in the frame numbers, a static mask; the classifier here is the oracle's (on CPU tensors, bit-identical to
+    XPG's classifier and to the device's), so what is compared is the batching, masking, read-back, clustering and
+    the spot order (XPG's streaming clustering emits spots flush by flush)."""
+    import torch
+    import make_findspots_golden as F
+    from oracle import spotfind as OS
+    from oracle.gather import prepare_frame
+    from xpg_b200.spotfind import find_spots
+    raw = F.raw_frames()
+
+    class Images:
+        nx, ny, first, last = F.NX, F.NY, 1, F.NF
+
+        def get(self, f):
+            return prepare_frame(raw[f - 1], F.OVERLOAD)
+
+    def finder(t, gain):
+        s, m = OS.find(t.numpy(), gain)
+        return torch.from_numpy(s), torch.from_numpy(m)
+    got = find_spots(Images(), F.FRAMES, mask=F.static_mask(), verbose=False, finder=finder, device="cpu", **F.KW)
+    want = np.load(HERE / "golden" / "findspots.npz")
+    assert len(got) == want["x"].size > 100
+    for key in KEYS:
+        assert np.array_equal(getattr(got, key), want[key]), key
+
+
+@pytest.mark.gpu
+def test_find_spots_on_device_matches_reference():
+    """The same run with the device classifier (`find_spots`' default): XPG's spots, in XPG's order."""
+    import make_findspots_golden as F
+    from oracle.gather import prepare_frame
+    from xpg_b200.spotfind import find_spots
+    raw = F.raw_frames()
+
+    class Images:
+        nx, ny, first, last = F.NX, F.NY, 1, F.NF
+
+        def get(self, f):
+            return prepare_frame(raw[f - 1], F.OVERLOAD)
+    got = find_spots(Images(), F.FRAMES, mask=F.static_mask(), verbose=False, **F.KW)
+    want = np.load(HERE / "golden" / "findspots.npz")
+    for key in KEYS:
+        assert np.array_equal(getattr(got, key), want[key]), key

@@ -103,8 +103,8 @@ def _dip_below(q, r_list, px, cnet, net, thr, coords):
 
 
 def split_merged(z, y, x, v, b, lab, nx, ny):
-    """Labels after splitting clusters of touching spots at their separated peaks (label * stride + 1 + peak rank
-    in a split cluster, label * stride elsewhere)."""
+    """Labels after splitting clusters of touching spots at their separated peaks: label * stride + 1 + peak rank in
+    a split cluster, label * stride elsewhere (stride 1 when nothing splits, else at least 4096)."""
     n = z.size
     if n == 0:
         return lab
@@ -186,10 +186,11 @@ def split_merged(z, y, x, v, b, lab, nx, ny):
     return lab.astype(np.int64) * max(4096, most + 1) + sub
 
 
-def spot_properties(z, y, x, v, b, lab, min_pix, max_pix, max_centroid_dist):
+def spot_properties(z, y, x, v, b, lab, min_pix, max_pix, max_centroid_dist, parent_last=None):
     """Per spot (in label order): centroid x, y, z (pixel and frame centres), intensity, pixel count, first frame,
-    last frame + 1; spots outside the pixel-count range, without signal or off-centre dropped."""
-    _, lab = np.unique(lab, return_inverse=True)
+    last frame + 1; spots outside the pixel-count range, without signal or off-centre dropped. parent_last: per
+    pixel, the last frame of its unsplit cluster, returned per spot as `parent_last`."""
+    _, first, lab = np.unique(lab, return_index=True, return_inverse=True)
     nc = int(lab.max()) + 1 if lab.size else 0
     w = np.maximum(v - b, 0.0).astype(np.float64)
     npix = np.bincount(lab, minlength=nc)
@@ -206,17 +207,53 @@ def spot_properties(z, y, x, v, b, lab, min_pix, max_pix, max_centroid_dist):
     brightest = srt[np.r_[np.flatnonzero(np.diff(lab[srt])), lab.size - 1]] if lab.size else srt
     off = np.hypot(x[brightest] + PIX0 - cx, y[brightest] + PIX0 - cy)
     ok = (npix >= min_pix) & (npix <= max_pix) & (sw > 0) & (off <= max_centroid_dist)
-    return dict(x=cx[ok], y=cy[ok], z=cz[ok], intensity=sw[ok], npix=npix[ok], zmin=zmin[ok].astype(float),
-                zmax=zmax[ok] + 1.0)
+    out = dict(x=cx[ok], y=cy[ok], z=cz[ok], intensity=sw[ok], npix=npix[ok], zmin=zmin[ok].astype(float),
+               zmax=zmax[ok] + 1.0)
+    if parent_last is not None:
+        out["parent_last"] = np.asarray(parent_last)[first][ok]
+    return out
 
 
-def cluster_spots(z, y, x, v, b, nx, ny, min_pix, max_pix, max_centroid_dist=3.0, cluster_radius=2):
-    """Spots of strong pixels (frame index z, row y, column x, value v, local background b), all at once."""
+def cluster_spots(z, y, x, v, b, nx, ny, min_pix, max_pix, max_centroid_dist=3.0, cluster_radius=2,
+                  with_parents=False):
+    """Spots of strong pixels (frame index z, row y, column x, value v, local background b, in frame-major, row-major
+    order), all at once; with_parents adds each spot's unsplit cluster's last frame (`parent_last`)."""
     z, y, x = (np.asarray(a, np.int32) for a in (z, y, x))
     v, b = np.asarray(v, np.float32), np.asarray(b, np.float32)
     if z.size == 0:
         e = np.zeros(0)
-        return dict(x=e, y=e, z=e, intensity=e, npix=e.astype(int), zmin=e, zmax=e)
-    lab, _ = components(z, y, x, nx, ny, cluster_radius)
+        out = dict(x=e, y=e, z=e, intensity=e, npix=e.astype(int), zmin=e, zmax=e)
+        if with_parents:
+            out["parent_last"] = e.astype(np.int64)
+        return out
+    lab, nc = components(z, y, x, nx, ny, cluster_radius)
+    last = None
+    if with_parents:
+        zc = np.full(nc, -1, np.int64)
+        np.maximum.at(zc, lab, z)
+        last = zc[lab]
     lab = split_merged(z, y, x, v, b, lab, nx, ny)
-    return spot_properties(z, y, x, v, b, lab, min_pix, max_pix, max_centroid_dist)
+    return spot_properties(z, y, x, v, b, lab, min_pix, max_pix, max_centroid_dist, last)
+
+
+def flush_thresholds(batches):
+    """The flushes of XPG's streaming clustering over frame batches (`xpg/spotcluster.py:378-402`): after each batch,
+    clusters ending before its last frame close; at a gap in the frame numbers every open cluster closes; the last
+    flush closes the rest. Returns the thresholds (0-based frames, non-decreasing): a cluster closes at the first
+    flush whose threshold exceeds its last frame."""
+    c, prev = [], None
+    for fr in batches:
+        for f in fr:
+            if prev is not None and f != prev + 1:
+                c.append(prev)
+            prev = f
+        c.append(prev - 1)
+    c.append(np.iinfo(np.int64).max)
+    return np.array(c, np.int64)
+
+
+def streaming_order(spots, batches):
+    """The order XPG's streaming clustering emits the spots of `cluster_spots(..., with_parents=True)` in: by the
+    flush that closes their cluster, then as the one pass orders them (clusters by first pixel, split spots by peak)."""
+    flush = np.searchsorted(flush_thresholds(batches), spots["parent_last"], side="right")
+    return np.argsort(flush, kind="stable")
