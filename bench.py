@@ -255,6 +255,24 @@ def _cpu_baseline(blk, budget_s=20.0, max_rows=400):
                       f"reflections"}
 
 
+def _parity(blk, res, n_min=500):
+    """Post-check of the timed run's results (after the timed region): a stratified sample of the block's rows
+    (every shoebox shape group) integrated again by the CPU restatement from the same raw frames with the block's
+    learnt profiles and adapted widths; worst error per key relative to max(|value|, scale) (tests/tolerance.py),
+    and the rows outside tolerance per key (integers: rows that differ)."""
+    from oracle.blockcheck import check_rows, stratified_rows
+    p, s = blk.plan, blk.spec
+    rows = stratified_rows(p, np.arange(p.n), n_min=n_min)
+
+    def crop(f0, f1, y0, y1, x0, x1):
+        return blk.frames[f0:f1, y0:y1, x0:x1].cpu().numpy().view(np.uint32)
+    t0 = time.perf_counter()
+    worst, bad, info = check_rows(crop, p, rows, res, 0, blk.exp.geom, blk.n_frames, s.ny, s.nx, s.overload,
+                                  blk.model.gain)
+    return dict(info, worst={k: float(f"{v:.3g}") for k, v in worst.items()}, outside_tolerance=bad,
+                seconds=round(time.perf_counter() - t0, 1))
+
+
 def run(args):
     import torch
     rank, world, local = _env()
@@ -295,6 +313,7 @@ def run(args):
     torch.cuda.synchronize()
     D.TIMER.enabled = False
     clk = clocks.stop()
+    res_timed = res
     t = e0.elapsed_time(e1) * 1e-3
     step_ms = [round(a.elapsed_time(b), 1) for a, b in zip([e0] + marks[:-1], marks)]
     ksum = D.TIMER.summary()
@@ -350,6 +369,9 @@ def run(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = _cpu_baseline(blk)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = _parity(blk, res_timed)
     if dist is not None:
         dist.barrier()
     if rank == 0:
@@ -364,7 +386,8 @@ def run(args):
                            "l2": "inputs larger than L2 (frame stack ~{:.0f} GB)".format(blk.frames.numel() * 4 / 1e9),
                            "parallelism": f"replicas x{world} (one block per rank)"},
                 "integrated_per_step": n_ok // max(args.steps, 1),
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "parity": parity}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -590,6 +613,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the post-check of the results against the oracle")
     ap.add_argument("--decode", action="store_true", help="time the bitshuffle-LZ4 frame decode instead")
     ap.add_argument("--spots", action="store_true", help="time the spot-finding classifier instead")
     args = ap.parse_args()

@@ -100,6 +100,10 @@ typedef struct {
     float *fz;                      /* per-frame */
     float *img2, *J, *u1, *u2;      /* per-pixel */
     uint8_t *all_valid2;            /* per-pixel */
+    int64_t *isum_raw;              /* (n) raw summed counts: the recorded counts of the summation voxels (foreground,
+                                       valid, not a neighbour's), an exact integer sum; no counterpart output in XPG,
+                                       whose float32 `vsum` holds gain times the same sum (xpg/integrate_kernels.py:
+                                       318-329) */
 } XiPass1Out;
 
 /* Pass-1 inputs that pass 2 reuses (the `pix` argument, xpg/integrate.py:560-563) plus the background. */
@@ -138,7 +142,7 @@ typedef struct {
 
 /* Last error message of this thread (empty when none). */
 const char *xi_last_error(void);
-/* ABI version: increases when a signature above changes. */
+/* ABI version: increases when a signature or struct above changes (3: XiPass1Out.isum_raw). */
 int xi_version(void);
 /* Synchronises the stream and reports (then clears) the kernels' status word: XI_E_SHAPE when a row was skipped
  * because its shape exceeded its call's max_bx / max_dz. */

@@ -282,6 +282,7 @@ def pass1(sb, r, nb, det, s0, axis, frames_phi0, osc, sd, sm, gain, rcw):
     nfg = F32(fgv.sum())
     sfb = sum32(np.where(fgv, bref[None], 0))
     isum = sum32(np.where(fgv, net, 0))
+    isum_raw = int(np.where(fgv, c, F32(0)).astype(np.int64).sum())    # counts are integers: an exact sum
     tail = ((sfb * sfb) * gain) * np.maximum(b, F32(VAR_FLOOR)) / np.maximum(nbg, F32(1.0))
     vsum = gain * sum32(np.where(fgv, c, 0)) + tail
     vsum0 = gain * sum32(np.where(fgv, np.broadcast_to(bpix, c.shape), 0)) + tail
@@ -315,7 +316,7 @@ def pass1(sb, r, nb, det, s0, axis, frames_phi0, osc, sd, sm, gain, rcw):
     return dict(bg=b, nbg=nbg, isum=isum, vsum=F32(vsum), vsum0=F32(vsum0), xo=F32(xo), yo=F32(yo), zo=F32(zo),
                 m_d=F32(m_d), m_m=F32(m_m), fz=fz, img2=img2, all_valid2=all_valid2, frac_rec=frac_rec,
                 n_over=n_over, n_fg_masked=n_fg_masked, nfg=nfg, zeta=gt["zeta"], J=gt["J"], u1=gt["u1"],
-                u2=gt["u2"], seff=gt["seff"], n_fg_nb=n_fg_nb)
+                u2=gt["u2"], seff=gt["seff"], n_fg_nb=n_fg_nb, isum_raw=isum_raw)
 
 
 # ------------------------------------------------------------------------------------------------------------------

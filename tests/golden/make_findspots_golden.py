@@ -43,7 +43,8 @@ def static_mask():
 
 
 def main():
-    sys.path.insert(0, "/root/reference")
+    from refpath import import_reference
+    import_reference()
     for k, v in (("XPG_DEVICE", "cpu"), ("XPG_COMPILE", "0"), ("XPG_SPOTS_PROCESS", "0"), ("XPG_DECODE_PROCS", "0")):
         os.environ.setdefault(k, v)
     from xpg.io.images import ImageSet

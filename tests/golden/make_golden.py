@@ -34,7 +34,6 @@ from pathlib import Path
 
 import numpy as np
 
-REF = "/root/reference"
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent.parent))
 
@@ -76,13 +75,16 @@ def _cases():
     # config 3's error model on a small sweep: weak reflections and shoeboxes > 40% masked
     c["precision"] = (synth.config1(name="precision", nframes=40, weak_fraction=0.05, dead_fraction=0.02, seed=3),
                       dict())
+    # spots of another crystal given as foreign_spots: masked like non-modelled neighbours (extra neighbour columns)
+    c["foreign"] = (synth.config1(name="foreign", nframes=40, seed=6), dict(foreign=True))
     # spot-width estimation (moments-only integrate calls on sub-ranges)
     c["sigmas"] = (synth.config1(name="sigmas", nframes=60, mean_i0=2000.0, seed=4), dict(estimate=True))
     return c
 
 
 def _ref_modules():
-    sys.path.insert(0, REF)
+    from refpath import import_reference
+    import_reference()
     import xpg.integrate as RI
     import xpg.integrate_kernels as RK
     from xpg.geometry import Geometry as RGeometry
@@ -102,6 +104,13 @@ def _ref_experiment(spec, RGeometry, RCrystal, RExperiment):
                    polarization_normal=g.polarization_normal, sensor_thickness=g.sensor_thickness, mu=g.mu)
     rc = RCrystal(U=spec.orientation(), cell=np.array(spec.cell, float), space_group=spec.space_group)
     return RExperiment(rg, rc)
+
+
+def foreign_spots(spec, n=2400, seed=21):
+    """Spot positions of a foreign crystal (x, y in pixels, z in frames), seeded: uniform over the detector and the
+    sweep, so that many fall within a reflection's neighbour reach and some within 2.5 sigma of its centre."""
+    rng = np.random.default_rng(seed)
+    return (rng.uniform(1.0, spec.nx, n), rng.uniform(1.0, spec.ny, n), rng.uniform(0.0, spec.nframes, n))
 
 
 def _template(spec):
@@ -143,6 +152,8 @@ def run_case(name, spec, kw, out_dir=HERE):
     args = dict(frames=(1, spec.nframes), mask=mask, minimum_zeta=0.05, verbose=False,
                 n_regions_xy=spec.n_regions_xy, exclude_frames=tuple(kw.get("exclude_frames", ())),
                 bkg_template=tmpl)
+    if kw.get("foreign"):
+        args["foreign_spots"] = foreign_spots(spec)
     calls = []
     orig = RK.make_kernels
 

@@ -41,7 +41,8 @@ def split_hkl(text):
 
 
 def main():
-    sys.path.insert(0, "/root/reference")
+    from refpath import import_reference
+    import_reference()
     from xpg.geometry import Geometry as RGeometry
     from xpg.io.legacy import write_integrate_hkl
     from xpg.models import Crystal as RCrystal, Experiment as RExperiment

@@ -47,7 +47,8 @@ def strong_pixels(seed, nf, ny, nx, nspots, bright, crowd, ring):
 
 
 def main():
-    sys.path.insert(0, "/root/reference")
+    from refpath import import_reference
+    import_reference()
     os.environ.setdefault("XPG_DEVICE", "cpu")
     import xpg.spotcluster as RC
     out = {}

@@ -35,7 +35,8 @@ def frames(trial):
 
 
 def main():
-    sys.path.insert(0, "/root/reference")
+    from refpath import import_reference
+    import_reference()
     os.environ.setdefault("XPG_DEVICE", "cpu")
     import torch
     import xpg.spotfind as SF

@@ -11,7 +11,7 @@ import numpy as np
 from xpg_b200 import synth
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = ("config1", "adaptive", "superpix", "binned", "crowded", "precision")
+CASES = ("config1", "adaptive", "superpix", "binned", "crowded", "precision", "foreign")
 
 
 @lru_cache(maxsize=None)
@@ -41,6 +41,16 @@ def static_mask(spec):
     m = np.ones((spec.ny, spec.nx), bool)
     m[spec.ny // 3: spec.ny // 3 + 9, spec.nx // 4: spec.nx // 2] = False
     return m
+
+
+def foreign_of(name):
+    """The foreign-spot list (x, y, z) a case was integrated with, or None (same seeded list as the generator's)."""
+    if not kwargs_of(name).get("foreign"):
+        return None
+    spec = spec_of(name)
+    rng = np.random.default_rng(21)
+    n = 2400
+    return (rng.uniform(1.0, spec.nx, n), rng.uniform(1.0, spec.ny, n), rng.uniform(0.0, spec.nframes, n))
 
 
 def case_inputs(name):

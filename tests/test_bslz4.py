@@ -6,6 +6,7 @@ saturated / overloaded counts, uint32 and uint16."""
 from __future__ import annotations
 
 import ctypes as C
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -191,3 +192,48 @@ def test_imageset_adapter_takes_bitshuffled_chunks():
     im.static_mask = None
     im.bitshuffled_ok = lambda: False
     assert isinstance(FR.as_frame_source(im, device="cpu"), FR.ImageSetFrames)
+
+
+def _xpg_cases():
+    z = np.load(Path(__file__).resolve().parent / "golden" / "bitunshuffle.npz")
+    return [{k: z[f"c{i}_{k}"] for k in ("esize", "n", "block", "staged", "xpg_frame")}
+            for i in range(len([k for k in z.files if k.endswith("_esize")]))], z
+
+
+def _xpg_values(c):
+    """XPG's decoded frame as the uint32 frame path holds it: flagged (-1) as all ones, counts as they are."""
+    f = c["xpg_frame"]
+    return np.where(f == -1.0, np.float64(0xFFFFFFFF), f).astype(np.uint32)
+
+
+def test_oracle_unshuffle_matches_xpg_decoder():
+    """The oracle's unshuffle (and its test encoder, the inverse) against XPG's own decoder's output on the same
+    LZ4-stage bytes (fixture made by tests/golden/make_bitunshuffle_golden.py with the reference's
+    unshuffle_frame_torch and _bitunshuffle)."""
+    cases, z = _xpg_cases()
+    for c in cases:
+        esize, n, belem = int(c["esize"]), int(c["n"]), int(c["block"])
+        v = B.unshuffle(c["staged"], n, esize, belem).view(np.uint16 if esize == 2 else np.uint32)
+        want = _xpg_values(c)
+        got = v.astype(np.uint32)
+        if esize == 2:
+            got[v == 0xFFFF] = 0xFFFFFFFF
+        assert np.array_equal(got, want), (esize, n)
+    np.testing.assert_array_equal(B.bitunshuffle(z["np_in"], 64, 4), z["np_out"])
+    np.testing.assert_array_equal(B.bitshuffle(z["np_out"], 64, 4), z["np_in"])
+
+
+@pytest.mark.gpu
+def test_bitunshuffle_matches_xpg_decoder():
+    """xi_bitunshuffle on the fixture's LZ4-stage bytes gives XPG's decoded frames (flagged pixels all ones)."""
+    import torch
+    lib = native.load()
+    cases, _ = _xpg_cases()
+    for c in cases:
+        esize, n, belem = int(c["esize"]), int(c["n"]), int(c["block"])
+        d_in = torch.from_numpy(np.ascontiguousarray(c["staged"])).cuda()
+        out = torch.zeros(n, dtype=torch.int32, device="cuda")
+        native.check(lib.xi_bitunshuffle(native.ptr(d_in), n, esize, belem, native.ptr(out), native.stream_handle()),
+                     "xi_bitunshuffle")
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), _xpg_values(c)), (esize, n)

@@ -29,7 +29,8 @@ def _run(case, images=None, **over):
         images = FR.U32Frames(G.frames_of(case), first=1, overload=spec.overload)
     model = IntegrationModel(sigma_d=spec.sigma_d, sigma_m=spec.sigma_m, gain=1.0)
     kw = dict(frames=(1, spec.nframes), mask=mask, minimum_zeta=0.05, verbose=False,
-              n_regions_xy=spec.n_regions_xy, exclude_frames=excl, bkg_template=tmpl)
+              n_regions_xy=spec.n_regions_xy, exclude_frames=excl, bkg_template=tmpl,
+              foreign_spots=G.foreign_of(case))
     kw.update(over)
     return integrate(images, [exp] * (len(edges) - 1), edges, model, float(z["dmin"]), **kw)
 

@@ -86,7 +86,8 @@ def case_results(request):
     return request.param, _run_case(request.param)
 
 
-EXACT = ("n_over", "n_fg_masked", "n_fg_nb", "nfg", "bg", "nbg", "zeta", "seff", "all_valid2", "J", "u1", "u2")
+EXACT = ("n_over", "n_fg_masked", "n_fg_nb", "nfg", "isum_raw", "bg", "nbg", "zeta", "seff", "all_valid2", "J", "u1",
+         "u2")
 
 
 def test_pass1_matches_oracle(case_results):

@@ -58,7 +58,7 @@ def test_device_plan_matches_reference(case):
     edges = z["edges"]
     model = IntegrationModel(sigma_d=spec.sigma_d, sigma_m=spec.sigma_m)
     p = plan_integration([spec.experiment()] * (len(edges) - 1), edges, model, float(z["dmin"]), 1e9,
-                         (1, spec.nframes), 0.05, spec.n_regions_xy, True, True)
+                         (1, spec.nframes), 0.05, spec.n_regions_xy, True, True, foreign_spots=G.foreign_of(case))
     out = {k[4:]: v for k, v in z.items() if k.startswith("out_")}
     assert p.n == len(out["x"])
     np.testing.assert_array_equal(p.refl["hkl"], out["hkl"])

@@ -109,3 +109,18 @@ def test_find_spots_on_device_matches_reference():
     want = np.load(HERE / "golden" / "findspots.npz")
     for key in KEYS:
         assert np.array_equal(getattr(got, key), want[key]), key
+
+
+@pytest.mark.parametrize("frames", [[3, 5, 4], [1, 2, 2, 3]])
+def test_find_spots_refuses_frame_lists_that_are_not_increasing(frames):
+    """Clustering all strong pixels at once links frames by number, which equals XPG's streaming clustering (closed at
+    every break in the frame list) only when the frames increase: other lists are refused before any work."""
+    from xpg_b200.spotfind import find_spots
+
+    class Images:
+        nx, ny, first, last = 8, 8, 1, 5
+
+        def get(self, f):
+            raise AssertionError("no frame is read")
+    with pytest.raises(ValueError, match="strictly increasing"):
+        find_spots(Images(), frames, verbose=False, finder=lambda t, g: None, device="cpu")

@@ -4,7 +4,8 @@ It exists for callers that cannot allocate device memory: a program that binds l
 next to a framework that has already taken the GPU's memory into its own pool. It keeps its scratch memory in an
 array inside the library, so these checks compare it with `xi_knn` (the same search on a caller-provided workspace):
 two calls in a row, the second smaller and with fewer columns, so that counters left over from the first call would
-show, and a call above the array's point limit, which must fail cleanly. Neighbour indices and distances are
+show, then a call whose bounds need more grid cells than the array holds (the no-alloc form takes coarser cells
+there), and a call above the array's point limit, which must fail cleanly. Neighbour indices and distances are
 integer / exact results: they must be identical.
 
 The file name keeps it last in collection order; it passes alone in a fresh process as well as after the suite.
@@ -56,7 +57,8 @@ def _without_allocation(lib, q):
 def test_noalloc_knn_matches_workspace_form_on_consecutive_calls():
     lib = N.load()
     cases = [(60_000, 8, (9000.0, 7000.0, 100.0), 11),      # ~5 neighbours in reach: full and partial lists
-             (20_000, 5, (3000.0, 2500.0, 60.0), 12)]       # a smaller second call on the same array
+             (20_000, 5, (3000.0, 2500.0, 60.0), 12),       # a smaller second call on the same array
+             (300_000, 8, (40000.0, 40000.0, 100.0), 14)]  # ~1.4M cells of the search radius: coarser cells here
     for n, k, extent, seed in cases:
         q, keep = _query(n, k, extent, seed)
         j_ref, d_ref = _with_workspace(lib, q)

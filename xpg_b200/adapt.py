@@ -151,101 +151,136 @@ def adapt_block(g, strong, sd_run, sm_run, sd_b, sm_b, rcw_b):
 
 
 def rocking_resolved(r, max_edge=0.5):
-    """Rows whose net counts show a rocking curve inside the box (first and last recorded bins well below the bin
-    of the predicted centre)."""
+    """Rows whose per-frame net counts show a rocking curve inside the box (`xpg/integrate.py:1107-1127`): the mean of
+    the outermost recorded bins (bins beyond the sweep hold exactly 0) is below `max_edge` times the bin holding the
+    predicted centre, with at least three bins between them; boxes under 3 bins always pass."""
     fz = r.get("fz")
+    n_rows = len(r["x"])
     if fz is None:
-        return np.ones(len(r["x"]), bool)
-    n = len(fz)
-    dz = np.minimum(np.asarray(r["dz"], int), fz.shape[1])
-    rows = np.arange(n)
-    c = np.clip(np.floor((r["z"] - r["iz0"]) / np.maximum(r["fb"], 1)).astype(int), 0, np.maximum(dz - 1, 0))
-    centre = fz[rows, c]
-    k = np.arange(fz.shape[1])[None]
-    rec = (fz != 0) & (k < dz[:, None])
-    first = np.where(rec.any(1), np.argmax(rec, 1), 0)
-    last = np.where(rec.any(1), fz.shape[1] - 1 - np.argmax(rec[:, ::-1], 1), 0)
-    edge = 0.5 * (fz[rows, first] + fz[rows, last])
-    return (dz < 3) | ((centre > 0) & (edge < max_edge * centre) & (last - first >= 2))
+        return np.ones(n_rows, bool)
+    depth = fz.shape[1]
+    dz = np.minimum(np.asarray(r["dz"], np.int64), depth)
+    bins = np.arange(depth)
+    recorded = (fz != 0) & (bins[None, :] < dz[:, None])
+    lo = np.where(recorded, bins[None, :], depth).min(axis=1)
+    hi = np.where(recorded, bins[None, :], -1).max(axis=1)
+    none = hi < 0
+    lo[none] = 0
+    hi[none] = 0
+    centre_bin = np.floor((r["z"] - r["iz0"]) / np.maximum(r["fb"], 1)).astype(np.int64)
+    centre_bin = np.minimum(np.maximum(centre_bin, 0), np.maximum(dz - 1, 0))
+    take = lambda k: np.take_along_axis(fz, k[:, None], axis=1)[:, 0]
+    peak = take(centre_bin)
+    rim = 0.5 * (take(lo) + take(hi))
+    return (dz < 3) | ((peak > 0) & (rim < max_edge * peak) & (hi - lo >= 2))
+
+
+def _sample_ranges(f0, f1, osc, n_sample_frames, n_ranges=5):
+    """The frame ranges the spot widths are measured on: n_ranges evenly spaced ranges of at least 5 degrees (and of
+    n_sample_frames / 3 frames), no longer than the sweep's n_ranges-th part."""
+    nf = f1 - f0 + 1
+    span = max(int(round(n_sample_frames / 3)), int(np.ceil(5.0 / max(abs(osc), 1e-6))), 3)
+    span = min(span, max(nf // n_ranges, 3))
+    starts = [f0 + int(k * (nf - span) / max(n_ranges - 1, 1)) for k in range(n_ranges)]
+    return [(a, min(a + span - 1, f1)) for a in starts]
+
+
+class _RangeRows:
+    """Moment-only results of one sampled range: the rows usable for the width estimate (`base`), their I/sigma,
+    and the per-row corrections of the second moments (pixel footprint, frame-bin width)."""
+
+    def __init__(self, r, a, b, g):
+        self.r = r
+        ok = (r["z"] >= a - 1) & (r["z"] < b) & (r.get("lattice", 0) == 0) & ~r["overlap"]
+        ok &= np.isfinite(r["isum"]) & (r["isum"] > 0) & (r["n_over"] == 0) & (r["frac_rec"] > 0.98)
+        self.base = ok & rocking_resolved(r)
+        self.isig = r["isum"] / np.sqrt(np.maximum(r["vsum"], 1e-6))
+        self.g = g
+
+    def count_above(self, t):
+        return int((self.base & (self.isig > t)).sum())
+
+    def pick(self, t):
+        return self.base & (self.isig > t)
+
+    def moments(self, sel):
+        """(m_d, footprint) pairs, frame-width-corrected m_m, and the per-frame fit rows of the selected rows."""
+        r, g = self.r, self.g
+        lab = g.pixel_to_lab(r["x"][sel], r["y"][sel])
+        dist = np.linalg.norm(lab, axis=1)
+        cos_in = np.abs(lab @ g.ed3) / dist
+        foot = (g.qx / dist) ** 2 * (1 + cos_in ** 2) / 24.0      # pixel footprint per axis (eps units)
+        if "pxs" in r:
+            foot = foot * r["pxs"][sel] ** 2
+        fb = r["fb"][sel] if "fb" in r else 1
+        mm = r["m_m"][sel] - (np.radians(g.osc) * fb * r["zeta_k"][sel]) ** 2 / 12.0
+        per_frame = sel & (r["fb"] == 1) if "fb" in r else sel
+        fit = (r["fz"][per_frame], r["iz0"][per_frame], r["phi"][per_frame], r["zeta_k"][per_frame])
+        return np.c_[r["m_d"][sel], foot], mm, fit
+
+
+def _thresholds(ranges):
+    """Per-range I/sigma threshold of the strong rows, or None for a range left out: 20, or 10 where fewer than
+    150 rows pass 20; a range with fewer than 20 rows at its threshold is left out. When every range is left out
+    and the ranges together hold at least 30 rows above 5, every range takes 5."""
+    counts = np.array([[rr.count_above(t) for t in (20.0, 10.0, 5.0)] for rr in ranges]).reshape(-1, 3)
+    thr = np.where(counts[:, 0] >= 150, 20.0, 10.0)
+    kept = np.where(counts[:, 0] >= 150, counts[:, 0], counts[:, 1]) >= 20
+    if not kept.any() and counts[:, 2].sum() >= 30:
+        return [5.0] * len(ranges)
+    return [float(t) if k else None for t, k in zip(thr, kept)]
+
+
+def _growing(new, cur, prev):
+    """The width estimate grows with the box (both the last step and this one by more than 15%): contamination."""
+    up = lambda a, b: a.sigma_d > 1.15 * b.sigma_d or a.sigma_m > 1.15 * b.sigma_m
+    return up(new, cur) and up(cur, prev)
 
 
 def estimate_sigmas(integrate_fn, images, exp, model0, dmin, frames, n_sample_frames=30, verbose=True, log=print,
                     extra_exps=(), bkg_template=None, foreign_spots=None, max_iter=None, guard=None):
-    """sigma_D / sigma_M from second moments and rocking curves of strong spots over 5 sampled frame ranges,
-    iterated up to 3 times (`xpg/integrate.py:1002-1092`). `integrate_fn` is the moments-only integration."""
+    """sigma_D / sigma_M of a sweep from the truncation-corrected second moments and rocking curves of strong spots
+    over sampled frame ranges (`xpg/integrate.py:1002-1092`), up to 3 rounds, each round integrating the ranges with
+    the previous round's widths. `integrate_fn` is the moments-only integration."""
     from .plan import IntegrationModel
     g = exp.geom
     f0, f1 = frames
-    nf = f1 - f0 + 1
-    nr = 5
-    span = max(int(round(n_sample_frames / 3)), int(np.ceil(5.0 / max(abs(g.osc), 1e-6))), 3)
-    span = min(span, max(nf // nr, 3))
-    ranges = []
-    for i in range(nr):
-        a = f0 + int(i * (nf - span) / max(nr - 1, 1))
-        ranges.append((a, min(a + span - 1, f1)))
-    model = prev = model0
+    ranges = _sample_ranges(f0, f1, g.osc, n_sample_frames)
+    lattices = [[e] for e in extra_exps] or None
+    cur = prev = model0
     history = []
-    for it in range(max_iter or 3):
-        sel_md, sel_mm, sel_fit, per_range = [], [], [], []
+    for rnd in range(max_iter or 3):
+        stats = []
         for a, b in ranges:
-            edges = np.array([a - 1.0, float(b)])
-            res = integrate_fn(images, [exp], edges, model, dmin, frames=(max(f0, a - 5), min(f1, b + 5)),
-                               verbose=False, learn_profiles=False, adaptive=False, bkg_template=bkg_template,
-                               extra_lattices=[[e] for e in extra_exps] or None, foreign_spots=foreign_spots,
-                               moments_only=True)
-            r = res.refl
-            z_ok = (r["z"] >= a - 1) & (r["z"] < b) & (r.get("lattice", 0) == 0) & ~r["overlap"]
-            isg = r["isum"] / np.sqrt(np.maximum(r["vsum"], 1e-6))
-            base = z_ok & np.isfinite(r["isum"]) & (r["isum"] > 0) & (r["n_over"] == 0) & (r["frac_rec"] > 0.98)
-            base &= rocking_resolved(r)
-            per_range.append((r, base, isg))
-        sels = []
-        for r, base, isg in per_range:
-            strong = base & (isg > 20)
-            if strong.sum() < 150:
-                strong = base & (isg > 10)
-            sels.append(strong if strong.sum() >= 20 else None)
-        if all(x is None for x in sels) and sum(int((bs & (ig > 5.0)).sum()) for _, bs, ig in per_range) >= 30:
-            sels = [bs & (ig > 5.0) for _, bs, ig in per_range]
-        for (r, base, isg), strong in zip(per_range, sels):
-            if strong is None or not strong.any():
-                continue
-            Xv = g.pixel_to_lab(r["x"][strong], r["y"][strong])
-            Xlen = np.linalg.norm(Xv, axis=1)
-            cosa = np.abs(Xv @ g.ed3) / Xlen
-            pix = (g.qx / Xlen) ** 2 * (1 + cosa ** 2) / 24.0
-            if "pxs" in r:
-                pix = pix * r["pxs"][strong] ** 2
-            sel_md.append(np.c_[r["m_d"][strong], pix])
-            fbs = r["fb"][strong] if "fb" in r else 1
-            sel_mm.append(r["m_m"][strong] - (np.radians(g.osc) * fbs * r["zeta_k"][strong]) ** 2 / 12.0)
-            one = strong & (r["fb"] == 1) if "fb" in r else strong
-            sel_fit.append((r["fz"][one], r["iz0"][one], r["phi"][one], r["zeta_k"][one]))
-        if not sel_md:
+            res = integrate_fn(images, [exp], np.array([a - 1.0, float(b)]), cur, dmin,
+                               frames=(max(f0, a - 5), min(f1, b + 5)), verbose=False, learn_profiles=False,
+                               adaptive=False, bkg_template=bkg_template, extra_lattices=lattices,
+                               foreign_spots=foreign_spots, moments_only=True)
+            stats.append(_RangeRows(res.refl, a, b, g))
+        picked = [rr.moments(rr.pick(t)) for rr, t in zip(stats, _thresholds(stats))
+                  if t is not None and rr.pick(t).any()]
+        if not picked:
             break
-        md2 = np.concatenate(sel_md)
-        mm = np.concatenate(sel_mm)
-        md = md2[:, 0] / _truncation_factor() - md2[:, 1]
-        sd_new = np.degrees(np.sqrt(max(np.median(md), 1e-12)))
-        sm_new = fit_rocking_width(sel_fit, g, max(np.degrees(np.sqrt(max(np.median(mm), 1e-12))),
-                                                  0.5 * model.sigma_m))
-        new = IntegrationModel(sigma_d=float(np.clip(sd_new, 0.005, 1.0)), sigma_m=float(np.clip(sm_new, 0.005, 5.0)),
-                               gain=model.gain)
+        md_pairs = np.concatenate([p[0] for p in picked])
+        mm = np.concatenate([p[1] for p in picked])
+        md = md_pairs[:, 0] / _truncation_factor() - md_pairs[:, 1]
+        sd_deg = np.degrees(np.sqrt(max(np.median(md), 1e-12)))
+        mm_deg = np.degrees(np.sqrt(max(np.median(mm), 1e-12)))
+        sm_deg = fit_rocking_width([p[2] for p in picked], g, max(mm_deg, 0.5 * cur.sigma_m))
+        new = IntegrationModel(sigma_d=float(np.clip(sd_deg, 0.005, 1.0)), sigma_m=float(np.clip(sm_deg, 0.005, 5.0)),
+                               gain=cur.gain)
         history.append((float(new.sigma_d), float(new.sigma_m), int(md.size)))
         if verbose:
             log(f"  INTEGRATE: estimated sigma_D {new.sigma_d:.4f} deg, sigma_M {new.sigma_m:.4f} deg "
-                f"from {md.size} strong spots (iteration {it + 1})")
-        if (guard is None or guard) and it >= 1 and (new.sigma_d > 1.15 * model.sigma_d
-                                                      or new.sigma_m > 1.15 * model.sigma_m) and \
-                (model.sigma_d > 1.15 * prev.sigma_d or model.sigma_m > 1.15 * prev.sigma_m):
+                f"from {md.size} strong spots (iteration {rnd + 1})")
+        if (guard is None or guard) and rnd >= 1 and _growing(new, cur, prev):
             if verbose:
                 log(f"  INTEGRATE: spot-width estimate keeps growing with the box (contamination): keeping "
-                    f"iteration {it} values")
+                    f"iteration {rnd} values")
             break
-        prev, model = model, new
-        if max_iter and it >= 2 and abs(model.sigma_d / prev.sigma_d - 1) < 0.03 and \
-                abs(model.sigma_m / prev.sigma_m - 1) < 0.03:
+        prev, cur = cur, new
+        settled = abs(cur.sigma_d / prev.sigma_d - 1) < 0.03 and abs(cur.sigma_m / prev.sigma_m - 1) < 0.03
+        if max_iter and rnd >= 2 and settled:
             break
-    model.history = history
-    return model
+    cur.history = history
+    return cur

@@ -659,9 +659,9 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         O.img2[po + p] = O.img2[po + p] - (float)(m & 0x7f) * (b * brefs[p]);
         O.all_valid2[po + p] = m >> 7;
     }
-    double acc[15];
+    double acc[16];
 #pragma unroll
-    for (int q = 0; q < 15; ++q) acc[q] = 0.0;
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
     for (int z = threadIdx.x; z < Dz; z += NT)
         for (int w = 0; w < NT / 32; ++w) fzw[w][z] = 0.0f;
     __syncthreads();
@@ -693,6 +693,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         }
         const float bpix = b * bref;
         float c_n = 0.f, c_net = 0.f, c_c = 0.f, c_w = 0.f, c_wz = 0.f, c_e3 = 0.f, c_e33 = 0.f;
+        int c_raw = 0;                                       // exact: <= 65 counts below 2^23 each
 #pragma unroll
         for (int w = 0; w < 3; ++w) {
             if (32 * w >= Dz) break;
@@ -721,6 +722,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
                             c_n += 1.0f;
                             c_net += net;
                             c_c += c;
+                            c_raw += (int)c;
                             const float wpos = fmaxf(net, 0.0f);
                             c_w += wpos;
                             c_wz += wpos * fzz[z];
@@ -754,9 +756,10 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
             acc[11] += (double)c_net * (double)e12;
             acc[12] += (double)c_e3;
             acc[13] += (double)c_e33;
+            acc[15] += (double)c_raw;                         // integer partial sums below 2^53: exact
         }
     }
-    block_sum<NT, 15>(acc, red, tot);
+    block_sum<NT, 16>(acc, red, tot);
     for (int z = threadIdx.x; z < Dz; z += NT) {
         float s = 0.0f;
         for (int w = 0; w < NT / 32; ++w) s += fzw[w][z];
@@ -797,6 +800,7 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         O.n_over[row] = n_over;
         O.n_fg_masked[row] = n_fg_masked;
         O.n_fg_nb[row] = n_fg_nb;
+        if (O.isum_raw) O.isum_raw[row] = (int64_t)tot[15];
     }
 }
 
@@ -1509,7 +1513,7 @@ extern "C" {
 
 const char* xi_last_error(void) { return g_err; }
 
-int xi_version(void) { return 2; }
+int xi_version(void) { return 3; }
 
 int xi_tune(int key, long long value) {
     if (key == XI_TUNE_PASS1_STAGE_BYTES || key == XI_TUNE_PASS2_STAGE_BYTES) {

@@ -793,9 +793,10 @@ int xi_knn_noalloc(const XiKnn* q, int32_t* nbj, double* nbd, void* stream) {
     if (w.bytes > kNoAllocBytes) return xi_fail(XI_E_LIMIT, "xi_knn_noalloc: scratch layout beyond the array");
     cudaStream_t s = (cudaStream_t)stream;
     const unsigned nb = (unsigned)((q->n + 255) / 256);
-    // the array keeps the previous call's contents: the cell counters and fill cursors start from zero
-    cudaMemsetAsync(w.count, 0, sizeof(int) * g.n_cells, s);
-    cudaMemsetAsync(w.fill, 0, sizeof(int) * g.n_cells, s);
+    // the array keeps the previous call's contents: the cell counters and fill cursors start from zero (zeroed by a
+    // kernel, as in xi_knn: a memset could queue behind host-to-device transfers in the copy engine)
+    const int64_t zb = (g.n_cells + 255) / 256;
+    k_zero2<<<(unsigned)(zb < 4096 ? zb : 4096), 256, 0, s>>>(w.count, w.fill, g.n_cells);
     k_knn_bin<<<nb, 256, 0, s>>>(*q, g, w.count, w.cell_of);
     size_t cb = w.cub_bytes;
     if (cub::DeviceScan::ExclusiveSum(w.cub, cb, w.count, w.start, (int)g.n_cells, s) != cudaSuccess)

@@ -300,7 +300,7 @@ class Pass1Buffers:
 
     SCALARS = ("bg", "nbg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m", "frac_rec", "nfg", "zeta",
                "seff")
-    COUNTS = ("n_over", "n_fg_masked", "n_fg_nb")
+    COUNTS = ("n_over", "n_fg_masked", "n_fg_nb", "isum_raw")
 
     def __init__(self, rows: RowSet):
         d = rows.device

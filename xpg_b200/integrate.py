@@ -172,13 +172,14 @@ def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, b
     out = {k: np.empty(n, np.float64) for k in OUT_F64}           # every processed block fills its rows
     out["n_over"] = np.zeros(n, np.int32)
     out["n_fg_masked"] = np.zeros(n, np.int32)
+    out["isum_raw"] = np.full(n, -1, np.int64)                    # -1: not integrated (rows of no processed block)
     keep_fz = not learn_profiles
     fz_out = np.zeros((n, MAX_DZ), np.float32) if keep_fz else None
     nreg = plan.nreg
     sd = np.radians(model.sigma_d)
     sm = np.radians(model.sigma_m)
     state = dict(sd=sd, sm=sm, rcw=A.rc_default_weights())
-    block_params, prof_by_block = {}, {}
+    block_params, prof_by_block, block_widths = {}, {}, {}
     t_dev = 0.0
     nblocks = len(exp_blocks)
     blocks_rows = plan.blocks_refl                     # plan order (a launch groups its rows by shape itself)
@@ -245,6 +246,7 @@ def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, b
         if rem.size:
             pass1_rows(b, blk, rem)
         sd_b, sm_b, rcw_b = blk.c1[:3]
+        widths_p1 = (float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy())
         p1 = blk.p1
         num = torch.zeros((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float64, device=device)
         den = torch.zeros_like(num)
@@ -265,6 +267,8 @@ def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, b
             block_params[b] = params
         prof = torch.empty((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
         D.finalize_profiles(num, den, prof)
+        block_widths[b] = dict(pass1=widths_p1,
+                               pass2=(float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy()))
         cols = {k: p1.t[k] for k in P1_OUT}
         if not moments_only:
             c2, k2 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
@@ -363,11 +367,13 @@ def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, b
         log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - t0:.1f}s (device {t_dev:.1f}s)")
     res = IntegrationResult(refl, model, prof_by_block, dict(total=time.time() - t0, gpu=t_dev))
     res.block_params = block_params
+    res.block_widths = block_widths      # (sigma_D, sigma_M in radians, rocking-curve weights) of each block's passes
     return res
 
 
 ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")
-P1_OUT = ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m", "n_over", "n_fg_masked")
+P1_OUT = ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m", "n_over", "n_fg_masked",
+          "isum_raw")
 P2_OUT = ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "rho", "p_fg")
 
 

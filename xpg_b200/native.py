@@ -43,7 +43,7 @@ class XiBlock(C.Structure):
 class XiPass1Out(C.Structure):
     _fields_ = [(k, _fp) for k in ("bg", "nbg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "m_d", "m_m",
                                    "frac_rec", "nfg", "zeta", "seff", "n_over", "n_fg_masked", "n_fg_nb", "fz",
-                                   "img2", "J", "u1", "u2", "all_valid2")]
+                                   "img2", "J", "u1", "u2", "all_valid2", "isum_raw")]
 
 
 class XiPass2In(C.Structure):

@@ -79,7 +79,11 @@ def find_spots(images, frames, gain=1.0, mask=None, strong_pixel=3.0, background
     host all at once, the spots in the order XPG's streaming clustering emits them for these batches."""
     from .spotcluster import cluster_spots, streaming_order
     import time
-    frames = list(frames)
+    frames = [int(f) for f in frames]
+    if any(b <= a for a, b in zip(frames, frames[1:])):
+        # XPG's streaming accumulator closes its clusters at every break in the frame list; clustering all strong
+        # pixels at once links frames by their numbers, which matches it only for increasing frame lists
+        raise ValueError("find_spots: frame numbers must be strictly increasing")
     t0 = time.time()
     finder = finder or make_finder(nbx, nby, strong_pixel, background_pixel, extended=extended)
     nx, ny = int(images.nx), int(images.ny)
