@@ -1,24 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the B200 shoebox integration (drop-in for XPG's INTEGRATE stage).
 
-Workload (default `config2-block`): one 360-frame phi block of the 16M-pixel sweep (4148 x 4362 px of 75 um at
-120 mm, lambda 0.98 A, 0.1 deg frames, P 21 21 21 60/85/120 A, sigma_M 0.15 deg, sigma_D 0.03 deg, background 0.2,
-5 x 5 profile regions). A step is one full `integrate()` call of the drop-in API on that block: predictions and shoebox
-plan, frame gather, pass 1, profile learning, adaptive widths, pass 2, results back on the host. The block's frames
-(every frame its boxes reach) are synthetic, seeded and rendered on the device before timing (`data`); the frame
-stack (~34 GB) is far larger than L2, so no flush is needed between steps.
+Workload (default `config2-sweep`): the whole 16M-pixel sweep, 3600 frames of 4148 x 4362 px (75 um at 120 mm,
+lambda 0.98 A, 0.1 deg frames, P 21 21 21 60/85/120 A, sigma_M 0.15 deg, sigma_D 0.03 deg, background 0.2, 5 x 5
+profile regions), integrated in 10 phi blocks of 360 frames with the adapted widths carried from block to block. A
+step is one full `integrate()` call of the drop-in API on the sweep: predictions and shoebox plan, frames streamed in
+32-frame wedges, gather, pass 1, profile learning, adaptive widths, pass 2 of every block, results back on the host.
+The frames are synthetic and seeded, rendered on the device before timing and kept in HBM in the library's packed
+transfer encoding (one byte a pixel plus exception pairs, 65 GB for the 260 GB of uint32 frames), widened wedge by
+wedge inside the timed region. Other workloads: `config2-block` (one 360-frame block, raw frames resident),
+`config2-small` (20 frames, for profiling captures), `config1` (config 1's 100-frame sweep). Inputs are far larger
+than L2, so no flush is needed between steps.
 
   value  reflections integrated per second with the frames resident in HBM (device-timed, CUDA events, max over
-         ranks), whole job over all ranks;
-  e2e    the same with the frames in pinned host memory, uploaded inside every step (the transfer thread sends
-         each 2-frame chunk raw or packed to one byte a pixel on the host's cores, whichever keeps the link busy;
-         h2d_bytes_per_step counts the bytes that crossed);
+         ranks), whole job over all ranks; pixel_gbs = the path's algorithmic bytes (every uint32 frame pixel once,
+         every voxel a second time, 32 outputs per reflection) per second, pixel_hbm_frac against the measured peak;
+  e2e    the same through the same API with the frames in pinned host memory (the sweep: its packed store; a block:
+         raw uint32, packed by the transfer thread where that keeps the link busy), uploaded inside every step;
   roofline  of the dominant kernel (largest share of device time): algorithmic bytes per launch / live CUDA-event
          launch duration, against the measured HBM copy bandwidth;
-  cpu_baseline  the oracle (numpy restatement of the reference's CPU path) on a bounded sample of the same block.
+  parity  after the timed region: stratified samples of rows of the first and the middle block integrated again by
+         the CPU restatement from the same frames, the worst error per result key;
+  cpu_baseline  the restatement of the reference's CPU path on a bounded random sample of the same workload.
 
-With --gpus N (torchrun, one rank per GPU) every rank integrates a block of its own sweep (replicas: sweeps are
-independent; weak scaling). `--impl reference` times the CPU restatement of the reference on all host cores.
+With --gpus N (torchrun, one rank per GPU) every rank integrates a sweep of its own (replicas: sweeps are
+independent; weak scaling). `--impl reference` times the CPU restatement of the reference on all host cores, on the
+same workload and config, without CUDA.
 """
 from __future__ import annotations
 
@@ -36,8 +43,13 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# large shoebox arenas are freed and allocated block after block: segments that grow avoid fragmenting HBM
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
-METRIC = "integrated reflections/s (one 360-frame phi block of the 16M-pixel sweep per step)"
+METRICS = {"config2-sweep": "integrated reflections/s (the 16M-pixel, 3600-frame sweep per step)",
+           "config2-block": "integrated reflections/s (one 360-frame phi block of the 16M-pixel sweep per step)",
+           "config2-small": "integrated reflections/s (a 20-frame phi block of the 16M-pixel sweep per step)",
+           "config1": "integrated reflections/s (the 1M-pixel, 100-frame sweep of config 1 per step)"}
 UNIT = "refl/s"
 
 
@@ -131,64 +143,146 @@ def replica_seed(workload, rank):
     return (2 if workload.startswith("config2") else 1) + rank
 
 
-class Block:
-    """One phi block of a synthetic sweep, planned and rendered on the device."""
+WEDGE_FRAMES = 32
+
+
+def workload_geometry(name, seed_offset=0):
+    """(spec, block edges, frames integrated) of a workload: the whole 3600-frame sweep (10 phi blocks of 360 frames),
+    one 360-frame block of it with every frame its boxes reach, a 20-frame block (profiling captures), or config 1's
+    100-frame sweep."""
+    from xpg_b200 import synth
+    seed = replica_seed(name, seed_offset)
+    if name == "config2-sweep":
+        s = synth.config2(seed=seed)
+        return s, s.block_edges(), s.nframes
+    if name in ("config2-block", "config2-small"):
+        s = synth.config2(seed=seed)
+        return s, np.array([0.0, 360.0 if name == "config2-block" else 20.0]), None
+    if name == "config1":
+        s = synth.config1(seed=seed)
+        return s, np.array([0.0, 100.0]), s.nframes
+    raise ValueError(name)
+
+
+def plan_workload(name, seed_offset, plan_integration):
+    """The workload's spec, edges, frame count and shoebox plan (the device planner for the GPU arm, the CPU
+    restatement for the reference arm: the same integers)."""
+    from xpg_b200.plan import IntegrationModel
+    s, edges, n_frames = workload_geometry(name, seed_offset)
+    exp = s.experiment()
+    model = IntegrationModel(sigma_d=s.sigma_d, sigma_m=s.sigma_m)
+    args = (edges, model, s.resolution_limit(), 1e9)
+    nb = len(edges) - 1
+    if n_frames is None:                      # a block: every frame its boxes reach
+        probe = plan_integration([exp] * nb, *args, (1, s.nframes), 0.05, s.n_regions_xy, True, True)
+        n_frames = int(min(max(probe.need_hi) + 1, s.nframes))
+    plan = plan_integration([exp] * nb, *args, (1, n_frames), 0.05, s.n_regions_xy, True, True)
+    return s, exp, model, edges, n_frames, plan
+
+
+def workload_config(name, spec, edges, n_frames, plan, world):
+    """The `config` object of the bench line (the same for both arms)."""
+    P = spec.nx * spec.ny
+    return {"workload": name, "reflections_per_step": int(plan.n), "frames_per_step": int(n_frames),
+            "phi_blocks": len(edges) - 1, "detector": [spec.nx, spec.ny],
+            "voxels_per_step": int((plan.Dz * plan.bx.astype(np.int64) ** 2).sum()),
+            "l2": f"inputs larger than L2 (frame stack {4 * P * n_frames / 1e9:.3g} GB of uint32)",
+            "parallelism": f"replicas x{world} (one sweep per rank)"}
+
+
+def alg_bytes(spec, n_frames, plan):
+    """Algorithmic bytes of a step of the path: every uint32 frame pixel read once, every shoebox voxel read a second
+    time by pass 2, 32 float64 outputs per reflection."""
+    V = float((plan.Dz * plan.bx.astype(np.float64) ** 2).sum())
+    return 4.0 * spec.nx * spec.ny * n_frames + 4.0 * V + 8.0 * 32 * plan.n
+
+
+def bytes_per_kernel(plan, n_frames):
+    """Algorithmic bytes of every kernel over one step: each shoebox voxel read once (4 B), the per-pixel and
+    per-frame tables written or read once, the row's scalars; the gather reads every raw pixel its boxes cover and
+    writes the box once; decode_bins reads and writes the binned rows; the unpack reads a packed byte and writes a
+    uint32 per frame pixel."""
+    p = plan
+    V = (p.Dz * p.bx * p.bx).astype(np.float64)
+    P = (p.bx * p.bx).astype(np.float64)
+    raw = (np.minimum(p.Dz * p.fb, np.maximum(n_frames - p.iz0, 0)) * (p.bx * p.pxs) ** 2).astype(np.float64)
+    return {"pass1": float((4 * V + 17 * P + 4 * p.Dz + 92).sum()),
+            "pass2": float((4 * V + 12 * P + 52).sum()),
+            "gather": float((4 * raw + 4 * V).sum()),
+            "decode_bins": float((8 * V * (p.fb > 1)).sum())}
+
+
+class Workload:
+    """A workload on the device: its plan, its frames (resident in HBM: raw uint32 for a block, the whole sweep in
+    the packed transfer encoding), and the same frames in pinned host memory for the end-to-end run."""
 
     def __init__(self, name, seed_offset=0, device="cuda"):
+        import torch
         from xpg_b200 import synth
-        from xpg_b200.plan import IntegrationModel, plan_integration
-        seed = replica_seed(name, seed_offset)
-        if name == "config2-block":
-            self.spec = synth.config2(seed=seed)
-            self.edges = np.array([0.0, 360.0])
-        elif name == "config2-small":          # a 20-frame block of the same sweep (profiling captures)
-            self.spec = synth.config2(seed=seed)
-            self.edges = np.array([0.0, 20.0])
-        elif name == "config1":
-            self.spec = synth.config1(seed=seed)
-            self.edges = np.array([0.0, 100.0])
-        else:
-            raise ValueError(name)
+        from xpg_b200.plan import plan_integration
+        self.name, self.device = name, device
+        (self.spec, self.exp, self.model, self.edges, self.n_frames,
+         self.plan) = plan_workload(name, seed_offset, plan_integration)
         s = self.spec
-        self.exp = s.experiment()
-        self.dmin = s.resolution_limit()
-        self.model = IntegrationModel(sigma_d=s.sigma_d, sigma_m=s.sigma_m)
-        # frames the block's boxes reach
-        probe = plan_integration([self.exp], self.edges, self.model, self.dmin, 1e9, (1, s.nframes), 0.05,
-                                 s.n_regions_xy, True, True)
-        self.n_frames = int(min(max(probe.need_hi) + 1, s.nframes))
-        self.plan = plan_integration([self.exp], self.edges, self.model, self.dmin, 1e9, (1, self.n_frames), 0.05,
-                                     s.n_regions_xy, True, True)
-        self.n_refl = self.plan.n
         _, self.table = synth.reflection_table(s, z_range=(-5.0, self.n_frames + 5.0))
-        self.frames = synth.device_frames(s, self.table, 1, self.n_frames, device=device)
-        self.device = device
+        self.frames = self.store = self.dev_store = None
+        if name == "config2-sweep":
+            from xpg_b200 import frames as FR
+
+            def render(k, n, out):
+                synth.device_frames(s, self.table, k + 1, n, out=out, device=device)
+            self.store = FR.pack_generated(render, self.n_frames, s.ny, s.nx, wedge=WEDGE_FRAMES, device=device)
+            self.dev_store = self.store.to(device)
+            self._tmp = torch.empty((s.ny, s.nx), dtype=torch.int32, device=device)
+        else:
+            self.frames = synth.device_frames(s, self.table, 1, self.n_frames, device=device)
+        self.n_refl = self.plan.n
 
     def integrate(self, frames):
         from xpg_b200.integrate import integrate
-        return integrate(frames, [self.exp], self.edges, self.model, self.dmin, frames=(1, self.n_frames),
-                         verbose=False, n_regions_xy=self.spec.n_regions_xy)
+        nb = len(self.edges) - 1
+        return integrate(frames, [self.exp] * nb, self.edges, self.model, self.spec.resolution_limit(),
+                         frames=(1, self.n_frames), verbose=False, n_regions_xy=self.spec.n_regions_xy,
+                         wedge_frames=WEDGE_FRAMES)
 
-    def source(self, host=None):
-        from xpg_b200.frames import U32Frames
-        return U32Frames(self.frames if host is None else host, first=1, overload=self.spec.overload,
-                         device=self.device)
+    def source(self):
+        """Frames resident in HBM."""
+        from xpg_b200.frames import PackedFrames, U32Frames
+        if self.dev_store is not None:
+            return PackedFrames(self.dev_store, first=1, overload=self.spec.overload, device=self.device)
+        return U32Frames(self.frames, first=1, overload=self.spec.overload, device=self.device)
 
-    def bytes_per_kernel(self):
-        """Algorithmic bytes of every kernel over one step: each shoebox voxel read once (4 B), the per-pixel and
-        per-frame tables written or read once, the row's scalars; the gather reads every raw pixel its boxes cover
-        and writes the box once; decode_bins reads and writes the binned rows."""
-        p = self.plan
-        V = (p.Dz * p.bx * p.bx).astype(np.float64)
-        P = (p.bx * p.bx).astype(np.float64)
-        raw = (np.minimum(p.Dz * p.fb, np.maximum(self.n_frames - p.iz0, 0)) * (p.bx * p.pxs) ** 2).astype(np.float64)
-        return {"pass1": float((4 * V + 17 * P + 4 * p.Dz + 92).sum()),
-                "pass2": float((4 * V + 12 * P + 52).sum()),
-                "gather": float((4 * raw + 4 * V).sum()),
-                "decode_bins": float((8 * V * (p.fb > 1)).sum())}
+    def host_source(self):
+        """The same frames in pinned host memory (the sweep: its packed store; a block: raw uint32)."""
+        import torch
+        from xpg_b200.frames import PackedFrames, U32Frames
+        if self.store is not None:
+            return PackedFrames(self.store, first=1, overload=self.spec.overload, device=self.device, depth=12)
+        host = torch.empty(self.frames.shape, dtype=torch.int32, pin_memory=True)
+        host.copy_(self.frames)
+        return U32Frames(host, first=1, overload=self.spec.overload, device=self.device)
 
+    def drop_resident(self):
+        """Frees the HBM copy of the sweep's packed frames (the end-to-end run reads the host copy)."""
+        import torch
+        if self.dev_store is not None:
+            self.dev_store = None
+            torch.cuda.empty_cache()
 
-SAMPLE = dict(a=100, wz=24, crop=1024)     # frame window and detector crop of the CPU sample
+    def crop(self, f0, f1, y0, y1, x0, x1):
+        """uint32 window [y0, y1) x [x0, x1) of frames f0..f1-1 (0-based) on the host."""
+        import torch
+        if self.frames is not None:
+            return self.frames[f0:f1, y0:y1, x0:x1].cpu().numpy().view(np.uint32)
+        out = np.empty((f1 - f0, y1 - y0, x1 - x0), np.uint32)
+        for k in range(f0, f1):
+            self.dev_store.unpack(k, self._tmp, torch.cuda.current_stream())
+            out[k - f0] = self._tmp[y0:y1, x0:x1].cpu().numpy().view(np.uint32)
+        return out
+
+    def frame_bytes_on_host(self):
+        return self.store.nbytes if self.store is not None else 4 * self.spec.nx * self.spec.ny * self.n_frames
+
 
 # DRAM bytes (read + write) per shoebox voxel of the pass kernels, from one ncu capture of a launch of the same
 # kernels on the config-2 geometry (a 20-frame block, `--workload config2-small`: the 2,597-reflection launch of
@@ -196,14 +290,31 @@ SAMPLE = dict(a=100, wz=24, crop=1024)     # frame window and detector crop of t
 DRAM_BYTES_PER_VOXEL = {"pass1": 4.554, "pass2": 4.439}
 
 
-def _sample_rows(p, nx, ny):
-    """Rows of the CPU sample: boxes inside frames [a, a + wz) and inside a crop x crop detector patch."""
-    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
-    x0, y0 = nx // 2 + 300, ny // 2 + 300
-    x0, y0 = min(x0, nx - c), min(y0, ny - c)
-    inside = (p.iz0 >= a) & (p.iz0 + p.Dz * p.fb <= a + wz) & (p.pxs == 1) & \
-        (p.ix0 >= x0) & (p.ix0 + p.bx <= x0 + c) & (p.iy0 >= y0) & (p.iy0 + p.bx <= y0 + c)
-    return np.flatnonzero(inside), (y0, x0)
+def _parity(wl, res, n_min=500):
+    """Post-check of a timed run's results (after the timed region): stratified samples of rows (every shoebox shape
+    group) of the first block and, for a sweep, of its middle block (widths carried over from the blocks before),
+    integrated again by the CPU restatement from the same raw frames with each block's learnt profiles and adapted
+    widths; worst error per key relative to max(|value|, scale) (tests/tolerance.py), and the rows outside tolerance
+    per key (integers: rows that differ)."""
+    from oracle.blockcheck import check_rows, stratified_rows
+    p, s = wl.plan, wl.spec
+    nb = len(wl.edges) - 1
+    blocks = sorted({0, nb // 2})
+    t0 = time.perf_counter()
+    worst, bad, rows_n, fitted = {}, {}, 0, 0
+    for b in blocks:
+        rows = stratified_rows(p, p.blocks_refl[b], n_min=n_min // len(blocks), seed=b)
+        w, k, info = check_rows(wl.crop, p, rows, res, b, wl.exp.geom, wl.n_frames, s.ny, s.nx, s.overload,
+                                wl.model.gain)
+        for key, v in w.items():
+            worst[key] = max(worst.get(key, 0.0), v)
+        for key, v in k.items():
+            bad[key] = bad.get(key, 0) + v
+        rows_n += info["rows"]
+        fitted += info["rows_fitted"]
+    return dict(rows=rows_n, rows_fitted=fitted, blocks=blocks,
+                worst={k: float(f"{v:.3g}") for k, v in worst.items()}, outside_tolerance=bad,
+                seconds=round(time.perf_counter() - t0, 1))
 
 
 def _frame_prep_seconds(raw_full, overload):
@@ -217,60 +328,72 @@ def _frame_prep_seconds(raw_full, overload):
     return float(np.median(ts))
 
 
-def _cpu_baseline(blk, budget_s=20.0, max_rows=400):
-    """The oracle restatement of the reference's CPU path on a bounded sample of the block, 1 core: gather, pass 1
-    and pass 2 of sample rows timed directly, plus each reflection's share of the full-frame preparation (one frame
-    timed, charged as frames / reflections of the block)."""
+def random_rows(plan, n, seed=0):
+    """A uniform random sample of n rows (the workload's mix of shoebox shapes in proportion), sorted."""
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(plan.n, min(n, plan.n), replace=False))
+
+
+def row_work(prep, payload, consts):
+    """The restatement's work on rows whose box frames are prepared: gather, pass 1 and pass 2 (the CPU path of
+    XPG for those reflections; default widths and the Gaussian prior profile, which do not change the work)."""
+    from oracle import gather as OG
     from oracle import kernels as OK
-    from oracle import pipeline as OP
-    p = blk.plan
-    s = blk.spec
-    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
-    rows, (y0, x0) = _sample_rows(p, s.nx, s.ny)
-    rows = rows[:max_rows]
-    full = blk.frames[a:a + 3].cpu().numpy().view(np.uint32)
-    t_prep = _frame_prep_seconds(full, s.overload)
-    raw = blk.frames[a:a + wz, y0:y0 + c, x0:x0 + c].cpu().numpy().view(np.uint32)
-    prep = OP.prepared_frames(raw, a, s.overload, [1])
-    g = blk.exp.geom
-    det = OK.detector_consts(g, None)
-    prof = np.repeat(OK.gaussian_profile()[None], p.nreg, 0)
+    det, s0, axis, phi0, osc, sd, sm, rcw, prof = consts
+    vox = 0
+    for (r, nb), (frames, (oy, ox)) in zip(payload, prep):
+        sb = OG.gather_shoebox(frames, sorted(frames), r["iz0"], r["fbi"], r["Dz"], r["bx"], r["iy0"] - oy,
+                               r["ix0"] - ox)
+        o1 = OK.pass1(sb, r, nb, det, s0, axis, phi0, osc, sd, sm, 1.0, rcw)
+        pix = dict(zeta=o1["zeta"], J=o1["J"], u1=o1["u1"], u2=o1["u2"], seff=o1["seff"])
+        OK.pass2(sb, r, nb, det, s0, axis, phi0, osc, sd, sm, 1.0, prof, o1["bg"], o1["nbg"], rcw, pix)
+        vox += sb.size
+    return len(payload), vox
+
+
+def row_consts(spec, geom, nreg):
+    from oracle import kernels as OK
+    prof = np.repeat(OK.gaussian_profile()[None], nreg, 0)
     prof = prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2)
+    return (OK.detector_consts(geom, None), geom.s0.astype(np.float32), geom.axis.astype(np.float32),
+            np.float32(np.radians(geom.z_to_phi(0.0))), np.float32(np.radians(geom.osc)), np.radians(spec.sigma_d),
+            np.radians(spec.sigma_m), OK.rc_default_weights(), prof)
+
+
+def prepared_boxes(crop, plan, rows, n_frames, ny, nx, overload):
+    """Per row: its box frames prepared as XPG's frame loop prepares them, and the window origin."""
+    from oracle.blockcheck import _box_frames
+    return [_box_frames(crop, plan, j, n_frames, ny, nx, overload) for j in rows]
+
+
+def _cpu_baseline(wl, budget_s=20.0, n_rows=400):
+    """The restatement of the reference's CPU path on a bounded sample of the workload, 1 core: gather, pass 1 and
+    pass 2 of a uniform random sample of its rows timed directly, plus each reflection's share of the full-frame
+    preparation (one frame timed, charged as frames / reflections)."""
+    from oracle.pipeline import row_payload
+    p, s = wl.plan, wl.spec
+    rows = random_rows(p, n_rows, seed=7)
+    prep = prepared_boxes(wl.crop, p, rows, wl.n_frames, s.ny, s.nx, s.overload)
+    full = wl.crop(0, 3, 0, s.ny, 0, s.nx)
+    t_prep = _frame_prep_seconds(full, s.overload)
+    consts = row_consts(s, wl.exp.geom, p.nreg)
+    pay = row_payload(p, rows)
     t0 = time.perf_counter()
-    done = 0
+    done = vox = 0
     for k in range(0, rows.size, 20):
-        OP.integrate_rows(prep, list(range(a, a + wz)), OP.row_payload(p, rows[k:k + 20]), det,
-                          g.s0.astype(np.float32), g.axis.astype(np.float32), np.float32(np.radians(g.z_to_phi(0.0))),
-                          np.float32(np.radians(g.osc)), np.radians(s.sigma_d), np.radians(s.sigma_m), 1.0,
-                          OK.rc_default_weights(), prof, origin=(y0, x0))
-        done = k + min(20, rows.size - k)
+        n, v = row_work(prep[k:k + 20], pay[k:k + 20], consts)
+        done += n
+        vox += v
         if time.perf_counter() - t0 > budget_s:
             break
     t_rows = time.perf_counter() - t0
-    per_refl = t_rows / max(done, 1) + t_prep * blk.n_frames / blk.n_refl
+    per_refl = t_rows / max(done, 1) + t_prep * wl.n_frames / wl.n_refl
     return {"value": round(1.0 / per_refl, 2), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{done} reflections of the block (boxes inside frames {a + 1}-{a + wz}): gather, pass 1 and "
-                      f"pass 2 by the numpy oracle in {t_rows:.1f} s, plus the block's full-frame preparation "
-                      f"({t_prep * 1e3:.0f} ms per frame x {blk.n_frames} frames) shared over its {blk.n_refl} "
+            "voxels_per_s": round(vox / t_rows, 1),
+            "sample": f"{done} reflections drawn at random from the workload (its mix of box shapes): gather, pass 1 "
+                      f"and pass 2 by the numpy restatement in {t_rows:.1f} s, plus the full-frame preparation "
+                      f"({t_prep * 1e3:.0f} ms per frame x {wl.n_frames} frames) shared over its {wl.n_refl} "
                       f"reflections"}
-
-
-def _parity(blk, res, n_min=500):
-    """Post-check of the timed run's results (after the timed region): a stratified sample of the block's rows
-    (every shoebox shape group) integrated again by the CPU restatement from the same raw frames with the block's
-    learnt profiles and adapted widths; worst error per key relative to max(|value|, scale) (tests/tolerance.py),
-    and the rows outside tolerance per key (integers: rows that differ)."""
-    from oracle.blockcheck import check_rows, stratified_rows
-    p, s = blk.plan, blk.spec
-    rows = stratified_rows(p, np.arange(p.n), n_min=n_min)
-
-    def crop(f0, f1, y0, y1, x0, x1):
-        return blk.frames[f0:f1, y0:y1, x0:x1].cpu().numpy().view(np.uint32)
-    t0 = time.perf_counter()
-    worst, bad, info = check_rows(crop, p, rows, res, 0, blk.exp.geom, blk.n_frames, s.ny, s.nx, s.overload,
-                                  blk.model.gain)
-    return dict(info, worst={k: float(f"{v:.3g}") for k, v in worst.items()}, outside_tolerance=bad,
-                seconds=round(time.perf_counter() - t0, 1))
 
 
 def run(args):
@@ -287,11 +410,11 @@ def run(args):
         build.build()
     clocks = Clocks(local)
     clocks.start()                # before the set-up: nvidia-smi's start-up load stays out of the timed steps
-    blk = Block(args.workload, seed_offset=rank)
-    src = blk.source()
+    wl = Workload(args.workload, seed_offset=rank)
+    src = wl.source()
     res = None
     for _ in range(args.warmup):  # results held across calls as in the timed loop: the pinned result buffers that
-        res = blk.integrate(src)  # two live results need are allocated here, not in a timed step
+        res = wl.integrate(src)   # two live results need are allocated here, not in a timed step
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -305,7 +428,7 @@ def run(args):
     n_ok = 0
     marks = []
     for _ in range(args.steps):
-        res = blk.integrate(src)
+        res = wl.integrate(src)
         n_ok += int(np.isfinite(res.refl["iprf"]).sum())
         marks.append(torch.cuda.Event(enable_timing=True))
         marks[-1].record()
@@ -318,18 +441,22 @@ def run(args):
     step_ms = [round(a.elapsed_time(b), 1) for a, b in zip([e0] + marks[:-1], marks)]
     ksum = D.TIMER.summary()
     launches = D.TIMER.launches
-    t_max, n_total = reduce_over_ranks(t, blk.n_refl * args.steps, dist)
+    t_max, n_total = reduce_over_ranks(t, wl.n_refl * args.steps, dist)
     value = n_total / t_max
-    # roofline of the dominant kernel
     peak, peak_kind = _peaks()
-    bpk = blk.bytes_per_kernel()
+    b_alg = alg_bytes(wl.spec, wl.n_frames, wl.plan) * args.steps * world
+    pixel_gbs = b_alg / t_max / 1e9
+    # roofline of the dominant kernel
+    bpk = bytes_per_kernel(wl.plan, wl.n_frames)
+    if "unpack" in ksum:
+        bpk["unpack"] = 5.0 * wl.spec.nx * wl.spec.ny * wl.n_frames
     dom = max(ksum, key=lambda k: ksum[k][1]) if ksum else None
     roof = None
     if dom is not None:
         n_l, t_k = ksum[dom]
         per_launch = bpk.get(dom, 0.0) * args.steps / max(n_l, 1)
         achieved = per_launch / (t_k / n_l) / 1e9
-        vox = float((blk.plan.Dz * blk.plan.bx.astype(np.float64) ** 2).sum()) * args.steps / max(n_l, 1)
+        vox = float((wl.plan.Dz * wl.plan.bx.astype(np.float64) ** 2).sum()) * args.steps / max(n_l, 1)
         traffic = round(DRAM_BYTES_PER_VOXEL[dom] * vox / 1e9, 3) if dom in DRAM_BYTES_PER_VOXEL else None
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_unit": "GB per launch",
@@ -337,14 +464,18 @@ def run(args):
                 "launches": n_l, "ms_per_launch": round(t_k / n_l * 1e3, 4),
                 "share": {k: round(v[1] / max(sum(x[1] for x in ksum.values()), 1e-12), 4) for k, v in ksum.items()},
                 "ms_per_step": {k: round(v[1] / args.steps * 1e3, 2) for k, v in ksum.items()}}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = _parity(wl, res_timed)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = _cpu_baseline(wl)
     # end to end: frames from pinned host memory, uploaded inside every step; results read back by the API
     e2e = None
     if not args.no_e2e:
-        host = torch.empty(blk.frames.shape, dtype=torch.int32, pin_memory=True)
-        host.copy_(blk.frames)
-        hsrc = blk.source(host)
-        res = blk.integrate(hsrc)
-        res = blk.integrate(hsrc)
+        wl.drop_resident()
+        hsrc = wl.host_source()
+        res = wl.integrate(hsrc)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
@@ -354,37 +485,34 @@ def run(args):
         moved0 = dict(hsrc.transfer)
         f0.record()
         for _ in range(k2):
-            res = blk.integrate(hsrc)
+            res = wl.integrate(hsrc)
         f1.record()
         torch.cuda.synchronize()
         te, _ = reduce_over_ranks(f0.elapsed_time(f1) * 1e-3, 0, dist)
         n_out = sum(v.nbytes for v in res.refl.values() if isinstance(v, np.ndarray))
-        moved = {k: (hsrc.transfer.get(k, 0) - moved0.get(k, 0)) / k2 for k in ("h2d_bytes", "chunks_raw",
-                                                                                 "chunks_packed")}
-        e2e = {"value": round(blk.n_refl * world * k2 / te, 1), "unit": UNIT,
+        moved = {k: (hsrc.transfer.get(k, 0) - moved0.get(k, 0)) / k2
+                 for k in ("h2d_bytes", "chunks_raw", "chunks_packed")}
+        e2e = {"value": round(wl.n_refl * world * k2 / te, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(moved["h2d_bytes"]), "d2h_bytes_per_step": int(n_out), "steps": k2,
-               "frame_bytes_per_step": int(host.numel() * 4),
-               "chunks_per_step": {"raw": moved["chunks_raw"], "packed": moved["chunks_packed"]}}
-        del host
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = _cpu_baseline(blk)
-    parity = None
-    if rank == 0 and not args.no_parity:
-        parity = _parity(blk, res_timed)
+               "ms_per_step": round(te / k2 * 1e3, 1),
+               "frames_on_host": ("packed transfer encoding, pinned" if wl.store is not None else "uint32, pinned"),
+               "frame_bytes_per_step": int(4 * wl.spec.nx * wl.spec.ny * wl.n_frames)}
+        if wl.store is None:
+            e2e["chunks_per_step"] = {"raw": moved["chunks_raw"], "packed": moved["chunks_packed"]}
     if dist is not None:
         dist.barrier()
     if rank == 0:
-        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": METRICS[args.workload], "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 3), "step_ms": step_ms,
                 "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulation)",
-                "data": "synthetic: seeded 16M-pixel frames rendered on the device (spec in xpg_b200/synth.py)",
-                "config": {"workload": args.workload, "reflections_per_step": blk.n_refl,
-                           "frames_per_step": blk.n_frames, "detector": [blk.spec.nx, blk.spec.ny],
-                           "voxels_per_step": int((blk.plan.Dz * blk.plan.bx ** 2).sum()),
-                           "l2": "inputs larger than L2 (frame stack ~{:.0f} GB)".format(blk.frames.numel() * 4 / 1e9),
-                           "parallelism": f"replicas x{world} (one block per rank)"},
+                "data": "synthetic: seeded 16M-pixel frames rendered on the device (spec in xpg_b200/synth.py)"
+                        + ("; the sweep held in HBM in the packed transfer encoding (widened per wedge in the "
+                           "timed region)" if wl.store is not None else ""),
+                "config": workload_config(args.workload, wl.spec, wl.edges, wl.n_frames, wl.plan, world),
+                "pixel_gbs": round(pixel_gbs, 1), "pixel_hbm_frac": round(pixel_gbs / peak, 4),
+                "voxels_per_s": round(float((wl.plan.Dz * wl.plan.bx.astype(np.float64) ** 2).sum()) * args.steps
+                                      * world / t_max, 1),
                 "integrated_per_step": n_ok // max(args.steps, 1),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "parity": parity}
@@ -396,95 +524,89 @@ def run(args):
 _REF = {}
 
 
-def _ref_init(prep, a, wz, spec_d, nreg, origin):
-    """Worker set-up (spawned process, once per pool): the prepared frame crops and the block constants."""
-    from oracle import kernels as OK
-    from xpg_b200 import synth
-    spec = synth.SweepSpec(**spec_d)
-    g = spec.geometry()
-    prof = np.repeat(OK.gaussian_profile()[None], nreg, 0)
-    _REF.update(prep=prep, a=a, wz=wz, spec=spec, g=g, det=OK.detector_consts(g, None), origin=origin,
-                prof=prof / (prof.sum(axis=(1, 2), keepdims=True) * (9.0 / 40) ** 2))
+def _ref_init(consts):
+    _REF["consts"] = consts
 
 
-def _ref_worker(payload):
-    """Oracle work of one chunk of rows: gather, pass 1, pass 2 from the worker's prepared frame crops."""
-    from oracle import kernels as OK
-    from oracle import pipeline as OP
-    r = _REF
-    g, spec = r["g"], r["spec"]
-    OP.integrate_rows(r["prep"], list(range(r["a"], r["a"] + r["wz"])), payload, r["det"], g.s0.astype(np.float32),
-                      g.axis.astype(np.float32), np.float32(np.radians(g.z_to_phi(0.0))), np.float32(np.radians(g.osc)),
-                      np.radians(spec.sigma_d), np.radians(spec.sigma_m), 1.0, OK.rc_default_weights(), r["prof"],
-                      origin=r["origin"])
-    return len(payload)
+def _ref_worker(job):
+    """Restatement work of one chunk of rows (prepared box frames, payloads) in a worker process."""
+    prep, payload = job
+    return row_work(prep, payload, _REF["consts"])
+
+
+def _native_mapped():
+    """Whether this process has mapped the library (it must not: the reference arm runs no code of this repo's
+    library)."""
+    try:
+        return "libxpgi" in Path("/proc/self/maps").read_text()
+    except OSError:
+        return False
 
 
 def reference_arm(args):
-    """The reference's CPU path (its numpy restatement in oracle/) on all host cores: per step a bounded sample of
-    the block's reflections (gather, pass 1, pass 2 spread over spawned processes) plus their share of the block's
-    full-frame preparation (one frame timed per step, frames spread over the cores as XPG's decode pool does)."""
+    """The reference's CPU path (its numpy restatement in oracle/) on all host cores, on the same workload and config
+    as the device arm: the workload planned by the CPU restatement of the planner, then per step a uniform random
+    sample of its reflections (gather, pass 1, pass 2 spread over spawned processes, from box windows of the same
+    synthetic sweep rendered on the host) plus their share of the full-frame preparation XPG's frame loop does for
+    every frame. No CUDA and none of this repository's library is used."""
     rank, world, local = _env()
     if rank != 0:
         return
     import multiprocessing as mp
-    from dataclasses import asdict
 
-    import torch
-    from oracle import pipeline as OP
+    from oracle.pipeline import row_payload
     from oracle.plan import plan_integration
     from xpg_b200 import synth
-    from xpg_b200.plan import IntegrationModel
     cores = len(os.sched_getaffinity(0))
-    spec = synth.config2() if args.workload == "config2-block" else synth.config1()
-    edges = np.array([0.0, 360.0]) if args.workload == "config2-block" else np.array([0.0, 100.0])
-    exp = spec.experiment()
-    model = IntegrationModel(spec.sigma_d, spec.sigma_m)
-    dmin = spec.resolution_limit()
-    probe = plan_integration([exp], edges, model, dmin, 1e9, (1, spec.nframes), 0.05, spec.n_regions_xy, True, True)
-    n_frames = int(min(max(probe.need_hi) + 1, spec.nframes))
-    p = plan_integration([exp], edges, model, dmin, 1e9, (1, n_frames), 0.05, spec.n_regions_xy, True, True)
-    a, wz, c = SAMPLE["a"], SAMPLE["wz"], SAMPLE["crop"]
-    rows_all, (y0, x0) = _sample_rows(p, spec.nx, spec.ny)
-    _, table = synth.reflection_table(spec, z_range=(a - 40.0, a + wz + 40.0))
-    if torch.cuda.is_available():
-        raw = synth.device_frames(spec, table, a + 1, wz).cpu().numpy().view(np.uint32)
-    else:
-        raw = synth.render_frames(spec, range(a + 1, a + wz + 1), table)
-    prep = OP.prepared_frames(raw[:, y0:y0 + c, x0:x0 + c], a, spec.overload, [1])
-    per_step = max(cores * 24, 48)
-    sd = asdict(spec)
-    sd.pop("U", None)
+    spec, exp, model, edges, n_frames, plan = plan_workload(args.workload, 0, plan_integration)
+    _, table = synth.reflection_table(spec, z_range=(-5.0, n_frames + 5.0))
+
+    def crop(f0, f1, y0, y1, x0, x1):
+        return synth.render_window(spec, table, range(f0 + 1, f1 + 1), y0, y1, x0, x1)
+    per_step = max(cores * 8, 96)
+    n_all = per_step * 2                       # two distinct samples, cycled over the steps
+    rows_all = random_rows(plan, n_all, seed=11)
+    rng = np.random.default_rng(12)
+    rows_all = rows_all[rng.permutation(rows_all.size)]
+    prep_all = prepared_boxes(crop, plan, rows_all, n_frames, spec.ny, spec.nx, spec.overload)
+    pay_all = row_payload(plan, rows_all)
+    full = synth.render_window(spec, table, [1], 0, spec.ny, 0, spec.nx)
+    t_prep = _frame_prep_seconds(full, spec.overload)
+    consts = row_consts(spec, exp.geom, plan.nreg)
     ctx = mp.get_context("spawn")
-    n_done, t_all = 0, 0.0
-    with ctx.Pool(cores, initializer=_ref_init, initargs=(prep, a, wz, sd, p.nreg, (y0, x0))) as pool:
+    n_done, t_all, vox_all = 0, 0.0, 0
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(consts,)) as pool:
         def step(k):
-            lo = (k * per_step) % max(rows_all.size - per_step, 1)
-            rows = rows_all[lo:lo + per_step]
-            chunks = [OP.row_payload(p, rows[i::cores]) for i in range(cores)]
+            lo = (k * per_step) % max(rows_all.size - per_step + 1, 1)
+            idx = list(range(lo, min(lo + per_step, rows_all.size)))
+            jobs = [([prep_all[i] for i in idx[c::cores]], [pay_all[i] for i in idx[c::cores]]) for c in range(cores)]
             t0 = time.perf_counter()
-            n = sum(pool.map(_ref_worker, [ch for ch in chunks if ch]))
+            out = pool.map(_ref_worker, [j for j in jobs if j[1]])
             t_rows = time.perf_counter() - t0
-            t_prep = _frame_prep_seconds(raw[:1], spec.overload)
-            return n, t_rows + t_prep * n_frames / p.n * n / cores
+            n = sum(o[0] for o in out)
+            return n, sum(o[1] for o in out), t_rows + t_prep * n_frames / plan.n * n / cores
         for k in range(args.warmup):
             step(k)
         for k in range(args.steps):
-            n, t = step(args.warmup + k)
+            n, v, t = step(args.warmup + k)
             n_done += n
+            vox_all += v
             t_all += t
     value = n_done / t_all
-    line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    line = {"metric": METRICS[args.workload], "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_all / args.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 accumulation)", "impl": "reference",
-            "data": "synthetic: seeded 16M-pixel frames (spec in xpg_b200/synth.py)",
-            "config": {"workload": args.workload, "reflections_per_step": per_step},
+            "data": "synthetic: the same seeded sweep (spec in xpg_b200/synth.py), box windows rendered on the host",
+            "config": workload_config(args.workload, spec, edges, n_frames, plan, world),
+            "voxels_per_s": round(vox_all / t_all, 1),
             "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{per_step} reflections per step of the block (boxes inside frames "
-                                       f"{a + 1}-{a + wz}, a {c} px detector patch): gather + pass 1 + pass 2 by the "
-                                       f"numpy restatement over {cores} spawned processes, plus their share of the "
-                                       f"block's full-frame preparation"},
-            "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": f"{per_step} reflections per step drawn at random from the workload's "
+                                       f"{plan.n} (its mix of box shapes): gather + pass 1 + pass 2 by the numpy "
+                                       f"restatement over {cores} spawned processes, plus their share of the "
+                                       f"full-frame preparation ({t_prep * 1e3:.0f} ms per frame x {n_frames} "
+                                       f"frames over {cores} cores)"},
+            "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_library_mapped": _native_mapped()}
     print(json.dumps(line), flush=True)
 
 
@@ -609,7 +731,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--workload", default="config2-block", choices=("config2-block", "config2-small", "config1"))
+    ap.add_argument("--workload", default="config2-sweep",
+                    choices=("config2-sweep", "config2-block", "config2-small", "config1"))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -142,7 +142,7 @@ typedef struct {
 
 /* Last error message of this thread (empty when none). */
 const char *xi_last_error(void);
-/* ABI version: increases when a signature or struct above changes (3: XiPass1Out.isum_raw). */
+/* ABI version: increases when a signature or struct above changes (3: XiPass1Out.isum_raw, XiRowSet). */
 int xi_version(void);
 /* Synchronises the stream and reports (then clears) the kernels' status word: XI_E_SHAPE when a row was skipped
  * because its shape exceeded its call's max_bx / max_dz. */
@@ -187,6 +187,30 @@ int xi_finalize_profiles(const double *num, const double *den, int n_regions, fl
  * partner, variances, correlation and recorded fractions. prof: (n_regions, 41, 41). */
 int xi_pass2(const XiDetector *det, const XiRows *rows, const XiBlock *blk, const float *arena, const float *prof,
              const XiPass2In *in, XiPass2Out *out, void *stream);
+
+/* ---- Batched passes: rows of many phi blocks and sweeps in one persistent launch ------------------------------
+ * XPG runs its kernels per shoebox shape and chunk of at most 8192 rows of one block (`process_block`'s chunk loop,
+ * xpg/integrate.py:463-520, `_chunk_size` :145-148, the per-shape kernel cache :347-351). Here one launch takes the
+ * rows of any phi blocks of any sweeps whose boxes fit a size bin: resident CTAs (as many as the SMs hold) take
+ * (set, row) items from a device queue until it is empty, with the same per-row arithmetic and results as
+ * xi_pass1 / xi_pass2. A set is one block's rows with that block's detector, constants, arena and buffers. */
+typedef struct {
+    XiDetector det;
+    XiRows rows;                    /* order, n_order, max_bx, max_dz are not used: the items name the rows */
+    XiBlock blk;                    /* pass 2: the widths adapted for the block's pass 2 */
+    const float *arena;
+    XiPass1Out p1;                  /* pass 1 writes these; pass 2 reads zeta, seff, J, u1, u2, bg and nbg */
+    const float *prof;              /* pass 2: the block's profiles (n_regions, 41, 41) */
+    XiPass2Out p2;                  /* pass 2 writes these */
+} XiRowSet;
+
+/* sets: device array; items: (n_items) int64 set << 32 | row, device, in the order CTAs take them (largest boxes
+ * first balances the launch); every item's box must fit max_bx / max_dz and its set's K <= max_k (others are skipped
+ * and flagged for xi_status); queue: one device int, reset by the call. */
+int xi_pass1_batched(const XiRowSet *sets, const int64_t *items, int n_items, int max_bx, int max_dz, int max_k,
+                     int *queue, void *stream);
+int xi_pass2_batched(const XiRowSet *sets, const int64_t *items, int n_items, int max_bx, int max_dz, int max_k,
+                     int *queue, void *stream);
 
 /* ---- Planning: predictions, shoebox boxes and neighbour lists (float64) -------------------------------------
  * XPG plans an integration run in numpy on the host (xpg/integrate.py:222-316 with the predictions of

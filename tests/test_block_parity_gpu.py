@@ -15,21 +15,18 @@ def test_config2_block_sample_matches_oracle():
     import torch
     import bench
     from oracle.blockcheck import check_rows, stratified_rows
-    blk = bench.Block("config2-block")
-    res = blk.integrate(blk.source())
-    p = blk.plan
+    wl = bench.Workload("config2-block")
+    res = wl.integrate(wl.source())
+    p = wl.plan
     np.testing.assert_array_equal(res.refl["iz0"], p.iz0)
     assert np.isfinite(res.refl["iprf"]).all()
     rows = stratified_rows(p, np.arange(p.n), n_min=500)
     assert rows.size >= 500
     assert p.has_partner[rows].any() and (p.fb[rows] > 1).any()
-    s = blk.spec
-
-    def crop(f0, f1, y0, y1, x0, x1):
-        return blk.frames[f0:f1, y0:y1, x0:x1].cpu().numpy().view(np.uint32)
-    worst, bad, info = check_rows(crop, p, rows, res, 0, blk.exp.geom, blk.n_frames, s.ny, s.nx, s.overload,
-                                  blk.model.gain)
-    del blk, res
+    s = wl.spec
+    worst, bad, info = check_rows(wl.crop, p, rows, res, 0, wl.exp.geom, wl.n_frames, s.ny, s.nx, s.overload,
+                                  wl.model.gain)
+    del wl, res
     torch.cuda.empty_cache()
     assert info["rows_fitted"] > 400
     assert all(v == 0 for v in bad.values()), (bad, worst)

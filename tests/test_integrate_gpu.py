@@ -189,3 +189,60 @@ def test_estimate_sigmas_matches_reference():
     assert hist.shape == z["history"].shape
     np.testing.assert_allclose(hist[:, :2], z["history"][:, :2], rtol=1e-6)
     assert np.array_equal(hist[:, 2], z["history"][:, 2])
+
+
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_packed_store_identical(where):
+    """Frames held in the packed transfer encoding (a PackedStore in pinned host memory, or resident in HBM) and
+    widened wedge by wedge give bit-identical results to the same frames given raw; "binned" has excluded frames
+    (never unpacked) and counts above the packed byte's range."""
+    import torch
+    from xpg_b200 import frames as FR
+    case = "binned"
+    spec = G.case_inputs(case)[0]
+    raw = G.frames_of(case)
+    store = FR.PackedStore(raw.shape[0], spec.ny, spec.nx)
+    store.add_wedge(0, torch.from_numpy(np.ascontiguousarray(raw).view(np.int32)).pin_memory())
+    assert store.index[:, 2].sum() > 0                       # exception pairs were needed
+    src = FR.PackedFrames(store if where == "host" else store.to("cuda"), first=1, overload=spec.overload)
+    a = _run(case).refl
+    b = _run(case, images=src).refl
+    for k in CHECK_F + ("n_over", "n_fg_masked", "isum_raw"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
+    if where == "host":
+        assert src.transfer["h2d_bytes"] > 0
+
+
+def test_pack_generated_frames_round_trip():
+    """pack_generated: frames rendered on the device, packed on the host, widened back on the device bit for bit."""
+    import torch
+    from xpg_b200 import frames as FR
+    from xpg_b200 import synth
+    spec = synth.config1(nframes=12)
+    _, table = synth.reflection_table(spec)
+    ref = synth.device_frames(spec, table, 1, 12)
+    store = FR.pack_generated(lambda k, n, out: out.copy_(ref[k:k + n]), 12, spec.ny, spec.nx, wedge=5)
+    dev = store.to("cuda")
+    out = torch.empty((spec.ny, spec.nx), dtype=torch.int32, device="cuda")
+    for k in range(12):
+        dev.unpack(k, out, torch.cuda.current_stream())
+        assert torch.equal(out, ref[k]), k
+
+
+def test_integration_in_parts_under_a_memory_budget(monkeypatch):
+    """A device budget below the open blocks' buffers: each phi block is integrated in parts of consecutive phi
+    (own profiles and widths), as XPG does when its host budget is short; as the reference's own test of that mode
+    (tests/test_pipeline.py:146-177): the same reflections, median |dI| / sigma < 0.1 against one pass."""
+    from xpg_b200 import memplan
+    case = "adaptive"
+    a = _run(case).refl
+    monkeypatch.setenv("XPG_INTEGRATE_MEM_GB", "0.0002")
+    monkeypatch.setattr(memplan, "BLOCK_PARTS_MAX", 3)
+    res = _run(case)
+    b = res.refl
+    assert len(res.profiles) > 2                          # more parts than the two phi blocks
+    np.testing.assert_array_equal(a["hkl"], b["hkl"])
+    ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
+    assert ok.mean() > 0.9
+    d = np.abs(a["iprf"][ok] - b["iprf"][ok]) / np.sqrt(a["vprf"][ok])
+    assert np.median(d) < 0.1

@@ -251,3 +251,48 @@ def test_largest_box_matches_oracle(with_partner):
     for k in want:
         ok, worst = T.within(k, got[k], want[k], ctx, rel=2e-6)
         assert ok, (k, worst, got[k], want[k])
+
+
+def test_batched_passes_match_per_shape_launches():
+    """Pass 1 and pass 2 of the stored chunks of every fixture (several detectors, block constants, box shapes and
+    neighbour column counts) in shared persistent launches (xi_pass1_batched / xi_pass2_batched, size bins of the
+    box side) give the same bits as one launch per shape (xi_pass1 / xi_pass2)."""
+    from xpg_b200 import device as D
+    sets, ref, keep = [], [], []
+    for case in CASES:
+        spec, tmpl, mask, excl = G.case_inputs(case)
+        det = D.DeviceDetector(spec.geometry(), tmpl)
+        for i in G.chunks(case):
+            d, rc, nb, o1, o2 = G.chunk(case, i)
+            if not o2:
+                continue
+            rows = _rows_from_chunk(d, rc, nb, "cuda")
+            arena = torch.as_tensor(d["sb"].reshape(-1)).cuda()
+            blk, k1 = _block(d)
+            blk2, k2 = _block(d, "p2_")
+            prof = torch.as_tensor(d["prof"]).cuda()
+            a1, a2 = D.Pass1Buffers(rows), D.Pass2Buffers(rows)          # one launch per shape
+            D.pass1(det, rows, blk, arena, a1)
+            D.pass2(det, rows, blk2, arena, prof, a1, a2)
+            b1, b2 = D.Pass1Buffers(rows), D.Pass2Buffers(rows)          # batched
+            sets.append((D.rowset_entry(det, rows, blk, arena, b1), D.rowset_entry(det, rows, blk2, arena, b1, prof,
+                                                                                   b2)))
+            ref.append((a1, a2, b1, b2, rows))
+            keep += [det, arena, k1, k2, prof]
+    D.status()
+    n = len(sets)
+    groups = [(s, np.arange(r[4].n), r[4].bx, r[4].Dz) for s, r in enumerate(ref)]
+    t1 = D.RowSetTable([s[0] for s in sets])
+    t2 = D.RowSetTable([s[1] for s in sets])
+    for bins in ((97,), (17, 23, 41, 97)):
+        launches = D.batched_items(groups, bins)
+        D.pass1_batched(t1, launches)
+        D.pass2_batched(t2, launches)
+        D.status()
+        same = lambda a, b: torch.equal(a.nan_to_num(7.0), b.nan_to_num(7.0)) if a.is_floating_point() else \
+            torch.equal(a, b)
+        for a1, a2, b1, b2, rows in ref:
+            for k in a1.t:
+                assert same(a1.t[k], b1.t[k]), (n, bins, k)
+            for k in a2.t:
+                assert same(a2.t[k], b2.t[k]), (n, bins, k)

@@ -113,3 +113,13 @@ def test_oracle_profile_finalisation_matches_reference(case):
             den += z[k[:-4] + "_den"]
     prof = OK.finalize_profiles(num, den)
     np.testing.assert_allclose(prof, z["prof_0"], rtol=2e-7, atol=0)
+
+
+def test_tolerance_exemption_counts():
+    """The per-fixture counts of rows the tolerance's conditioning rules exempt (tests/tolerance_report.py) stay a
+    small share: pass-2 outputs are compared on at least 90% of the rows, moments on at least half."""
+    import tolerance_report as TR
+    for case in G.CASES:
+        c = TR.counts(case)
+        assert c["pass2_exempt"] <= 0.1 * c["rows"], (case, c)
+        assert c["moments_exempt"] <= 0.5 * c["rows"], (case, c)

@@ -308,12 +308,13 @@ __device__ XiDetector cta_tables(const XiDetector& det, const XiBlock& B, CtaTab
     return d;
 }
 
-// Completes the staging of a shoebox in shared memory: waits for the bulk copy (bounded; on a timeout the status
-// word gets bit 2 and the values are copied with plain loads), or copies with plain loads when the row's arena
-// offset is not 16-byte aligned. Ends with a barrier.
-__device__ void stage_wait(bool tma, unsigned long long* bar, float* stage, const float* sb, int V, int* status) {
+// Completes the staging of a shoebox in shared memory: waits for phase `parity` of the bulk copy's barrier (bounded;
+// on a timeout the status word gets bit 2 and the values are copied with plain loads), or copies with plain loads
+// when the row's arena offset is not 16-byte aligned. Ends with a barrier.
+__device__ void stage_wait(bool tma, unsigned long long* bar, unsigned parity, float* stage, const float* sb, int V,
+                           int* status) {
     bool ok = true;
-    if (tma) ok = mbar_wait(bar, 0, 1ll << 24);
+    if (tma) ok = mbar_wait(bar, parity, 1ll << 24);
     if (!tma || !ok) {
         if (!ok && threadIdx.x == 0) atomicOr(status, 2);
         __syncthreads();
@@ -340,10 +341,13 @@ __host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * 
 // resident CTAs per SM the pass kernels are compiled for (registers per thread <= 65536 / (NT * blocks))
 template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 4 : 8); }
 
+// Pass 1 of one row, by the whole CTA. `bar`: the CTA's bulk-copy barrier (initialised once per CTA), `phase`: its
+// next phase (advanced here when the row is staged by a bulk copy). The caller separates consecutive rows of a CTA
+// with a barrier.
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
-                                              XiPass1Out O, const int32_t* __restrict__ order, int max_bx,
-                                              int max_dz, int* status) {
+__device__ __forceinline__ void pass1_row(const XiDetector& det_g, const XiRows& R, const XiBlock& B,
+                                          const float* __restrict__ arena, const XiPass1Out& O, int row, int max_bx,
+                                          int max_dz, int* status, unsigned long long* bar, unsigned& phase) {
     extern __shared__ __align__(16) unsigned char dyn1[];
     __shared__ CtaTables T;
     __shared__ float xs[XI_MAX_BX], ys[XI_MAX_BX];
@@ -369,7 +373,6 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
     __shared__ int wcnt[NT / 32];
     __shared__ double s_base[2];
 
-    const int row = order ? order[blockIdx.x] : blockIdx.x;
     const int Dz = R.Dz[row], bx = R.bx[row];
     if (Dz < 1 || Dz > max_dz || bx < 3 || bx > max_bx) {
         if (threadIdx.x == 0) atomicOr(status, 1);
@@ -398,14 +401,12 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
         return STAGED ? stage[(size_t)z * P + p] : sb[(size_t)z * P + p] - R.sb_bias;
     };
     // the shoebox streams into shared memory (bulk copy) while the geometry below is computed
-    __shared__ __align__(8) unsigned long long s_bar;
     const unsigned vbytes = (unsigned)(((size_t)Dz * P * sizeof(float)) & ~(size_t)15);   // whole 16-byte units
     const bool tma = STAGED && vbytes > 0 && ((reinterpret_cast<uintptr_t>(sb) & 15) == 0) &&
                      ((reinterpret_cast<uintptr_t>(stage) & 15) == 0);
     if (tma && threadIdx.x == 0) {
-        mbar_init(&s_bar, 1);
-        mbar_expect_tx(&s_bar, vbytes);
-        bulk_copy_g2s(stage, sb, vbytes, &s_bar);
+        mbar_expect_tx(bar, vbytes);
+        bulk_copy_g2s(stage, sb, vbytes, bar);
     }
 
     const XiDetector det = cta_tables(det_g, B, T);
@@ -495,7 +496,10 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
     // A pixel column's background counts are summed in float32 (exact for detector counts: integers whose column
     // sum stays below 2^24; a larger column is summed again in float64) and its template weight as count * bref,
     // so the float64 totals equal voxel-by-voxel float64 sums.
-    if (STAGED) stage_wait(tma, &s_bar, stage, sb, Dz * P, status);
+    if (STAGED) {
+        stage_wait(tma, bar, phase, stage, sb, Dz * P, status);
+        if (tma) phase ^= 1u;
+    }
     const float clip_floor = (0.0f + 3.0f * sqrtf(gain * fmaxf(0.0f, 0.5f))) + 1.0f;
     if (threadIdx.x == 0) s_ncand = 0;
     int neg_bref = 0;
@@ -804,6 +808,63 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, 
     }
 }
 
+// Pass 1, one CTA per row of `order` (one shoebox shape group per launch).
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, XiRows R, XiBlock B,
+                                                              const float* __restrict__ arena, XiPass1Out O,
+                                                              const int32_t* __restrict__ order, int max_bx,
+                                                              int max_dz, int* status) {
+    __shared__ __align__(8) unsigned long long s_bar;
+    if (STAGED && threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    unsigned phase = 0;
+    pass1_row<NT, STAGED>(det_g, R, B, arena, O, order ? order[blockIdx.x] : blockIdx.x, max_bx, max_dz, status,
+                          &s_bar, phase);
+}
+
+// A row set's description copied into the CTA's shared memory (all threads take the same branch: `cur` was read
+// after a barrier); thread 0 records which set it holds once every thread has passed the test.
+__device__ __forceinline__ void load_set(const XiRowSet* __restrict__ sets, int set, XiRowSet* buf, int* cur) {
+    const int* src = reinterpret_cast<const int*>(sets + set);
+    int* dst = reinterpret_cast<int*>(buf);
+    for (int w = threadIdx.x; w < (int)(sizeof(XiRowSet) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    if (threadIdx.x == 0) *cur = set;
+}
+
+// Pass 1 over a queue of (set, row) items: resident CTAs take items in queue order until it is empty, so rows of
+// any blocks and sweeps (of one size bin) share one launch with no tail between shape groups.
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1_q(const XiRowSet* __restrict__ sets,
+                                                                const int64_t* __restrict__ items, int n_items,
+                                                                int max_bx, int max_dz, int max_k, int* queue,
+                                                                int* status) {
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ XiRowSet s_set;
+    __shared__ int s_item, s_cur;
+    if (threadIdx.x == 0) {
+        if (STAGED) mbar_init(&s_bar, 1);
+        s_cur = -1;
+    }
+    unsigned phase = 0;
+    for (;;) {
+        __syncthreads();                 // the previous row's shared memory is free
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) return;
+        const int64_t v = items[it];
+        const int set = (int)(v >> 32);
+        if (set != s_cur) load_set(sets, set, &s_set, &s_cur);
+        if (s_set.rows.K > max_k) {          // neighbour tables are sized for max_k columns: skip, flag
+            if (threadIdx.x == 0) atomicOr(status, 1);
+            continue;
+        }
+        pass1_row<NT, STAGED>(s_set.det, s_set.rows, s_set.blk, s_set.arena, s_set.p1, (int)(v & 0xffffffffll),
+                              max_bx, max_dz, status, &s_bar, phase);
+    }
+}
+
 // ==================================================================================================================
 // pass 2
 // ==================================================================================================================
@@ -821,11 +882,12 @@ __host__ __device__ inline size_t pass2_stage_offset(int P, int max_dz, int cap)
     return pass2_pix_bytes(P, max_dz) + pass2_list_bytes(cap);
 }
 
+// Pass 2 of one row, by the whole CTA (barrier and phase as in pass1_row).
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, XiRows R, XiBlock B, const float* __restrict__ arena,
-                                              const float* __restrict__ prof, XiPass2In I2, XiPass2Out O,
-                                              const int32_t* __restrict__ order, int max_bx, int max_dz, int cap,
-                                              int* status) {
+__device__ __forceinline__ void pass2_row(const XiDetector& det_g, const XiRows& R, const XiBlock& B,
+                                          const float* __restrict__ arena, const float* __restrict__ prof,
+                                          const XiPass2In& I2, const XiPass2Out& O, int row, int max_bx, int max_dz,
+                                          int cap, int* status, unsigned long long* bar, unsigned& phase) {
     extern __shared__ __align__(16) unsigned char dyn2[];
     __shared__ CtaTables T;
     __shared__ float s_prof[XI_GRID * XI_GRID];
@@ -841,7 +903,6 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     __shared__ double tot[16];
     __shared__ float fmax_w[NT / 32][2];
 
-    const int row = order ? order[blockIdx.x] : blockIdx.x;
     const int Dz = R.Dz[row], bx = R.bx[row];
     if (Dz < 1 || Dz > max_dz || bx < 3 || bx > max_bx) {
         if (threadIdx.x == 0) atomicOr(status, 1);
@@ -879,14 +940,12 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     for (int q = threadIdx.x; q < XI_GRID * XI_GRID; q += NT) s_prof[q] = prof_g[q];
     const float* prof_r = s_prof;
     const XiDetector det = cta_tables(det_g, B, T);
-    __shared__ __align__(8) unsigned long long s_bar;
     const unsigned vbytes = (unsigned)(((size_t)Dz * P * sizeof(float)) & ~(size_t)15);   // whole 16-byte units
     const bool tma = STAGED && vbytes > 0 && ((reinterpret_cast<uintptr_t>(sb) & 15) == 0) &&
                      ((reinterpret_cast<uintptr_t>(stage) & 15) == 0);
     if (tma && threadIdx.x == 0) {
-        mbar_init(&s_bar, 1);
-        mbar_expect_tx(&s_bar, vbytes);
-        bulk_copy_g2s(stage, sb, vbytes, &s_bar);
+        mbar_expect_tx(bar, vbytes);
+        bulk_copy_g2s(stage, sb, vbytes, bar);
     }
 
     for (int i = threadIdx.x; i < bx; i += NT) {
@@ -966,7 +1025,10 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
     Mask65 fgz;
     fgz.lo = s_fgz_lo;
     fgz.hi = s_fgz_hi;
-    if (STAGED) stage_wait(tma, &s_bar, stage, sb, Dz * P, status);
+    if (STAGED) {
+        stage_wait(tma, bar, phase, stage, sb, Dz * P, status);
+        if (tma) phase ^= 1u;
+    }
     if (threadIdx.x == 0) s_nlist = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -1226,6 +1288,61 @@ __global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, 
         O.ipartner[row] = Ip;
         O.rho[row] = has_p ? (float)(a12 / sqrt(fmax(a11 * a22, 1e-30))) : 0.0f;
         O.p_fg[row] = p_fgn / fmaxf(p_total, 1e-9f);
+    }
+}
+
+// Pass 2, one CTA per row of `order` (one shoebox shape group per launch).
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2(XiDetector det_g, XiRows R, XiBlock B,
+                                                              const float* __restrict__ arena,
+                                                              const float* __restrict__ prof, XiPass2In I2,
+                                                              XiPass2Out O, const int32_t* __restrict__ order,
+                                                              int max_bx, int max_dz, int cap, int* status) {
+    __shared__ __align__(8) unsigned long long s_bar;
+    if (STAGED && threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    unsigned phase = 0;
+    pass2_row<NT, STAGED>(det_g, R, B, arena, prof, I2, O, order ? order[blockIdx.x] : blockIdx.x, max_bx, max_dz,
+                          cap, status, &s_bar, phase);
+}
+
+// Pass 2 over a queue of (set, row) items (as k_pass1_q); a set's pass-1 outputs are its pass-2 inputs.
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass2_q(const XiRowSet* __restrict__ sets,
+                                                                const int64_t* __restrict__ items, int n_items,
+                                                                int max_bx, int max_dz, int max_k, int cap,
+                                                                int* queue, int* status) {
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ XiRowSet s_set;
+    __shared__ int s_item, s_cur;
+    if (threadIdx.x == 0) {
+        if (STAGED) mbar_init(&s_bar, 1);
+        s_cur = -1;
+    }
+    unsigned phase = 0;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) return;
+        const int64_t v = items[it];
+        const int set = (int)(v >> 32);
+        if (set != s_cur) load_set(sets, set, &s_set, &s_cur);
+        if (s_set.rows.K > max_k) {
+            if (threadIdx.x == 0) atomicOr(status, 1);
+            continue;
+        }
+        XiPass2In in;
+        in.zeta = s_set.p1.zeta;
+        in.seff = s_set.p1.seff;
+        in.J = s_set.p1.J;
+        in.u1 = s_set.p1.u1;
+        in.u2 = s_set.p1.u2;
+        in.bg = s_set.p1.bg;
+        in.nbg = s_set.p1.nbg;
+        pass2_row<NT, STAGED>(s_set.det, s_set.rows, s_set.blk, s_set.arena, s_set.prof, in, s_set.p2,
+                              (int)(v & 0xffffffffll), max_bx, max_dz, cap, status, &s_bar, phase);
     }
 }
 
@@ -1496,6 +1613,52 @@ int launch_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const
     return cuda_check("xi_pass2");
 }
 
+__global__ void k_zero_int(int* p) { *p = 0; }
+
+// Resident CTAs of a persistent launch: as many as the SMs hold at once (at least one).
+template <typename K>
+int resident_grid(K kernel, int nt, size_t smem, int n_items) {
+    int dev = 0, n_sm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess)
+        return -1;
+    const long long g = (long long)(per_sm > 0 ? per_sm : 1) * n_sm;
+    return (int)(g < n_items ? g : n_items);
+}
+
+template <int NT, bool STAGED>
+int launch_pass1_q(const XiRowSet* sets, const int64_t* items, int n_items, int max_bx, int max_dz, int K, int* queue,
+                   cudaStream_t s) {
+    const size_t P = (size_t)max_bx * max_bx;
+    const size_t sm = pass1_pix_bytes((int)P) + (STAGED ? (P * max_dz * sizeof(float) + 15) / 16 * 16 : 0) +
+                      nb_bytes(K, max_bx, max_dz);
+    cudaFuncSetAttribute(k_pass1_q<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_pass1_q<NT, STAGED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    const int grid = resident_grid(k_pass1_q<NT, STAGED>, NT, sm, n_items);
+    if (grid <= 0) return cuda_check("xi_pass1_batched: occupancy");
+    k_zero_int<<<1, 1, 0, s>>>(queue);
+    k_pass1_q<NT, STAGED><<<grid, NT, sm, s>>>(sets, items, n_items, max_bx, max_dz, K, queue, status_ptr());
+    return cuda_check("xi_pass1_batched");
+}
+
+template <int NT, bool STAGED>
+int launch_pass2_q(const XiRowSet* sets, const int64_t* items, int n_items, int max_bx, int max_dz, int K, int cap,
+                   int* queue, cudaStream_t s) {
+    const size_t P = (size_t)max_bx * max_bx;
+    const size_t sm = pass2_stage_offset((int)P, max_dz, cap) +
+                      (STAGED ? (P * max_dz * sizeof(float) + 15) / 16 * 16 : 0) + nb_bytes(K, max_bx, max_dz);
+    cudaFuncSetAttribute(k_pass2_q<NT, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_pass2_q<NT, STAGED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    const int grid = resident_grid(k_pass2_q<NT, STAGED>, NT, sm, n_items);
+    if (grid <= 0) return cuda_check("xi_pass2_batched: occupancy");
+    k_zero_int<<<1, 1, 0, s>>>(queue);
+    k_pass2_q<NT, STAGED><<<grid, NT, sm, s>>>(sets, items, n_items, max_bx, max_dz, K, cap, queue, status_ptr());
+    return cuda_check("xi_pass2_batched");
+}
+
 // Dynamic shared memory available beside the kernels' static arrays (bytes).
 constexpr size_t kStageBudget = 190 * 1024;
 
@@ -1503,6 +1666,46 @@ constexpr size_t kStageBudget = 190 * 1024;
 // pass 2. Larger staging overlaps the box read with the set-up but costs resident CTAs per SM.
 size_t g_stage_max[2] = {48 * 1024, 48 * 1024};
 int g_list_cap = 2048;
+
+// Pass 1 stages boxes of up to g_stage_max[0] bytes when they fit beside the per-pixel tables.
+bool pass1_staged(size_t P, int max_dz) {
+    return P * max_dz * sizeof(float) <= g_stage_max[0] &&
+           pass1_pix_bytes((int)P) + P * max_dz * sizeof(float) + 16 <= kStageBudget;
+}
+
+// Pass 2's shared-memory plan for boxes up to max_bx pixels a side and max_dz bins with K neighbour columns: whether the box is
+// staged, and the fit list's capacity. The largest boxes (up to 97 px, 65 frames) take what the device allows a CTA
+// beyond the kernel's static arrays and the neighbour tables, not the default budget. The fit list holds up to every
+// voxel of small boxes and g_list_cap fitted voxels of large ones (less when shared memory is short; rows whose list
+// overflows fit from the box); the box is staged only when small (it is read once: staging buys the copy's overlap
+// with the set-up, not re-reads).
+int pass2_plan(int max_bx, int max_dz, int K, const char* who, bool* staged, int* cap_out) {
+    const size_t P = (size_t)max_bx * max_bx;
+    const size_t V = P * max_dz;
+    size_t budget = kStageBudget;
+    if (pass2_pix_bytes((int)P, max_dz) + pass2_list_bytes(0) > budget) {
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa, fq;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+            cudaFuncGetAttributes(&fa, k_pass2<256, false>) != cudaSuccess ||
+            cudaFuncGetAttributes(&fq, k_pass2_q<256, false>) != cudaSuccess)
+            return cuda_check(who);
+        const size_t st = fa.sharedSizeBytes > fq.sharedSizeBytes ? fa.sharedSizeBytes : fq.sharedSizeBytes;
+        const size_t fixed = st + nb_bytes(K, max_bx, max_dz);
+        budget = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
+        if (pass2_pix_bytes((int)P, max_dz) + pass2_list_bytes(0) > budget)
+            return fail(XI_E_LIMIT, "pass 2: box too large (per-pixel tables exceed shared memory)");
+    }
+    const size_t fit = (budget - pass2_pix_bytes((int)P, max_dz)) / 8 / 4 * 4;
+    size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
+    if (capz > fit) capz = fit;
+    *cap_out = (int)capz;
+    const size_t base = pass2_stage_offset((int)P, max_dz, *cap_out);
+    if (base > budget) return fail(XI_E_LIMIT, "pass 2: shared memory");
+    *staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= budget;
+    return XI_OK;
+}
 
 }  // namespace
 
@@ -1556,8 +1759,7 @@ int xi_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     if (nblk == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    const bool staged = P * R->max_dz * sizeof(float) <= g_stage_max[0] &&
-                        pass1_pix_bytes((int)P) + P * R->max_dz * sizeof(float) + 16 <= kStageBudget;
+    const bool staged = pass1_staged(P, R->max_dz);
     if (staged) {
         if (P <= 96) return launch_pass1<64, true>(det, R, B, arena, O, s, nblk);
         if (P <= 200) return launch_pass1<128, true>(det, R, B, arena, O, s, nblk);
@@ -1578,32 +1780,10 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     if (nblk == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t P = (size_t)R->max_bx * R->max_bx;
-    const size_t V = P * R->max_dz;
-    // the largest boxes (up to 97 px, 65 frames) take what the device allows a CTA beyond the kernel's static arrays
-    // and the neighbour tables, not the default budget
-    size_t budget = kStageBudget;
-    if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > budget) {
-        int dev = 0, optin = 0;
-        cudaFuncAttributes fa;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-            cudaFuncGetAttributes(&fa, k_pass2<256, false>) != cudaSuccess)
-            return cuda_check("xi_pass2: shared memory limits");
-        const size_t fixed = fa.sharedSizeBytes + nb_bytes(R->K, R->max_bx, R->max_dz);
-        budget = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
-        if (pass2_pix_bytes((int)P, R->max_dz) + pass2_list_bytes(0) > budget)
-            return fail(XI_E_LIMIT, "xi_pass2: box too large (per-pixel tables exceed shared memory)");
-    }
-    // the fit list holds up to every voxel of small boxes and 2048 fitted voxels of large ones; the box itself is
-    // staged only when small (it is read once: staging buys the copy's overlap with the set-up, not re-reads)
-    // (the list shrinks to what shared memory leaves beside the tables; rows whose list overflows fit from the box)
-    const size_t fit = (budget - pass2_pix_bytes((int)P, R->max_dz)) / 8 / 4 * 4;
-    size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
-    if (capz > fit) capz = fit;
-    const int cap = (int)capz;
-    const size_t base = pass2_stage_offset((int)P, R->max_dz, cap);
-    if (base > budget) return fail(XI_E_LIMIT, "xi_pass2: shared memory");
-    const bool staged = V * sizeof(float) <= g_stage_max[1] && base + V * sizeof(float) + 16 <= budget;
+    bool staged = false;
+    int cap = 0;
+    rc = pass2_plan(R->max_bx, R->max_dz, R->K, "xi_pass2", &staged, &cap);
+    if (rc) return rc;
     if (staged) {
         if (P <= 96) return launch_pass2<64, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
         if (P <= 200) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
@@ -1612,6 +1792,51 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     if (P <= 96) return launch_pass2<64, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
     if (P <= 200) return launch_pass2<128, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
     return launch_pass2<256, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
+}
+
+static int batched_check(const XiRowSet* sets, const int64_t* items, int n_items, int max_bx, int max_dz, int max_k,
+                         int* queue, const char* who) {
+    if (n_items < 0) return fail(XI_E_ARG, who);
+    if (n_items && (!sets || !items || !queue)) return fail(XI_E_ARG, who);
+    if (max_bx < 3 || max_bx > XI_MAX_BX || max_dz < 1 || max_dz > XI_MAX_DZ || max_k < 0 || max_k > XI_MAX_K)
+        return fail(XI_E_LIMIT, "batched pass: max_bx / max_dz / max_k outside 3..97 / 1..65 / 0..16");
+    return XI_OK;
+}
+
+int xi_pass1_batched(const XiRowSet* sets, const int64_t* items, int n_items, int max_bx, int max_dz, int max_k,
+                     int* queue, void* stream) {
+    int rc = batched_check(sets, items, n_items, max_bx, max_dz, max_k, queue, "xi_pass1_batched: bad argument");
+    if (rc || n_items == 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t P = (size_t)max_bx * max_bx;
+    if (pass1_staged(P, max_dz)) {
+        if (P <= 96) return launch_pass1_q<64, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+        if (P <= 200) return launch_pass1_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+        return launch_pass1_q<256, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+    }
+    if (P <= 96) return launch_pass1_q<64, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+    if (P <= 200) return launch_pass1_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+    return launch_pass1_q<256, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+}
+
+int xi_pass2_batched(const XiRowSet* sets, const int64_t* items, int n_items, int max_bx, int max_dz, int max_k,
+                     int* queue, void* stream) {
+    int rc = batched_check(sets, items, n_items, max_bx, max_dz, max_k, queue, "xi_pass2_batched: bad argument");
+    if (rc || n_items == 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t P = (size_t)max_bx * max_bx;
+    bool staged = false;
+    int cap = 0;
+    rc = pass2_plan(max_bx, max_dz, max_k, "xi_pass2_batched", &staged, &cap);
+    if (rc) return rc;
+    if (staged) {
+        if (P <= 96) return launch_pass2_q<64, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+        if (P <= 200) return launch_pass2_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+        return launch_pass2_q<256, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+    }
+    if (P <= 96) return launch_pass2_q<64, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+    if (P <= 200) return launch_pass2_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+    return launch_pass2_q<256, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
 }
 
 int xi_gather(const XiFrames* F, const XiGatherRows* G, float* arena, int32_t* cnt, void* stream) {

@@ -2,8 +2,9 @@
 // radial ramp, Gaussian spots (tangential / radial widths, frame-integrated Gaussian rocking curve), Poisson noise
 // from a counter-based hash of (seed, frame, pixel), module gaps at 0xFFFFFFFF.
 //
-// The expected counts are built in place: the output wedge is first used as a float32 image (background, then
-// spots added with atomics) and each pixel is then replaced by its Poisson draw. No scratch memory.
+// Two launches and no scratch memory: every pixel's background draw is written once, then each spot adds its own
+// Poisson draw to the pixels of its window (atomics; a sum of independent Poisson draws is the draw of the summed
+// mean), so a frame costs one write of the wedge plus the spot windows.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -37,87 +38,95 @@ __device__ __forceinline__ bool in_gap(int y, int x, int gaps) {
     return false;
 }
 
-__global__ void k_background(float* __restrict__ img, int n_frames, int ny, int nx, XiSynthBackground bg) {
-    const size_t P = (size_t)ny * nx;
-    const size_t total = P * n_frames;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const size_t p = i % P;
-        const int y = (int)(p / nx), x = (int)(p % nx);
-        const double r = hypot(x + 1.0 - bg.orgx, y + 1.0 - bg.orgy);
-        img[i] = (float)(bg.level * (1.0 + bg.ramp * r / bg.rmax));
-    }
-}
-
-// one CTA per spot: every frame of the wedge its rocking curve reaches (|z - zc| < 5 sigma_z), a window of
-// +-4.5 radial sigma (4..60 px), 2 x 2 sub-pixel samples
-__global__ void k_spots(float* __restrict__ img, int first_frame, int n_frames, int ny, int nx, XiSynthSpots S) {
-    const int r = blockIdx.x;
-    if (r >= S.n) return;
-    const double xc = S.x[r], yc = S.y[r], zc = S.z[r];
-    const double st = S.sig_t[r], sr = S.sig_r[r], sz = S.sig_z[r];
-    const double counts = S.counts[r];
-    double rx = xc - S.orgx, ry = yc - S.orgy;
-    const double rn = hypot(rx, ry);
-    if (rn > 1e-6) { rx /= rn; ry /= rn; } else { rx = 1.0; ry = 0.0; }
-    const int half = min(max((int)ceil(4.5 * sr), 4), 60);
-    const int W = 2 * half + 1;
-    const int ix = (int)floor(xc - 1.0 + 0.5), iy = (int)floor(yc - 1.0 + 0.5);
-    const double norm = 1.0 / (4.0 * 2.0 * 3.141592653589793 * sr * st);
-    for (int w = 0; w < n_frames; ++w) {
-        const double z0 = first_frame - 1 + w, z1 = z0 + 1.0;
-        if (!(zc + 5.0 * sz > z0 && zc - 5.0 * sz < z1)) continue;
-        const double fz = 0.5 * (erf((z1 - zc) / (1.4142135623730951 * sz)) - erf((z0 - zc) / (1.4142135623730951 * sz)));
-        const double amp = counts * fz * norm;
-        float* F = img + (size_t)w * ny * nx;
-        for (int q = threadIdx.x; q < W * W; q += blockDim.x) {
-            const int px = ix - half + q % W, py = iy - half + q / W;
-            if (px < 0 || px >= nx || py < 0 || py >= ny) continue;
-            double g = 0.0;
-            for (int a = 0; a < 2; ++a)
-                for (int b = 0; b < 2; ++b) {
-                    const double dx = px + 1.0 + (b + 0.5) * 0.5 - 0.5 - xc;
-                    const double dy = py + 1.0 + (a + 0.5) * 0.5 - 0.5 - yc;
-                    const double ur = dx * rx + dy * ry, ut = -dx * ry + dy * rx;
-                    g += exp(-0.5 * ((ur / sr) * (ur / sr) + (ut / st) * (ut / st)));
-                }
-            atomicAdd(F + (size_t)py * nx + px, (float)(amp * g));
+// Poisson draw of mean lam from one uniform u (inversion for small means, rounded normal approximation above 40,
+// with a second uniform from the same hash)
+__device__ __forceinline__ uint32_t poisson_draw(float lam, uint64_t h) {
+    const float u = (float)unit_double(h);
+    if (lam < 40.0f) {
+        float pk = __expf(-lam), F = pk;
+        uint32_t n = 0;
+        while (u > F && n < 400) {
+            ++n;
+            pk *= lam / (float)n;
+            F += pk;
         }
+        return n;
     }
+    const float u2 = (float)unit_double(mix64(h ^ 0xD1B54A32D192ED03ull));
+    const float g = sqrtf(-2.0f * __logf(u)) * __cosf(6.2831853f * u2);
+    const float v = floorf(lam + sqrtf(lam) * g + 0.5f);
+    return v <= 0.0f ? 0u : (v >= 4294967040.0f ? 0xFFFFFF00u : (uint32_t)v);
 }
 
-__global__ void k_poisson(float* __restrict__ img, int first_frame, int n_frames, int ny, int nx, uint64_t seed,
-                          int gaps) {
+// background counts of every pixel of the wedge (flat level with a radial ramp), gaps flagged
+__global__ void k_background_counts(uint32_t* __restrict__ out, int first_frame, int n_frames, int ny, int nx,
+                                    XiSynthBackground bg, uint64_t seed, int gaps) {
     const size_t P = (size_t)ny * nx;
     const size_t total = P * n_frames;
-    uint32_t* out = reinterpret_cast<uint32_t*>(img);
+    const float ox = (float)bg.orgx, oy = (float)bg.orgy, lev = (float)bg.level, k = (float)(bg.ramp / bg.rmax);
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const size_t p = i % P;
         const int f = first_frame + (int)(i / P);
         const int y = (int)(p / nx), x = (int)(p % nx);
-        const double lam = (double)img[i];
-        uint32_t k = 0;
+        uint32_t c;
         if (in_gap(y, x, gaps)) {
-            k = 0xFFFFFFFFu;
+            c = 0xFFFFFFFFu;
         } else {
-            const uint64_t h = mix64(seed * 0x9E3779B97F4A7C15ull + ((uint64_t)f << 40) + p);
-            const double u = unit_double(h);
-            if (lam < 40.0) {
-                double pk = exp(-lam), F = pk;
-                uint32_t n = 0;
-                while (u > F && n < 400) {
-                    ++n;
-                    pk *= lam / n;
-                    F += pk;
-                }
-                k = n;
-            } else {
-                const double u2 = unit_double(mix64(h ^ 0xD1B54A32D192ED03ull));
-                const double g = sqrt(-2.0 * log(u)) * cos(6.283185307179586 * u2);
-                const double v = floor(lam + sqrt(lam) * g + 0.5);
-                k = v <= 0.0 ? 0u : (v >= 4294967294.0 ? 0xFFFFFFFEu : (uint32_t)v);
-            }
+            const float r = hypotf((float)x + 1.0f - ox, (float)y + 1.0f - oy);
+            c = poisson_draw(lev * (1.0f + k * r), mix64(seed * 0x9E3779B97F4A7C15ull + ((uint64_t)f << 40) + p));
         }
-        out[i] = k;
+        out[i] = c;
+    }
+}
+
+// spot counts added to the background's: one CTA per spot, every frame of the wedge its rocking curve reaches
+// (|z - zc| < 5 sigma_z), a window of +-4.5 radial sigma (4..60 px), 2 x 2 sub-pixel samples of the Gaussian, an
+// independent Poisson draw per pixel (the sum of the two draws is the Poisson draw of the summed mean)
+__global__ void k_spot_counts(uint32_t* __restrict__ out, int first_frame, int n_frames, int ny, int nx,
+                              XiSynthSpots S, uint64_t seed, int gaps) {
+    if ((int)blockIdx.x >= S.n) return;
+    const int r = S.index ? S.index[blockIdx.x] : (int)blockIdx.x;
+    const double xc = S.x[r], yc = S.y[r], zc = S.z[r];
+    const double sz = S.sig_z[r];
+    const float st = (float)S.sig_t[r], sr = (float)S.sig_r[r];
+    double rx = xc - S.orgx, ry = yc - S.orgy;
+    const double rn = hypot(rx, ry);
+    if (rn > 1e-6) { rx /= rn; ry /= rn; } else { rx = 1.0; ry = 0.0; }
+    const float frx = (float)rx, fry = (float)ry;
+    const int half = min(max((int)ceil(4.5 * (double)sr), 4), 60);
+    const int W = 2 * half + 1;
+    const int ix = (int)floor(xc - 1.0 + 0.5), iy = (int)floor(yc - 1.0 + 0.5);
+    const float fxc = (float)(xc - ix), fyc = (float)(yc - iy);       // centre relative to the middle pixel's index
+    const double norm = 1.0 / (4.0 * 2.0 * 3.141592653589793 * (double)sr * (double)st);
+    const uint64_t salt = seed * 0xC2B2AE3D27D4EB4Full + (uint64_t)r * 0x165667B19E3779F9ull;
+    for (int w = 0; w < n_frames; ++w) {
+        const double z0 = first_frame - 1 + w, z1 = z0 + 1.0;
+        if (!(zc + 5.0 * sz > z0 && zc - 5.0 * sz < z1)) continue;
+        const double fz = 0.5 * (erf((z1 - zc) / (1.4142135623730951 * sz)) - erf((z0 - zc) / (1.4142135623730951 * sz)));
+        const float amp = (float)(S.counts[r] * fz * norm);
+        if (!(amp > 0.0f)) continue;
+        uint32_t* F = out + (size_t)w * ny * nx;
+        for (int q = threadIdx.x; q < W * W; q += blockDim.x) {
+            const int dxp = q % W - half, dyp = q / W - half;
+            const int px = ix + dxp, py = iy + dyp;
+            if (px < 0 || px >= nx || py < 0 || py >= ny || in_gap(py, px, gaps)) continue;
+            float g = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    // pixel (ix + dxp) spans coordinates ix + dxp + 0.5 .. + 1.5; sub-sample centres at +-0.25
+                    const float dx = (float)dxp + (1.0f - fxc) + ((b + 0.5f) * 0.5f - 0.5f);
+                    const float dy = (float)dyp + (1.0f - fyc) + ((a + 0.5f) * 0.5f - 0.5f);
+                    const float ur = dx * frx + dy * fry, ut = -dx * fry + dy * frx;
+                    g += __expf(-0.5f * ((ur / sr) * (ur / sr) + (ut / st) * (ut / st)));
+                }
+            const float lam = amp * g;
+            if (lam < 1e-7f) continue;
+            const uint32_t c = poisson_draw(lam, mix64(salt + ((uint64_t)(first_frame + w) << 40) +
+                                                        (uint64_t)py * nx + px));
+            if (c) atomicAdd(F + (size_t)py * nx + px, c);
+        }
     }
 }
 
@@ -135,11 +144,9 @@ int xi_synth_frames(const XiSynthSpots* spots, const XiSynthBackground* bg, int 
     }
     if (n_frames == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    float* img = reinterpret_cast<float*>(out);
     const int grid = 148 * 16;
-    k_background<<<grid, 256, 0, s>>>(img, n_frames, ny, nx, *bg);
-    if (spots->n > 0) k_spots<<<spots->n, 128, 0, s>>>(img, first_frame, n_frames, ny, nx, *spots);
-    k_poisson<<<grid, 256, 0, s>>>(img, first_frame, n_frames, ny, nx, seed, gaps);
+    k_background_counts<<<grid, 256, 0, s>>>(out, first_frame, n_frames, ny, nx, *bg, seed, gaps);
+    if (spots->n > 0) k_spot_counts<<<spots->n, 128, 0, s>>>(out, first_frame, n_frames, ny, nx, *spots, seed, gaps);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_err, sizeof g_err, "xi_synth_frames: %s", cudaGetErrorString(e));

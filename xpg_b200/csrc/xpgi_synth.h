@@ -10,7 +10,8 @@ extern "C" {
 #endif
 
 typedef struct {
-    int n;                                  /* spots */
+    int n;                                  /* spots rendered (entries of index, or the first n spots) */
+    const int32_t *index;                   /* (n) spots rendered, as indices into the arrays below; NULL: 0..n-1 */
     const double *x, *y, *z;                /* predicted centre (pixels, frame coordinate) */
     const double *counts;                   /* photons of the whole reflection */
     const double *sig_t, *sig_r, *sig_z;    /* tangential / radial width (pixels), rocking width (frames) */

@@ -475,3 +475,89 @@ def host_groups(rows: RowSet, idx):
 def subset_groups(rows: RowSet, idx):
     """Launch groups of the local rows idx, with device order tensors."""
     return [(b, dz, h2d(r, None, rows.device)) for b, dz, r in host_groups(rows, idx)]
+
+
+# ---- batched passes: rows of many blocks (of many sweeps) per launch --------------------------------------------
+
+def rowset_entry(det: DeviceDetector, rows: RowSet, blk, arena, p1: Pass1Buffers, prof=None, p2=None):
+    """XiRowSet of one block's rows: its detector, constants, arena and buffers (pass 2: profiles and outputs)."""
+    e = N.XiRowSet()
+    e.det = det.s
+    e.rows = rows.s
+    e.blk = blk
+    e.arena = N.ptr(arena)
+    e.p1 = p1.s
+    if prof is not None:
+        e.prof = N.ptr(prof)
+    if p2 is not None:
+        e.p2 = p2.s
+    return e
+
+
+class RowSetTable:
+    """The XiRowSet array of a batched call, in device memory."""
+
+    def __init__(self, entries, device="cuda"):
+        arr = (N.XiRowSet * len(entries))(*entries)
+        self.t = h2d(np.frombuffer(bytes(arr), np.uint8), None, device)
+        self.n = len(entries)
+        self.k_max = max((int(e.rows.K) for e in entries), default=0)
+
+
+# Size bins of a batched launch: upper bounds on the box side; a bin's launch sizes shared memory and threads for its
+# largest box (the side bucket) and depth. Chosen by xpg_b200.tune (measured) unless given.
+DEFAULT_BINS = (17, 31, 41, 55, 97)
+
+
+def batched_items(groups, bins=None, device="cuda"):
+    """Launch bins of a batched pass. groups: (set index, local rows, their sides, their depths) per set. Returns
+    [(max_bx, max_dz, items)] with items an int64 device tensor (set << 32 | row), each bin's rows largest box
+    first (resident CTAs take the big rows before the small ones, which balances the launch)."""
+    bins = tuple(bins or DEFAULT_BINS)
+    cols = [(np.full(len(r), s, np.int64), np.asarray(r, np.int64), np.asarray(b, np.int64), np.asarray(d, np.int64))
+            for s, r, b, d in groups if len(r)]
+    if not cols:
+        return []
+    st, rw, bx, dz = (np.concatenate([c[k] for c in cols]) for k in range(4))
+    which = np.searchsorted(np.asarray(bins), bx, side="left")
+    if (which >= len(bins)).any():
+        raise ValueError("a box side beyond the largest size bin")
+    out = []
+    for k in np.unique(which):
+        m = np.flatnonzero(which == k)
+        vol = bx[m] * bx[m] * dz[m]
+        o = m[np.argsort(-vol, kind="stable")]
+        items = (st[o] << 32) | rw[o]
+        out.append((int(bx[m].max()), int(dz[m].max()), h2d(items, None, device)))
+    return out
+
+
+_QUEUES = {}
+
+
+def _queue(device):
+    key = torch.device(device).index if torch.device(device).index is not None else torch.cuda.current_device()
+    if key not in _QUEUES:
+        _QUEUES[key] = torch.zeros(64, dtype=torch.int32, device=device)
+    return _QUEUES[key]
+
+
+def pass1_batched(table: RowSetTable, launches, stream=None):
+    """Pass 1 of every item of the launches (batched_items), one persistent launch per size bin."""
+    lib = N.load()
+    q = _queue(table.t.device)
+    for i, (mbx, mdz, items) in enumerate(launches):
+        with TIMER.span("pass1"):
+            N.check(lib.xi_pass1_batched(N.ptr(table.t), N.ptr(items), int(items.numel()), mbx, mdz, table.k_max,
+                                         C.c_void_p(q.data_ptr() + 4 * (i % 64)), _stream(stream)),
+                    "xi_pass1_batched")
+
+
+def pass2_batched(table: RowSetTable, launches, stream=None):
+    lib = N.load()
+    q = _queue(table.t.device)
+    for i, (mbx, mdz, items) in enumerate(launches):
+        with TIMER.span("pass2"):
+            N.check(lib.xi_pass2_batched(N.ptr(table.t), N.ptr(items), int(items.numel()), mbx, mdz, table.k_max,
+                                         C.c_void_p(q.data_ptr() + 4 * (i % 64)), _stream(stream)),
+                    "xi_pass2_batched")

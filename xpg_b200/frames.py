@@ -520,8 +520,260 @@ class BSLZ4Frames:
         return d, False
 
 
+class PackedStore:
+    """uint32 frames held in the library's transfer encoding (`xi_pack_u8`: one byte a pixel, exception pairs for
+    counts of 254 and above): about a quarter of the raw frames' size, so a whole sweep fits in host memory or in
+    HBM. Frames live in segments (uint8 tensors, pinned host memory or device memory) at 16-byte aligned offsets;
+    a frame with more than 1/64 exception pixels is kept raw (4 bytes a pixel). `to(device)` copies the segments to
+    the device (frames resident in HBM in packed form)."""
+
+    SEGMENT = 1 << 31
+
+    def __init__(self, n_frames, ny, nx, segments=None, index=None):
+        self.n_frames, self.ny, self.nx = int(n_frames), int(ny), int(nx)
+        self.P = self.ny * self.nx
+        self.plane = (self.P + 15) // 16 * 16
+        self.segments = segments if segments is not None else []
+        self.index = index if index is not None else np.zeros((self.n_frames, 4), np.int64)   # seg, off, n_exc, raw
+        self._fill = 0
+
+    @property
+    def nbytes(self):
+        return int(sum(int(self.frame_bytes(k)) for k in range(self.n_frames)))
+
+    def frame_bytes(self, k):
+        seg, off, ne, raw = self.index[k]
+        return 4 * self.P if raw else self.plane + (8 * ne + 15) // 16 * 16
+
+    def _room(self, nbytes):
+        if not self.segments or self._fill + nbytes > self.segments[-1].numel():
+            self.segments.append(torch.empty(max(self.SEGMENT, nbytes), dtype=torch.uint8, pin_memory=True))
+            self._fill = 0
+        off = self._fill
+        self._fill += (nbytes + 15) // 16 * 16
+        return len(self.segments) - 1, off
+
+    def add_wedge(self, first_k, host_u32, threads=0):
+        """Packs frames first_k.. from a pinned uint32 host tensor (n, ny, nx) on the host's cores."""
+        import ctypes as C
+        from . import native
+        lib = native.load()
+        cap = max(1024, self.P // 64)
+        n_exc = C.c_int64()
+        for w in range(int(host_u32.shape[0])):
+            src = host_u32[w]
+            seg, off = self._room(self.plane + 8 * cap)
+            base = self.segments[seg].data_ptr() + off
+            rc = lib.xi_pack_u8(C.c_void_p(src.data_ptr()), self.P, C.c_void_p(base), C.c_void_p(base + self.plane),
+                                cap, threads, C.byref(n_exc))
+            if rc == native.XI_E_LIMIT:                  # too many exceptions: the frame stays raw
+                self._fill = off
+                seg, off = self._room(4 * self.P)
+                self.segments[seg][off:off + 4 * self.P].copy_(src.reshape(-1).view(torch.uint8))
+                self.index[first_k + w] = (seg, off, 0, 1)
+                continue
+            native.check(rc, "xi_pack_u8")
+            used = self.plane + (8 * n_exc.value + 15) // 16 * 16
+            self._fill = off + used
+            self.index[first_k + w] = (seg, off, n_exc.value, 0)
+
+    def to(self, device):
+        """The same frames with every segment copied to `device` (trimmed to what the frames use)."""
+        used = np.zeros(len(self.segments), np.int64)
+        for k in range(self.n_frames):
+            seg, off = int(self.index[k, 0]), int(self.index[k, 1])
+            used[seg] = max(used[seg], off + self.frame_bytes(k))
+        segs = [s[:int(u)].to(device) for s, u in zip(self.segments, used)]
+        return PackedStore(self.n_frames, self.ny, self.nx, segs, self.index.copy())
+
+    def unpack(self, k, out, stream):
+        """Frame k into out (device uint32 / int32 frame, 16-byte aligned) on `stream`; the store must be on the
+        device."""
+        import ctypes as C
+        from . import native
+        seg, off, ne, raw = (int(v) for v in self.index[k])
+        src = self.segments[seg]
+        if raw:
+            with torch.cuda.stream(stream):
+                out.reshape(-1).view(torch.uint8).copy_(src[off:off + 4 * self.P], non_blocking=True)
+            return
+        base = src.data_ptr() + off
+        native.check(native.load().xi_unpack_u8(C.c_void_p(base), self.P, C.c_void_p(base + self.plane), ne,
+                                                C.c_void_p(out.data_ptr()), C.c_void_p(stream.cuda_stream)),
+                     "xi_unpack_u8")
+
+
+def pack_generated(render, n_frames, ny, nx, wedge=16, device="cuda"):
+    """PackedStore of n_frames frames rendered on the device: `render(first_k, n, out)` writes frames
+    first_k..first_k+n-1 (0-based) into the device int32 tensor out (n, ny, nx); each wedge is read back into pinned
+    memory and packed on the host's cores."""
+    store = PackedStore(n_frames, ny, nx)
+    dev = torch.empty((wedge, ny, nx), dtype=torch.int32, device=device)
+    host = torch.empty((wedge, ny, nx), dtype=torch.int32, pin_memory=True)
+    for k in range(0, n_frames, wedge):
+        n = min(wedge, n_frames - k)
+        render(k, n, dev[:n])
+        host[:n].copy_(dev[:n])
+        store.add_wedge(k, host[:n])
+    return store
+
+
+class _PackedFeeder:
+    """Unpacks the wedges of a run from a PackedStore ahead of the integration: one thread issues, per wedge, the
+    packed frames' copies to the device (from pinned host memory, on a copy stream; none when the store is on the
+    device) and their unpacks (on a stream of their own); at most `depth` wedges are held on the device."""
+
+    def __init__(self, store, first, wedges, oks, device, depth=3, stats=None):
+        self.store, self.first = store, first
+        self.wedges, self.oks = wedges, oks
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.s_cp, _, self.s_un = _transfer_streams(self.device)
+        self.on_device = store.segments[0].is_cuda if store.segments else True
+        self.ready = [threading.Event() for _ in wedges]
+        self.out = [None] * len(wedges)
+        self.held = [False] * len(wedges)
+        self.slots = threading.Semaphore(depth)
+        self.stats = stats if stats is not None else {}
+        self.stats.setdefault("h2d_bytes", 0)
+        self.error = None
+        self.stopping = False
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _run(self):
+        from .device import TIMER
+        try:
+            torch.cuda.set_device(self.device)
+            st = self.store
+            stage, stage_ev = [], []
+            if not self.on_device:
+                cap = max(st.frame_bytes(k) for k in range(st.n_frames)) if st.n_frames else 16
+                with torch.cuda.stream(self.s_cp):
+                    stage = [torch.empty(cap, dtype=torch.uint8, device=self.device) for _ in range(4)]
+                stage_ev = [None] * len(stage)
+                for t in stage:
+                    t.record_stream(self.s_un)
+            q = 0
+            for w, (fa, fb) in enumerate(self.wedges):
+                if not self.oks[w].any():
+                    self.ready[w].set()
+                    continue
+                self.slots.acquire()
+                if self.stopping:
+                    return
+                self.held[w] = True
+                n = fb - fa + 1
+                with torch.cuda.stream(self.s_un):
+                    d = torch.empty((n, st.ny, st.nx), dtype=torch.int32, device=self.device)
+                for i in range(n):
+                    if not self.oks[w][i]:
+                        continue
+                    k = fa - self.first + i
+                    if self.on_device:
+                        with torch.cuda.stream(self.s_un), TIMER.span("unpack"):
+                            st.unpack(k, d[i], self.s_un)
+                        continue
+                    seg, off = int(st.index[k, 0]), int(st.index[k, 1])
+                    nb = st.frame_bytes(k)
+                    if stage_ev[q] is not None:
+                        self.s_cp.wait_event(stage_ev[q])       # the unpack that last read this slot has run
+                    with torch.cuda.stream(self.s_cp):
+                        stage[q][:nb].copy_(st.segments[seg][off:off + nb], non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(self.s_cp)
+                    self.s_un.wait_event(ev)
+                    one = PackedStore(1, st.ny, st.nx, [stage[q]], np.array([[0, 0] + list(st.index[k, 2:])]))
+                    with torch.cuda.stream(self.s_un), TIMER.span("unpack"):
+                        one.unpack(0, d[i], self.s_un)
+                    ue = torch.cuda.Event()
+                    ue.record(self.s_un)
+                    stage_ev[q] = ue
+                    q = (q + 1) % len(stage)
+                    self.stats["h2d_bytes"] += nb
+                ready = torch.cuda.Event()
+                ready.record(self.s_un)
+                self.out[w] = (d, ready)
+                self.ready[w].set()
+        except BaseException as e:
+            self.error = e
+            for r in self.ready:
+                r.set()
+
+    def get(self, w):
+        self.ready[w].wait()
+        if self.error is not None:
+            raise RuntimeError("packed frame transfer failed") from self.error
+        d, ev = self.out[w]
+        self.out[w] = None
+        cur = torch.cuda.current_stream()
+        cur.wait_event(ev)
+        d.record_stream(cur)
+        return d
+
+    def done_with(self, w):
+        self.ready[w].wait()
+        self.out[w] = None
+        if self.held[w]:
+            self.held[w] = False
+            self.slots.release()
+
+    def close(self):
+        self.stopping = True
+        for _ in range(len(self.wedges) + 1):
+            self.slots.release()
+        self.t.join()
+
+
+class PackedFrames:
+    """Raw uint32 frames given as a PackedStore (in pinned host memory: each wedge's packed bytes cross the link and
+    are widened on the device; in device memory: widened there), then the uint32 path: the same results as the
+    frames given raw."""
+
+    def __init__(self, store, first=1, overload=1 << 20, min_valid=0, device="cuda", depth=3):
+        self.store = store
+        self.first = int(first)
+        self.last = self.first + store.n_frames - 1
+        self.ny, self.nx = store.ny, store.nx
+        self.overload = int(overload) if overload is not None else None
+        self.min_valid = int(min_valid)
+        self.device = device
+        self.resident = False
+        self.depth = depth
+        self.transfer = {}
+
+    def feeder(self, wedges, oks):
+        return _PackedFeeder(self.store, self.first, wedges, oks, self.device, self.depth, self.transfer)
+
+
+class GeneratedFrames:
+    """Frames of a synthetic sweep rendered on the device as the integration asks for them (the generator of
+    xpg_b200.synth, `DeviceSpots`): each wedge is rendered into a fresh device buffer on the current stream, then the
+    uint32 path. For sweeps and request streams whose frames are produced on the device (nothing crosses the host
+    link); the rendering is part of the timed work."""
+
+    def __init__(self, spots, first=1, last=None, overload=1 << 20, device="cuda"):
+        spec = spots.spec
+        self.spots = spots
+        self.first = int(first)
+        self.last = int(last) if last is not None else spec.nframes
+        self.ny, self.nx = spec.ny, spec.nx
+        self.overload = int(overload) if overload is not None else None
+        self.min_valid = 0
+        self.device = device
+        self.resident = False
+
+    def wedge(self, f_a, f_b, ok=None, stream=None):
+        from .device import TIMER
+        d = torch.empty((f_b - f_a + 1, self.ny, self.nx), dtype=torch.int32, device=self.device)
+        with TIMER.span("generate", 2):
+            self.spots.render(f_a, f_b - f_a + 1, d, stream)
+        return d, False
+
+
 def as_frame_source(images, device="cuda"):
-    if isinstance(images, (U32Frames, ImageSetFrames, BSLZ4Frames)):
+    if isinstance(images, (U32Frames, ImageSetFrames, BSLZ4Frames, PackedFrames, GeneratedFrames)):
         return images
     if _bitshuffled_imageset(images):
         return BSLZ4Frames(images.read_chunk, images.ny, images.nx, esize=int(np.dtype(images.dtype).itemsize),

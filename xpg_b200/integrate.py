@@ -21,6 +21,7 @@ import torch
 
 from . import adapt as A
 from . import device as D
+from . import memplan
 from . import native as N
 from .frames import as_frame_source
 from .geometry import centring_allowed
@@ -129,246 +130,337 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
               n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed):
     """Integrate a sweep (`xpg/integrate.py:209-999`). `exp_blocks`: one experiment per phi block, `block_edges` in
     frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id)."""
-    N.require_cuda()
-    t0 = time.time()
-    lattice_of = [0] * len(exp_blocks)
-    if extra_lattices:
-        exp_blocks = list(exp_blocks)
-        for li, lat in enumerate(extra_lattices, start=1):
-            exp_blocks += list(lat)
-            lattice_of += [li] * len(lat)
-    src = as_frame_source(images, device)
-    if frames is None:
-        frames = (src.first, src.last)
-    f_first, f_last = int(frames[0]), int(frames[1])
-    excl = set(int(f) for f in exclude_frames)
-    # wedges of the run; frames in pinned host memory start moving to the device now, under the planning
-    resident = bool(getattr(src, "resident", False))
-    W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
-    wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
-    oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in wedges]
-    feeder = src.feeder(wedges, oks) if (hasattr(src, "feeder") and not resident) else None
+    run = SweepRun(images, exp_blocks, block_edges, model, dmin, dmax, frames, mask, minimum_zeta, verbose, log,
+                   n_regions_xy, learn_profiles, exclude_frames, adaptive, deconvolve_overlaps, extra_lattices,
+                   bkg_template, foreign_spots, n_foreign, moments_only, wedge_frames=wedge_frames, device=device,
+                   allowed=allowed)
     try:
-        return _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, block_edges, model, dmin,
-                          dmax, f_first, f_last, excl, mask, minimum_zeta, verbose, log, n_regions_xy,
-                          learn_profiles, adaptive, deconvolve_overlaps, bkg_template, foreign_spots, n_foreign,
-                          moments_only, device, allowed)
+        for w in range(len(run.wedges)):
+            for b in run.feed(w):
+                run.process(b)
+            run.early_pass1(w)
+        for b in run.remaining():
+            run.process(b)
+        return run.result()
     finally:
-        if feeder is not None:
-            feeder.close()
+        run.close()
 
 
-def _integrate(src, feeder, wedges, oks, resident, t0, exp_blocks, lattice_of, block_edges, model, dmin, dmax,
-               f_first, f_last, excl, mask, minimum_zeta, verbose, log, n_regions_xy, learn_profiles, adaptive,
-               deconvolve_overlaps, bkg_template, foreign_spots, n_foreign, moments_only, device, allowed):
-    plan = plan_integration(exp_blocks, block_edges, model, dmin, dmax, (f_first, f_last), minimum_zeta,
-                            n_regions_xy, adaptive, deconvolve_overlaps, lattice_of, foreign_spots, n_foreign, allowed)
-    refl = plan.refl
-    n = plan.n
-    if verbose:
-        log(f"  INTEGRATE: {plan.info['n_predicted']} predicted reflections, box {plan.box}x{plan.box} px, sigma_D "
-            f"{model.sigma_d:.4f} sigma_M {model.sigma_m:.4f} deg; {plan.info['n_wide']} wide in phi (> {MAX_DZ} "
-            f"frames): integrated in bins, {plan.info['n_trunc']} of them still truncated")
-    out = {k: np.empty(n, np.float64) for k in OUT_F64}           # every processed block fills its rows
-    out["n_over"] = np.zeros(n, np.int32)
-    out["n_fg_masked"] = np.zeros(n, np.int32)
-    out["isum_raw"] = np.full(n, -1, np.int64)                    # -1: not integrated (rows of no processed block)
-    keep_fz = not learn_profiles
-    fz_out = np.zeros((n, MAX_DZ), np.float32) if keep_fz else None
-    nreg = plan.nreg
-    sd = np.radians(model.sigma_d)
-    sm = np.radians(model.sigma_m)
-    state = dict(sd=sd, sm=sm, rcw=A.rc_default_weights())
-    block_params, prof_by_block, block_widths = {}, {}, {}
-    t_dev = 0.0
-    nblocks = len(exp_blocks)
-    blocks_rows = plan.blocks_refl                     # plan order (a launch groups its rows by shape itself)
-    read = [f for f in range(f_first, f_last + 1) if f not in excl]
-    read_fi = np.array([f - 1 for f in read], np.int64)
-    # a block takes every frame read up to the first frame read at or after its last needed frame
-    # (`xpg/integrate.py:789-793`: completion is checked after the frame's gather)
-    eff_hi = {}
-    for b in range(nblocks):
-        if plan.blocks_refl[b].size:
-            k = np.searchsorted(read_fi, plan.need_hi[b], "left")
-            eff_hi[b] = int(read_fi[min(k, len(read_fi) - 1)]) if len(read_fi) else -1
-    pending = sorted((b for b in range(nblocks) if plan.blocks_refl[b].size), key=lambda b: plan.need_lo[b])
-    opened, open_order = {}, []
-    det_cache = {}
-    mask_t = None
-    if mask is not None and not np.asarray(mask).all():
-        mask_t = D.h2d(np.asarray(mask, np.uint8), None, device)
+class SweepRun:
+    """One sweep's integration as a sequence of stages a scheduler can interleave with other sweeps': `feed(w)`
+    gathers wedge w into the open blocks and returns the blocks it completed (in the order they are processed); a
+    completed block then goes through `pass1_stage` (bin decode; pass 1 of its rows not done yet, or their launch
+    items for a batched launch), `learn` (profile accumulation, the adaptation of the widths on the host, profile
+    finalisation, pass-2 constants), `pass2_stage` (pass 2, or its items) and `collect` (results to the host).
+    `process(b)` runs the four in order. Blocks of one sweep must be processed in the order feed / remaining return
+    them: each block's pass 1 takes the widths adapted by the blocks processed before it."""
 
-    def detector(g):
-        key = (id(g), id(bkg_template))
-        if key not in det_cache:
-            det_cache.clear()
-            det_cache[key] = D.DeviceDetector(g, bkg_template, device)
-        return det_cache[key]
+    def __init__(self, images, exp_blocks, block_edges, model, dmin, dmax=1e9, frames=None, mask=None,
+                 minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
+                 adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
+                 n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda",
+                 allowed=centring_allowed, early_pass1=True, plan=None, mem_budget=None):
+        N.require_cuda()
+        self.t0 = time.time()
+        lattice_of = [0] * len(exp_blocks)
+        if extra_lattices:
+            exp_blocks = list(exp_blocks)
+            for li, lat in enumerate(extra_lattices, start=1):
+                exp_blocks += list(lat)
+                lattice_of += [li] * len(lat)
+        self.exp_blocks = exp_blocks
+        src = as_frame_source(images, device)
+        if frames is None:
+            frames = (src.first, src.last)
+        f_first, f_last = int(frames[0]), int(frames[1])
+        excl = set(int(f) for f in exclude_frames)
+        # wedges of the run; frames in pinned host memory start moving to the device now, under the planning
+        self.resident = resident = bool(getattr(src, "resident", False))
+        W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
+        self.wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
+        self.oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in self.wedges]
+        self.src = src
+        self.feeder = src.feeder(self.wedges, self.oks) if (hasattr(src, "feeder") and not resident) else None
+        self.device, self.model, self.verbose, self.log = device, model, verbose, log
+        self.learn_profiles, self.adaptive, self.moments_only = learn_profiles, adaptive, moments_only
+        self.plan = p = plan if plan is not None else plan_integration(
+            exp_blocks, block_edges, model, dmin, dmax, (f_first, f_last), minimum_zeta, n_regions_xy, adaptive,
+            deconvolve_overlaps, lattice_of, foreign_spots, n_foreign, allowed)
+        # device memory: blocks split into parts of consecutive phi when their open buffers exceed the budget
+        wedge_bytes = 0 if resident else 3 * W * src.ny * src.nx * 4
+        limit = mem_budget if mem_budget is not None else memplan.budget(device)
+        self.plan, exp_blocks, self.mem = memplan.fit(p, exp_blocks, f_last, wedge_bytes, limit)
+        p = self.plan
+        self.exp_blocks = exp_blocks
+        self.refl = p.refl
+        n = p.n
+        if verbose and self.mem["parts"] > 1:
+            log(f"  INTEGRATE: open shoebox buffers ~{self.mem['one'] / 2 ** 30:.1f} GB > the device budget "
+                f"{limit / 2 ** 30:.1f} GB: each phi block in {self.mem['parts']} parts, peak "
+                f"~{self.mem['peak'] / 2 ** 30:.1f} GB")
+        if verbose:
+            log(f"  INTEGRATE: {p.info['n_predicted']} predicted reflections, box {p.box}x{p.box} px, sigma_D "
+                f"{model.sigma_d:.4f} sigma_M {model.sigma_m:.4f} deg; {p.info['n_wide']} wide in phi (> {MAX_DZ} "
+                f"frames): integrated in bins, {p.info['n_trunc']} of them still truncated")
+        self.out = out = {k: np.empty(n, np.float64) for k in OUT_F64}     # every processed block fills its rows
+        out["n_over"] = np.zeros(n, np.int32)
+        out["n_fg_masked"] = np.zeros(n, np.int32)
+        out["isum_raw"] = np.full(n, -1, np.int64)                 # -1: not integrated (rows of no processed block)
+        self.fz_out = np.zeros((n, MAX_DZ), np.float32) if not learn_profiles else None
+        self.nreg = p.nreg
+        self.sd = np.radians(model.sigma_d)
+        self.sm = np.radians(model.sigma_m)
+        self.state = dict(sd=self.sd, sm=self.sm, rcw=A.rc_default_weights())
+        self.block_params, self.prof_by_block, self.block_widths = {}, {}, {}
+        self.t_dev = 0.0
+        nblocks = len(exp_blocks)
+        self.read_fi = read_fi = np.array([f - 1 for f in range(f_first, f_last + 1) if f not in excl], np.int64)
+        # a block takes every frame read up to the first frame read at or after its last needed frame
+        # (`xpg/integrate.py:789-793`: completion is checked after the frame's gather)
+        self.eff_hi = {}
+        for b in range(nblocks):
+            if p.blocks_refl[b].size:
+                k = np.searchsorted(read_fi, p.need_hi[b], "left")
+                self.eff_hi[b] = int(read_fi[min(k, len(read_fi) - 1)]) if len(read_fi) else -1
+        self.pending = sorted((b for b in range(nblocks) if p.blocks_refl[b].size), key=lambda b: p.need_lo[b])
+        self.opened, self.open_order = {}, []
+        self.det_cache = {}
+        self.bkg_template = bkg_template
+        self.mask_t = None
+        if mask is not None and not np.asarray(mask).all():
+            self.mask_t = D.h2d(np.asarray(mask, np.uint8), None, device)
+        self.processed = []
+        self.live = {}                    # completed blocks between pass1_stage and collect
+        # when frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1
+        # as soon as their wedge is in: it overlaps the transfer of the later wedges (their widths are fixed: every
+        # block before it has been processed). Resident frames have no transfer to hide: their blocks run pass 1
+        # whole, in the fewest launches.
+        ok_parts = [ok.astype(np.uint8) for ok in self.oks if not ok.all()]
+        self.ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
+        self.ok_off = 0
+        self.early_rows = EARLY_PASS1_ROWS if (early_pass1 and not resident) else 0
 
-    def widths():
-        sd_b = state["sd"] if adaptive else sd
-        sm_b, rcw_b = (state["sm"], state["rcw"]) if adaptive else (sm, A.rc_default_weights())
+    # ---- device constants
+    def detector(self, g):
+        key = (id(g), id(self.bkg_template))
+        if key not in self.det_cache:
+            self.det_cache.clear()
+            self.det_cache[key] = D.DeviceDetector(g, self.bkg_template, self.device)
+        return self.det_cache[key]
+
+    def widths(self):
+        st = self.state
+        sd_b = st["sd"] if self.adaptive else self.sd
+        sm_b, rcw_b = (st["sm"], st["rcw"]) if self.adaptive else (self.sm, A.rc_default_weights())
         return sd_b, sm_b, rcw_b
 
-    def block_pass1_consts(b, blk: _Block):
+    def block_pass1_consts(self, b, blk: _Block):
         """The block's pass-1 constants from the current widths (those adapted by every block processed before it),
         made once; allocated with the buffers before any frame transfer of the block is queued."""
         if blk.p1 is None:
-            sd_b, sm_b, rcw_b = widths()
-            blk.c1 = (sd_b, sm_b, rcw_b) + D.block_consts(exp_blocks[b].geom, sd_b, sm_b, model.gain, rcw_b, device)
+            sd_b, sm_b, rcw_b = self.widths()
+            blk.c1 = (sd_b, sm_b, rcw_b) + D.block_consts(self.exp_blocks[b].geom, sd_b, sm_b, self.model.gain,
+                                                          rcw_b, self.device)
             blk.p1 = D.Pass1Buffers(blk.rowset)
 
-    def pass1_rows(b, blk: _Block, idx, groups=None, binned_t=None):
+    def pass1_rows(self, b, blk: _Block, idx, groups=None, binned_t=None):
         """Bin decode and pass 1 of the block's local rows idx, whose frames have all been gathered (launch groups
         and binned rows on the device when given, else made here)."""
-        block_pass1_consts(b, blk)
-        if binned_t is None:
-            binned = idx[blk.grows.binned[idx]]
-            binned_t = D.h2d(binned.astype(np.int32), None, device) if binned.size else None
-        if binned_t is not None:
-            D.decode_bins(blk.grows, blk.arena, blk.cnt, order=binned_t)
+        self.decode_rows(b, blk, idx, binned_t)
         if groups is None and idx.size != blk.rowset.n:
             groups = D.subset_groups(blk.rowset, idx)
-        D.pass1(detector(exp_blocks[b].geom), blk.rowset, blk.c1[3], blk.arena, blk.p1, groups=groups)
+        D.pass1(self.detector(self.exp_blocks[b].geom), blk.rowset, blk.c1[3], blk.arena, blk.p1, groups=groups)
         blk.p1_done[idx] = True
 
-    processed = []
+    def decode_rows(self, b, blk: _Block, idx, binned_t=None):
+        self.block_pass1_consts(b, blk)
+        if binned_t is None:
+            binned = idx[blk.grows.binned[idx]]
+            binned_t = D.h2d(binned.astype(np.int32), None, self.device) if binned.size else None
+        if binned_t is not None:
+            D.decode_bins(blk.grows, blk.arena, blk.cnt, order=binned_t)
 
-    def process(b, blk: _Block):
-        nonlocal t_dev
-        tg = time.time()
-        processed.append(b)
-        g = exp_blocks[b].geom
-        det = detector(g)
-        rs = blk.rowset
-        rem = np.flatnonzero(~blk.p1_done)
-        if rem.size:
-            pass1_rows(b, blk, rem)
-        sd_b, sm_b, rcw_b = blk.c1[:3]
-        widths_p1 = (float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy())
-        p1 = blk.p1
-        num = torch.zeros((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float64, device=device)
-        den = torch.zeros_like(num)
-        if learn_profiles:
-            D.accumulate(rs, p1, nreg, num, den)
-        h1 = _host_rows(p1.t, ADAPT_KEYS)
-        rows = blk.rows
-        if adaptive:
-            st = _adapt_rows(h1, plan, rows)
-            strong = None
-            if st.any():
-                rst = rows[st]
-                strong = dict(F=_fz_rows(p1, rs, np.flatnonzero(st)), phi=refl["phi"][rst], zeta_k=refl["zeta_k"][rst],
-                              iz0=plan.iz0[rst], m_d=h1["m_d"][st], x=refl["x"][rst], y=refl["y"][rst])
-            sm_b, rcw_b, sd_next, params = A.adapt_block(g, strong, sd, sm, sd_b, sm_b, rcw_b)
-            if sd_next is not None:
-                state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
-            block_params[b] = params
-        prof = torch.empty((nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
-        D.finalize_profiles(num, den, prof)
-        block_widths[b] = dict(pass1=widths_p1,
-                               pass2=(float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy()))
-        cols = {k: p1.t[k] for k in P1_OUT}
-        if not moments_only:
-            c2, k2 = D.block_consts(g, sd_b, sm_b, model.gain, rcw_b, device)
-            p2 = D.Pass2Buffers(rs)
-            D.pass2(det, rs, c2, blk.arena, prof, p1, p2)
-            cols.update({k: p2.t[k] for k in P2_OUT})
-        D.status()
-        prof_by_block[b] = prof.cpu().numpy()
-        h = _host_rows(cols, tuple(cols), blk.perm_t)     # in plan (global row) order
-        dst = slice(*blk.span) if blk.span is not None else blk.rows_sorted
-        for k, v in h.items():
-            out[k][dst] = v
-        if fz_out is not None:
-            fz_out[rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
-        t_dev += time.time() - tg
-
-    def next_block(extra=None):
+    def next_block(self, extra=None):
         """The unprocessed block that completes first (the order blocks are processed in); `extra`: a block being
         opened (after the open ones)."""
-        cand = [(eff_hi[b], 0, open_order.index(b), b) for b in opened]
+        eff, oo = self.eff_hi, self.open_order
+        cand = [(eff[b], 0, oo.index(b), b) for b in self.opened]
         if extra is not None:
-            cand.append((eff_hi[extra], 0, len(open_order), extra))
-        cand += [(eff_hi[b], 1, k, b) for k, b in enumerate(pending)]
+            cand.append((eff[extra], 0, len(oo), extra))
+        cand += [(eff[b], 1, k, b) for k, b in enumerate(self.pending)]
         return min(cand)[3] if cand else None
 
-    # ---- frame loop: wedges of consecutive frame numbers --------------------------------------------------------
-    # When frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1 at
-    # once: it overlaps the transfer of the later wedges (their widths are fixed: every block before it has been
-    # processed). Resident frames have no transfer to hide: their blocks run pass 1 whole, in the fewest launches.
-    ok_parts = [ok.astype(np.uint8) for ok in oks if not ok.all()]
-    ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
-    early_rows = 0 if resident else EARLY_PASS1_ROWS
-    ok_off = 0
-    for w, (f, f_b) in enumerate(wedges):
+    # ---- the frame loop: wedges of consecutive frame numbers
+    def feed(self, w):
+        """Gathers wedge w into every open block (opening the blocks it reaches first); returns the blocks it
+        completed, in processing order (each to be processed before the next block's pass 1)."""
+        p = self.plan
+        f, f_b = self.wedges[w]
         fi_a, fi_b = f - 1, f_b - 1
-        while pending and plan.need_lo[pending[0]] <= fi_b:
-            b = pending.pop(0)
-            blk = _Block(b, blocks_rows[b], plan, device)
-            blk.schedule(wedges, eff_hi[b], early_rows, device)
-            if early_rows and next_block(extra=b) == b:
-                block_pass1_consts(b, blk)
-            opened[b] = blk
-            open_order.append(b)
-        ok = oks[w]
+        while self.pending and p.need_lo[self.pending[0]] <= fi_b:
+            b = self.pending.pop(0)
+            blk = _Block(b, p.blocks_refl[b], p, self.device)
+            blk.schedule(self.wedges, self.eff_hi[b], self.early_rows, self.device)
+            if self.early_rows and self.next_block(extra=b) == b:
+                self.block_pass1_consts(b, blk)
+            self.opened[b] = blk
+            self.open_order.append(b)
+        ok = self.oks[w]
         ok_t = None
         if not ok.all():
-            ok_t = ok_dev[ok_off:ok_off + ok.size]
-            ok_off += ok.size
-        if ok.any() and opened:
-            data, is_f = (feeder.get(w), False) if feeder is not None else src.wedge(f, f_b, ok)
-            for b in open_order:
-                blk = opened.get(b)
+            ok_t = self.ok_dev[self.ok_off:self.ok_off + ok.size]
+            self.ok_off += ok.size
+        src = self.src
+        if ok.any() and self.opened:
+            data, is_f = (self.feeder.get(w), False) if self.feeder is not None else src.wedge(f, f_b, ok)
+            for b in self.open_order:
+                blk = self.opened.get(b)
                 if blk is None or w not in blk.w_gather:
                     continue
-                nf = min(fi_b, eff_hi[b]) - fi_a + 1
+                nf = min(fi_b, self.eff_hi[b]) - fi_a + 1
                 fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
-                                     mask_t, ok_t[:nf] if ok_t is not None else None)
+                                     self.mask_t, ok_t[:nf] if ok_t is not None else None)
                 D.gather(fs, blk.grows, blk.sched(blk.w_gather[w]), blk.arena, blk.cnt)
-        if feeder is not None:
-            feeder.done_with(w)
-        done = sorted((b for b in open_order if b in opened and eff_hi[b] <= fi_b),
-                      key=lambda b: (eff_hi[b], open_order.index(b)))
-        for b in done:
-            process(b, opened.pop(b))
-        nxt = next_block()
-        if nxt is not None and nxt in opened and w in opened[nxt].w_early:
-            blk = opened[nxt]
+        if self.feeder is not None:
+            self.feeder.done_with(w)
+        return sorted((b for b in self.open_order if b in self.opened and self.eff_hi[b] <= fi_b),
+                      key=lambda b: (self.eff_hi[b], self.open_order.index(b)))
+
+    def remaining(self):
+        """The open blocks left after the last wedge, in processing order."""
+        return [b for b in self.open_order if b in self.opened]
+
+    def early_pass1(self, w):
+        """Pass 1 of the next block's rows whose last frame arrived with wedge w (uploaded frames only; after the
+        blocks wedge w completed are processed)."""
+        nxt = self.next_block()
+        if nxt is not None and nxt in self.opened and w in self.opened[nxt].w_early:
+            blk = self.opened[nxt]
             idx, groups, bin_on = blk.w_early[w]
             idx = idx[~blk.p1_done[idx]]
             if idx.size == blk.w_early[w][0].size:          # none of them done yet: the precomputed launches apply
-                pass1_rows(nxt, blk, idx, [(bx, dz, blk.sched(o)) for bx, dz, o in groups],
-                           blk.sched(bin_on) if bin_on is not None else None)
-    for b in open_order:
-        if b in opened:
-            process(b, opened.pop(b))
+                self.pass1_rows(nxt, blk, idx, [(bx, dz, blk.sched(o)) for bx, dz, o in groups],
+                                blk.sched(bin_on) if bin_on is not None else None)
 
-    unfilled = np.ones(n, bool)                       # rows of blocks never processed: NaN, as XPG leaves them
-    for b in processed:
-        unfilled[plan.blocks_refl[b]] = False
-    for k in OUT_F64:
-        if moments_only and k not in P1_OUT:         # pass 2 did not run
-            out[k][:] = np.nan
-        else:
-            out[k][unfilled] = np.nan
-    refl.update(out)
-    refl["overlap"] = plan.overlap
-    if fz_out is not None:
-        refl["fz"] = fz_out
-    refl["iz0"], refl["dz"], refl["fb"] = plan.iz0, plan.dz, plan.fb
-    refl["region"] = plan.region
-    refl["ix0"], refl["iy0"] = plan.ix0 * plan.pxs, plan.iy0 * plan.pxs
-    if (plan.pxs > 1).any():
-        refl["pxs"] = plan.pxs
-    if verbose:
-        okk = np.isfinite(refl["iprf"])
-        log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - t0:.1f}s (device {t_dev:.1f}s)")
-    res = IntegrationResult(refl, model, prof_by_block, dict(total=time.time() - t0, gpu=t_dev))
-    res.block_params = block_params
-    res.block_widths = block_widths      # (sigma_D, sigma_M in radians, rocking-curve weights) of each block's passes
-    return res
+    # ---- a completed block
+    def process(self, b):
+        self.pass1_stage(b)
+        self.learn(b)
+        self.pass2_stage(b)
+        self.collect(b)
+
+    def pass1_stage(self, b, batched=False):
+        """Bin decode and pass 1 of the block's rows not done yet; batched: no launch, returns (set entry, local rows)
+        for a batched launch (the caller launches, then calls learn)."""
+        blk = self.opened.pop(b)
+        self.live[b] = blk
+        self.tg = time.time()
+        self.processed.append(b)
+        rem = np.flatnonzero(~blk.p1_done)
+        if not batched:
+            if rem.size:
+                self.pass1_rows(b, blk, rem)
+            return None
+        self.decode_rows(b, blk, rem)
+        blk.p1_done[rem] = True
+        det = self.detector(self.exp_blocks[b].geom)
+        return D.rowset_entry(det, blk.rowset, blk.c1[3], blk.arena, blk.p1), rem
+
+    def learn(self, b):
+        """Profiles and widths of a block whose pass 1 is complete: accumulation, the host adaptation (sigma_M,
+        rocking-curve weights for this block's pass 2, sigma_D for the next block), finalisation."""
+        blk = self.live[b]
+        p, rs, device = self.plan, blk.rowset, self.device
+        g = self.exp_blocks[b].geom
+        sd_b, sm_b, rcw_b = blk.c1[:3]
+        widths_p1 = (float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy())
+        p1 = blk.p1
+        num = torch.zeros((self.nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float64, device=device)
+        den = torch.zeros_like(num)
+        if self.learn_profiles:
+            D.accumulate(rs, p1, self.nreg, num, den)
+        h1 = _host_rows(p1.t, ADAPT_KEYS)
+        rows = blk.rows
+        if self.adaptive:
+            st = _adapt_rows(h1, p, rows)
+            strong = None
+            if st.any():
+                rst = rows[st]
+                strong = dict(F=_fz_rows(p1, rs, np.flatnonzero(st)), phi=self.refl["phi"][rst],
+                              zeta_k=self.refl["zeta_k"][rst], iz0=p.iz0[rst], m_d=h1["m_d"][st],
+                              x=self.refl["x"][rst], y=self.refl["y"][rst])
+            sm_b, rcw_b, sd_next, params = A.adapt_block(g, strong, self.sd, self.sm, sd_b, sm_b, rcw_b)
+            if sd_next is not None:
+                self.state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
+            self.block_params[b] = params
+        blk.prof = torch.empty((self.nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
+        D.finalize_profiles(num, den, blk.prof)
+        self.block_widths[b] = dict(pass1=widths_p1,
+                                    pass2=(float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy()))
+        blk.c2 = D.block_consts(g, sd_b, sm_b, self.model.gain, rcw_b, device)
+        blk.p2 = None if self.moments_only else D.Pass2Buffers(rs)
+
+    def pass2_stage(self, b, batched=False):
+        """Pass 2 of the block (none for moments-only runs); batched: its set entry for a batched launch."""
+        blk = self.live[b]
+        if self.moments_only:
+            return None
+        det = self.detector(self.exp_blocks[b].geom)
+        if batched:
+            return D.rowset_entry(det, blk.rowset, blk.c2[0], blk.arena, blk.p1, blk.prof, blk.p2)
+        D.pass2(det, blk.rowset, blk.c2[0], blk.arena, blk.prof, blk.p1, blk.p2)
+        return None
+
+    def collect(self, b):
+        """The block's results to the host, into the run's output columns."""
+        blk = self.live.pop(b)
+        p1, rs = blk.p1, blk.rowset
+        cols = {k: p1.t[k] for k in P1_OUT}
+        if blk.p2 is not None:
+            cols.update({k: blk.p2.t[k] for k in P2_OUT})
+        D.status()
+        self.prof_by_block[b] = blk.prof.cpu().numpy()
+        h = _host_rows(cols, tuple(cols), blk.perm_t)     # in plan (global row) order
+        dst = slice(*blk.span) if blk.span is not None else blk.rows_sorted
+        for k, v in h.items():
+            self.out[k][dst] = v
+        if self.fz_out is not None:
+            self.fz_out[blk.rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
+        self.t_dev += time.time() - self.tg
+
+    def result(self):
+        p, out, refl = self.plan, self.out, self.refl
+        unfilled = np.ones(p.n, bool)                     # rows of blocks never processed: NaN, as XPG leaves them
+        for b in self.processed:
+            unfilled[p.blocks_refl[b]] = False
+        for k in OUT_F64:
+            if self.moments_only and k not in P1_OUT:     # pass 2 did not run
+                out[k][:] = np.nan
+            else:
+                out[k][unfilled] = np.nan
+        refl.update(out)
+        refl["overlap"] = p.overlap
+        if self.fz_out is not None:
+            refl["fz"] = self.fz_out
+        refl["iz0"], refl["dz"], refl["fb"] = p.iz0, p.dz, p.fb
+        refl["region"] = p.region
+        refl["ix0"], refl["iy0"] = p.ix0 * p.pxs, p.iy0 * p.pxs
+        if (p.pxs > 1).any():
+            refl["pxs"] = p.pxs
+        if self.verbose:
+            okk = np.isfinite(refl["iprf"])
+            self.log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - self.t0:.1f}s "
+                     f"(device {self.t_dev:.1f}s)")
+        res = IntegrationResult(refl, self.model, self.prof_by_block, dict(total=time.time() - self.t0,
+                                                                           gpu=self.t_dev))
+        res.block_params = self.block_params
+        res.block_widths = self.block_widths  # (sigma_D, sigma_M in radians, rocking-curve weights) of each pass
+        return res
+
+    def close(self):
+        if self.feeder is not None:
+            self.feeder.close()
+            self.feeder = None
 
 
 ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")

@@ -67,7 +67,7 @@ class XiFrames(C.Structure):
 
 
 class XiSynthSpots(C.Structure):
-    _fields_ = [("n", C.c_int), ("x", _fp), ("y", _fp), ("z", _fp), ("counts", _fp), ("sig_t", _fp),
+    _fields_ = [("n", C.c_int), ("index", _fp), ("x", _fp), ("y", _fp), ("z", _fp), ("counts", _fp), ("sig_t", _fp),
                 ("sig_r", _fp), ("sig_z", _fp), ("orgx", C.c_double), ("orgy", C.c_double)]
 
 
@@ -138,6 +138,11 @@ class XiSpotParams(C.Structure):
 XI_SPOT_MAX_HALF = 8
 
 
+class XiRowSet(C.Structure):
+    _fields_ = [("det", XiDetector), ("rows", XiRows), ("blk", XiBlock), ("arena", _fp), ("p1", XiPass1Out),
+                ("prof", _fp), ("p2", XiPass2Out)]
+
+
 class XiHklRows(C.Structure):
     _fields_ = [("n", C.c_int64), ("hkl", C.c_void_p), ("I", C.c_void_p), ("sig", C.c_void_p), ("x", C.c_void_p),
                 ("y", C.c_void_p), ("zc", C.c_void_p), ("rlp", C.c_void_p), ("peak", C.c_void_p),
@@ -152,7 +157,8 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "
            "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
            "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
-           "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong", "xi_spot_workspace")
+           "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong", "xi_spot_workspace", "xi_pass1_batched",
+           "xi_pass2_batched")
 
 _LIB = None
 
@@ -210,6 +216,9 @@ def load(path=None):
     lib.xi_finalize_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.xi_pass2.argtypes = [C.POINTER(XiDetector), C.POINTER(XiRows), C.POINTER(XiBlock), C.c_void_p, C.c_void_p,
                              C.POINTER(XiPass2In), C.POINTER(XiPass2Out), C.c_void_p]
+    for name in ("xi_pass1_batched", "xi_pass2_batched"):
+        getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_void_p]
     lib.xi_synth_frames.restype = C.c_int
     lib.xi_synth_frames.argtypes = [C.POINTER(XiSynthSpots), C.POINTER(XiSynthBackground), C.c_int, C.c_int,
                                     C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p]

@@ -133,6 +133,47 @@ def config3(**kw) -> SweepSpec:
     return config1(name="config3", weak_fraction=0.05, dead_fraction=0.02, seed=3, **kw)
 
 
+CONFIG4_DETECTORS = ((1030, 1065), (2068, 2162), (4148, 4362))
+CONFIG4_CELLS = (((60.0, 85.0, 120.0, 90.0, 90.0, 90.0), "P 21 21 21"),
+                 ((150.0, 60.0, 90.0, 90.0, 105.0, 90.0), "C 1 2 1"),
+                 ((100.0, 100.0, 200.0, 90.0, 90.0, 120.0), "P 65 2 2"))
+
+
+def config4(seed=4, n_sweeps=12, **kw):
+    """Batched workload: n_sweeps sweeps with frames drawn log-uniform in 50..3600, a detector from
+    CONFIG4_DETECTORS (75 um pixels at 120 mm, lambda 0.98 A), a cell from CONFIG4_CELLS, sigma_M uniform in
+    0.05..0.5 deg; phi blocks of 360 frames, background 0.2, Wilson B 25. Seeded: the same list every call."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_sweeps):
+        nf = int(round(np.exp(rng.uniform(np.log(50.0), np.log(3600.0)))))
+        nx, ny = CONFIG4_DETECTORS[int(rng.integers(len(CONFIG4_DETECTORS)))]
+        cell, sg = CONFIG4_CELLS[int(rng.integers(len(CONFIG4_CELLS)))]
+        sm = float(rng.uniform(0.05, 0.5))
+        base = dict(name=f"config4-{k}", nx=nx, ny=ny, qx=0.075, distance=120.0, wavelength=0.98, osc=0.1,
+                    nframes=nf, cell=cell, space_group=sg, sigma_d=0.03, sigma_m=sm, wilson_b=25.0, mean_i0=50.0,
+                    background=0.2, ramp=0.5, seed=100 + 17 * seed + k, n_regions_xy=5 if nx > 2000 else 3,
+                    block_frames=360)
+        base.update(kw)
+        out.append(SweepSpec(**base))
+    return out
+
+
+def config5(seed=5, n_sweeps=4, nframes=3600, **kw):
+    """Served workload: n_sweeps concurrent sweeps of config 2's geometry (4148 x 4362 px, 75 um at 120 mm, lambda
+    0.98 A, 0.1 deg frames, sigma_M 0.15 deg, background 0.2), cells from CONFIG4_CELLS, 50-frame wedges."""
+    out = []
+    for k in range(n_sweeps):
+        cell, sg = CONFIG4_CELLS[k % len(CONFIG4_CELLS)]
+        base = dict(name=f"config5-{k}", nx=4148, ny=4362, qx=0.075, distance=120.0, wavelength=0.98, osc=0.1,
+                    nframes=nframes, cell=cell, space_group=sg, sigma_d=0.03, sigma_m=0.15, wilson_b=25.0,
+                    mean_i0=50.0, background=0.2, ramp=0.5, seed=200 + 17 * seed + k, n_regions_xy=5,
+                    block_frames=360)
+        base.update(kw)
+        out.append(SweepSpec(**base))
+    return out
+
+
 def _hash_unit(keys, salt):
     """Deterministic uniforms in (0, 1) from int64 keys (splitmix64 finaliser)."""
     with np.errstate(over="ignore"):
@@ -264,6 +305,55 @@ def render_frames(spec: SweepSpec, frames=None, table=None):
     return out
 
 
+def render_window(spec: SweepSpec, table, frames, y0, y1, x0, x1):
+    """uint32 counts (len(frames), y1 - y0, x1 - x0) of a detector window [y0, y1) x [x0, x1) (array indices) over the
+    given frames (1-based): the same model as `render_frames` (background with its ramp, the spots reaching the
+    window, Poisson noise seeded by (seed, frame, window origin), module gaps flagged) without rendering whole
+    frames. Dead rectangles are not applied."""
+    g = spec.geometry()
+    ys, xs = np.mgrid[y0:y1, x0:x1]
+    cx = np.array([1.0, spec.nx, 1.0, spec.nx])
+    cy = np.array([1.0, 1.0, spec.ny, spec.ny])
+    rmax = max(np.hypot(cx - g.orgx, cy - g.orgy).max(), 1.0)
+    bg = spec.background * (1.0 + spec.ramp * np.hypot(xs + PIX0 - g.orgx, ys + PIX0 - g.orgy) / rmax)
+    near = np.flatnonzero((table["x"] > x0 - 62) & (table["x"] < x1 + 62) & (table["y"] > y0 - 62) &
+                          (table["y"] < y1 + 62))
+    sub = {k: np.asarray(v)[near] for k, v in table.items() if np.ndim(v) >= 1 and len(v) == len(table["x"])}
+    gaps = spec.gap_mask()[y0:y1, x0:x1] if spec.gaps else np.zeros((y1 - y0, x1 - x0), bool)
+    out = np.empty((len(frames), y1 - y0, x1 - x0), np.uint32)
+    sub_off = (np.arange(2) + 0.5) / 2 - 0.5
+    for i, f in enumerate(frames):
+        lam = bg.copy()
+        z0, z1 = f - 1.0, float(f)
+        zc, sz = sub["z"], sub["sig_z"]
+        for r in np.flatnonzero((zc + 5 * sz > z0) & (zc - 5 * sz < z1)):
+            fz = 0.5 * (erf((z1 - zc[r]) / (np.sqrt(2) * sz[r])) - erf((z0 - zc[r]) / (np.sqrt(2) * sz[r])))
+            x, y, st, sr = sub["x"][r], sub["y"][r], sub["sig_t"][r], sub["sig_r"][r]
+            rd = np.array([x - g.orgx, y - g.orgy])
+            rn = np.linalg.norm(rd)
+            rd = rd / rn if rn > 1e-6 else np.array([1.0, 0.0])
+            half = int(np.clip(np.ceil(4.5 * sr), 4, 60))
+            ix, iy = int(np.floor(x - PIX0 + 0.5)), int(np.floor(y - PIX0 + 0.5))
+            px = np.arange(max(ix - half, x0), min(ix + half + 1, x1))
+            py = np.arange(max(iy - half, y0), min(iy + half + 1, y1))
+            if not px.size or not py.size:
+                continue
+            dens = 0.0
+            for oy in sub_off:
+                for ox in sub_off:
+                    dx = (px + PIX0 + ox - x)[None, :]
+                    dy = (py + PIX0 + oy - y)[:, None]
+                    ur, ut = dx * rd[0] + dy * rd[1], -dx * rd[1] + dy * rd[0]
+                    dens = dens + np.exp(-0.5 * ((ur / sr) ** 2 + (ut / st) ** 2))
+            lam[py[0] - y0:py[-1] + 1 - y0, px[0] - x0:px[-1] + 1 - x0] += \
+                sub["counts"][r] * fz * dens / 4.0 / (2 * np.pi * sr * st)
+        c = np.random.default_rng([spec.seed, int(f), int(y0), int(x0)]).poisson(lam)
+        c = np.minimum(c, 0xFFFFFFFE).astype(np.uint32)
+        c[gaps] = GAP_VALUE
+        out[i] = c
+    return out
+
+
 def encode_frame(raw, overload, min_valid=0, mask=None):
     """The float32 frame XPG's image readers hand to integration (`xpg/io/images.py:72-102`, Eiger
     `:408-419`): counts as float32, overloaded (raw >= overload) -2, flagged (raw == 0xFFFFFFFF) or below
@@ -287,34 +377,79 @@ def replace_spec(spec, **kw):
     return replace(spec, **kw)
 
 
-def device_frames(spec: SweepSpec, table, first_frame, n_frames, out=None, device="cuda", stream=None):
+class DeviceSpots:
+    """A sweep's spot table on the device for the frame generator, with per-bucket lists of the spots that reach
+    each run of BUCKET frames (|z - zc| < 5 sigma_z), so that a wedge's spots are found without a scan of the
+    table. The noise of a spot's pixels is keyed by the spot's index in the table and the frame: any partition of the
+    frames into wedges renders the same frames."""
+
+    BUCKET = 8
+
+    def __init__(self, spec: SweepSpec, table, device="cuda"):
+        import torch
+        self.spec = spec
+        g = spec.geometry()
+        self.t = {k: torch.as_tensor(np.ascontiguousarray(table[k], np.float64)).to(device)
+                  for k in ("x", "y", "z", "counts", "sig_t", "sig_r", "sig_z")}
+        z, sz = np.asarray(table["z"], float), np.asarray(table["sig_z"], float)
+        lo = np.floor((z - 5 * sz) / self.BUCKET).astype(np.int64)      # frame index f covers z in [f, f + 1)
+        hi = np.floor((z + 5 * sz) / self.BUCKET).astype(np.int64)
+        n_b = int(np.ceil((spec.nframes + 1) / self.BUCKET)) + 1
+        lo, hi = np.clip(lo, 0, n_b - 1), np.clip(hi, 0, n_b - 1)
+        cnt = hi - lo + 1
+        idx = np.repeat(np.arange(z.size, dtype=np.int64), cnt)
+        bk = np.repeat(lo, cnt) + (np.arange(idx.size) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+        o = np.argsort(bk, kind="stable")
+        self.idx = idx[o].astype(np.int32)
+        self.start = np.searchsorted(bk[o], np.arange(n_b + 1))
+        self.device = device
+        self.bg = (spec.background, spec.ramp, float(g.orgx), float(g.orgy),
+                   float(max(np.hypot(np.array([1.0, spec.nx, 1.0, spec.nx]) - g.orgx,
+                                      np.array([1.0, 1.0, spec.ny, spec.ny]) - g.orgy).max(), 1.0)))
+        self.org = (float(g.orgx), float(g.orgy))
+
+    def spots_for(self, first_frame, n_frames):
+        """Indices of the spots that reach frames first_frame..first_frame + n_frames - 1 (1-based)."""
+        b0 = max((first_frame - 1) // self.BUCKET, 0)
+        b1 = min((first_frame - 1 + n_frames - 1) // self.BUCKET, len(self.start) - 2)
+        if b1 < b0:
+            return np.zeros(0, np.int32)
+        return np.unique(self.idx[self.start[b0]:self.start[b1 + 1]])
+
+    def render(self, first_frame, n_frames, out, stream=None):
+        """Frames first_frame .. first_frame + n_frames - 1 into the device int32 tensor out (n_frames, ny, nx)."""
+        import ctypes as C
+
+        from . import native as N
+        from .device import h2d
+        spec = self.spec
+        idx = self.spots_for(first_frame, n_frames)
+        it = h2d(idx, None, self.device) if idx.size else None
+        sp = N.XiSynthSpots()
+        sp.n = int(idx.size)
+        sp.index = N.ptr(it)
+        for k, v in self.t.items():
+            setattr(sp, k, N.ptr(v))
+        sp.orgx, sp.orgy = self.org
+        bg = N.XiSynthBackground()
+        bg.level, bg.ramp, bg.orgx, bg.orgy, bg.rmax = self.bg
+        rc = N.load().xi_synth_frames(C.byref(sp), C.byref(bg), int(first_frame), int(n_frames), spec.ny, spec.nx,
+                                      int(spec.seed), 1 if spec.gaps else 0, N.ptr(out), N.stream_handle(stream))
+        if rc != 0:
+            raise RuntimeError("xi_synth_frames: " + N.load().xi_synth_last_error().decode())
+        return out
+
+
+def device_frames(spec: SweepSpec, table, first_frame, n_frames, out=None, device="cuda", stream=None, spots=None):
     """Frames first_frame .. first_frame + n_frames - 1 rendered on the device (int32 view of uint32 counts),
     shape (n_frames, ny, nx). Same model as `render_frames`, with a device counter-based Poisson draw (so the pixel
-    values differ from the host generator's)."""
-    import ctypes as C
-
+    values differ from the host generator's). `spots`: a DeviceSpots of the table (made here when not given)."""
     import torch
 
     from . import native as N
     N.require_cuda()
     if out is None:
         out = torch.empty((n_frames, spec.ny, spec.nx), dtype=torch.int32, device=device)
-    g = spec.geometry()
-    keep = (table["z"] + 5 * table["sig_z"] > first_frame - 1) & (table["z"] - 5 * table["sig_z"] < first_frame - 1 + n_frames)
-    t = {k: torch.as_tensor(np.ascontiguousarray(table[k][keep], np.float64)).to(device)
-         for k in ("x", "y", "z", "counts", "sig_t", "sig_r", "sig_z")}
-    sp = N.XiSynthSpots()
-    sp.n = int(keep.sum())
-    for k, v in t.items():
-        setattr(sp, k, N.ptr(v))
-    sp.orgx, sp.orgy = float(g.orgx), float(g.orgy)
-    bg = N.XiSynthBackground()
-    bg.level, bg.ramp, bg.orgx, bg.orgy = spec.background, spec.ramp, float(g.orgx), float(g.orgy)
-    cx = np.array([1.0, spec.nx, 1.0, spec.nx])
-    cy = np.array([1.0, 1.0, spec.ny, spec.ny])
-    bg.rmax = float(max(np.hypot(cx - g.orgx, cy - g.orgy).max(), 1.0))
-    rc = N.load().xi_synth_frames(C.byref(sp), C.byref(bg), int(first_frame), int(n_frames), spec.ny, spec.nx,
-                                  int(spec.seed), 1 if spec.gaps else 0, N.ptr(out), N.stream_handle(stream))
-    if rc != 0:
-        raise RuntimeError("xi_synth_frames: " + N.load().xi_synth_last_error().decode())
-    return out
+    if spots is None:
+        spots = DeviceSpots(spec, table, device)
+    return spots.render(first_frame, n_frames, out, stream)
