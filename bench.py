@@ -297,8 +297,8 @@ def _parity(wl, res, n_min=500):
     widths; worst error per key relative to max(|value|, scale) (tests/tolerance.py), and the rows outside tolerance
     per key (integers: rows that differ)."""
     from oracle.blockcheck import check_rows, stratified_rows
-    p, s = wl.plan, wl.spec
-    nb = len(wl.edges) - 1
+    p, s = getattr(res, "plan", wl.plan), wl.spec          # the plan integrated (blocks in parts if memory was short)
+    nb = len(p.blocks_refl)
     blocks = sorted({0, nb // 2})
     t0 = time.perf_counter()
     worst, bad, rows_n, fitted = {}, {}, 0, 0
@@ -514,6 +514,9 @@ def run(args):
                 "voxels_per_s": round(float((wl.plan.Dz * wl.plan.bx.astype(np.float64) ** 2).sum()) * args.steps
                                       * world / t_max, 1),
                 "integrated_per_step": n_ok // max(args.steps, 1),
+                "memory": {"block_parts": int(res_timed.memory["parts"]),
+                           "open_buffers_gb": round(res_timed.memory["peak"] / 1e9, 1),
+                           "budget_gb": round(res_timed.memory["budget"] / 1e9, 1)},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "parity": parity}
         print(json.dumps(line), flush=True)
@@ -607,6 +610,119 @@ def reference_arm(args):
                                        f"frames over {cores} cores)"},
             "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "native_library_mapped": _native_mapped()}
+    print(json.dumps(line), flush=True)
+
+
+def _jobs_of(specs, wedge_frames, device="cuda"):
+    """Batch jobs of synthetic sweeps whose frames are rendered on the device as the integration asks for them."""
+    from xpg_b200 import synth
+    from xpg_b200.batch import Job
+    from xpg_b200.frames import GeneratedFrames
+    from xpg_b200.plan import IntegrationModel
+    jobs, n_refl = [], 0
+    for s in specs:
+        exp = s.experiment()
+        _, table = synth.reflection_table(s, z_range=(-5.0, s.nframes + 5.0))
+        spots = synth.DeviceSpots(s, table, device)
+        edges = s.block_edges()
+        jobs.append(Job(GeneratedFrames(spots, first=1, last=s.nframes, overload=s.overload, device=device),
+                        [exp] * (len(edges) - 1), edges, IntegrationModel(sigma_d=s.sigma_d, sigma_m=s.sigma_m),
+                        s.resolution_limit(), dict(frames=(1, s.nframes), n_regions_xy=s.n_regions_xy,
+                                                   wedge_frames=wedge_frames), label=s.name))
+    return jobs
+
+
+def batched_bench(args):
+    """Config 4: 12 sweeps (log-uniform 50..3600 frames, three detectors, three cells, sigma_M 0.05..0.5 deg),
+    integrated one after another by `integrate()` (plain) and together by the batched scheduler (shared persistent
+    pass launches, admission by device footprint); frames rendered on the device inside both timed regions. One JSON
+    line: reflections/s of both and their ratio, and that every result is the same in both."""
+    import torch
+    from xpg_b200 import device as D
+    from xpg_b200 import synth
+    from xpg_b200.batch import run_jobs
+    from xpg_b200.csrc import build
+    from xpg_b200.integrate import integrate
+    if build.stale():
+        build.build()
+    specs = synth.config4()
+    jobs = _jobs_of(specs, WEDGE_FRAMES)
+
+    def plain():
+        return [integrate(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, verbose=False, **j.kwargs)
+                for j in jobs]
+
+    def batched():
+        return run_jobs(jobs, bins=args.bins)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) * 1e-3
+    for _ in range(max(args.warmup, 1)):
+        timed(plain)
+        timed(batched)
+    tp, tb, stats = [], [], None
+    D.TIMER.reset()
+    for _ in range(args.steps):
+        rp, t = timed(plain)
+        tp.append(t)
+        (rb, stats), t = timed(batched)
+        tb.append(t)
+    n = sum(len(r.refl["x"]) for r in rp)
+    same = all(np.array_equal(a.refl[k], b.refl[k], equal_nan=True) for a, b in zip(rp, rb)
+               for k in ("isum", "iprf", "vprf", "bg", "isum_raw"))
+    line = {"metric": "integrated reflections/s, 12 sweeps (config 4), batched vs plain", "unit": "refl/s",
+            "value": round(n / np.median(tb), 1), "plain": round(n / np.median(tp), 1),
+            "speedup": round(float(np.median(tp) / np.median(tb)), 3), "steps": args.steps, "warmup": args.warmup,
+            "seconds": {"plain": [round(t, 3) for t in tp], "batched": [round(t, 3) for t in tb]},
+            "reflections": n, "same_results": bool(same),
+            "sweeps": [{"frames": s.nframes, "detector": [s.nx, s.ny], "cell": s.space_group,
+                        "sigma_m": round(s.sigma_m, 3), "reflections": len(r.refl["x"])} for s, r in zip(specs, rp)],
+            "batched_stats": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "pass1_launches",
+                                                                      "peak_bytes")},
+            "data": "synthetic, frames rendered on the device inside the timed region (both forms)"}
+    print(json.dumps(line), flush=True)
+
+
+def served_bench(args):
+    """Config 5: concurrent sweeps of config 2's geometry (cells from config 4's list) whose 50-frame wedges arrive
+    at 500 Hz per sweep with Poisson jitter (exponential gaps of 0.1 s mean between wedges); each arriving wedge is
+    rendered on the device (the detector's frames landing in HBM) and fed to the request loop, which admits sweeps by
+    device footprint and batches their completed blocks. One JSON line: p50 / p99 wedge-to-intensities latency
+    against the 0.1 s acquisition time of a wedge, and sustained reflections/s."""
+    import torch
+    from xpg_b200 import synth
+    from xpg_b200.batch import run_jobs
+    from xpg_b200.csrc import build
+    if build.stale():
+        build.build()
+    specs = synth.config5(nframes=args.served_frames)
+    rng = np.random.default_rng(55)
+    wedge = 50
+    jobs = _jobs_of(specs, wedge)
+    for j in jobs:
+        nw = len(range(1, j.kwargs["frames"][1] + 1, wedge))
+        j.arrivals = np.cumsum(rng.exponential(wedge / 500.0, nw))
+    run_jobs(_jobs_of(specs[:1], wedge), bins=args.bins)           # warm-up: kernels loaded, allocator primed
+    torch.cuda.synchronize()
+    res, stats = run_jobs(jobs, bins=args.bins, served=True)
+    lat = np.array([x[2] for x in stats["latency"]])
+    n = sum(len(r.refl["x"]) for r in res)
+    last_arrival = max(float(j.arrivals[-1]) for j in jobs)
+    line = {"metric": "served: wedge-to-intensities latency and sustained reflections/s (config 5)", "unit": "s",
+            "p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4),
+            "max": round(float(lat.max()), 4), "wedge_acquisition_s": wedge / 500.0,
+            "sustained_refl_per_s": round(n / stats["seconds"], 1), "seconds": round(stats["seconds"], 3),
+            "last_arrival_s": round(last_arrival, 3), "wedges": int(lat.size), "reflections": n,
+            "sweeps": [{"frames": s.nframes, "cell": s.space_group, "reflections": len(r.refl["x"])}
+                       for s, r in zip(specs, res)],
+            "scheduler": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "peak_bytes", "waits")},
+            "data": "synthetic; wedges rendered on the device at their arrival"}
     print(json.dumps(line), flush=True)
 
 
@@ -732,7 +848,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--workload", default="config2-sweep",
-                    choices=("config2-sweep", "config2-block", "config2-small", "config1"))
+                    choices=("config2-sweep", "config2-block", "config2-small", "config1", "config4", "config5"))
+    ap.add_argument("--bins", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
+                    help="size bins (box sides) of the batched pass launches, e.g. 17,31,55,97")
+    ap.add_argument("--served-frames", type=int, default=720, help="frames per sweep of the served workload")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -744,6 +863,10 @@ def main():
         decode_bench(args)
     elif args.spots:
         spots_bench(args)
+    elif args.workload == "config4" and args.impl != "reference":
+        batched_bench(args)
+    elif args.workload == "config5" and args.impl != "reference":
+        served_bench(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

@@ -149,11 +149,12 @@ int xi_version(void);
 int xi_status(void *stream);
 
 /* Launch tuning (process-wide; no counterpart in XPG, whose torch kernels have no launch shape): the largest
- * shoebox (bytes) pass 1 / pass 2 stage in shared memory, and pass 2's fit-list capacity (voxels). Results do not
- * depend on these. */
+ * shoebox (bytes) pass 1 / pass 2 stage in shared memory, pass 2's fit-list capacity (voxels) and the CTA width of
+ * large boxes. Results do not depend on these. */
 #define XI_TUNE_PASS1_STAGE_BYTES 1
 #define XI_TUNE_PASS2_STAGE_BYTES 2
 #define XI_TUNE_PASS2_LIST_CAP 3
+#define XI_TUNE_WIDE_THREADS 4      /* threads per CTA of the pass kernels for boxes over 200 pixels: 128 or 256 */
 int xi_tune(int key, long long value);
 
 /* Frame gather (xpg/integrate.py:704-787 with the preparation of :667-699 and the encoding of
@@ -161,6 +162,19 @@ int xi_tune(int key, long long value);
  * to its arena slot (value + 3), or, for binned rows (fb > 1), added to its bin in IEEE encoding (overloaded: NaN,
  * masked: +inf) with the bin's frame counter incremented. Frames must be passed in increasing order over calls. */
 int xi_gather(const XiFrames *frames, const XiGatherRows *rows, float *arena, int32_t *cnt, void *stream);
+
+/* The gather of one wedge described in device memory (read when the kernel runs), for a launch captured once in a
+ * CUDA graph and replayed for every wedge of a block: write the wedge's descriptor, then replay. The rows' boxes
+ * (rows, arena, cnt) are fixed for the block; CTAs (grid) stride over the descriptor's rows. Same results as
+ * xi_gather with those frames and rows. No counterpart in XPG (its gather is a host loop). */
+typedef struct {
+    XiFrames frames;                /* the wedge (data, first_fi, n_frames, ...); n_frames 0: nothing to gather */
+    const int32_t *order;           /* (n_order) rows of the block gathered from this wedge, device */
+    int n_order;
+} XiGatherStep;
+
+int xi_gather_step(const XiGatherStep *step, const XiGatherRows *rows, float *arena, int32_t *cnt, int grid,
+                   void *stream);
 
 /* Binned-bin decode (xpg/shoebox.py:264-268, xpg/integrate.py:483-488): NaN -> -2, inf -> -1, stored + 3; bins
  * with fewer than fb frames recorded become unrecorded (0). Applies to rows with cnt_off >= 0 (of rows->order when
@@ -385,6 +399,20 @@ int xi_pack_u8(const uint32_t *src, int64_t n, uint8_t *plane, uint32_t *exc, in
 /* Widens a packed run on the device: out[i] (n uint32) from plane (n bytes) and the n_exc pairs at exc (all three
  * device memory; plane and out 16-byte aligned). */
 int xi_unpack_u8(const uint8_t *plane, int64_t n, const uint32_t *exc, int64_t n_exc, uint32_t *out, void *stream);
+
+/* A packed frame of a store of packed frames (device pointers): plane (16-byte aligned) and its exception pairs, or
+ * (raw = 1) the frame's uint32 values at plane. */
+typedef struct {
+    const uint8_t *plane;
+    const uint32_t *exc;
+    int64_t n_exc;
+    int raw;
+} XiPackedFrame;
+
+/* Widens n_frames packed frames of n pixels each (descriptors in device memory) into out + k * stride (out 16-byte
+ * aligned, stride a multiple of 4 and >= n) in one launch. */
+int xi_unpack_u8_frames(const XiPackedFrame *frames, int n_frames, int64_t n, uint32_t *out, int64_t stride,
+                        void *stream);
 
 /* ---- Bitshuffle-LZ4 frames (Eiger chunks, HDF5 filter 32008) ----------------------------------------------------
  * XPG's split of the decode (xpg/io/bslz4.py): the LZ4 stage on the host (`lz4_stage`, :35-64), the bit unshuffle on

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts_match_header(tmp_path):
-    structs = {"XiDetector": N.XiDetector, "XiRows": N.XiRows, "XiRowSet": N.XiRowSet, "XiBlock": N.XiBlock, "XiPass1Out": N.XiPass1Out,
+    structs = {"XiDetector": N.XiDetector, "XiRows": N.XiRows, "XiRowSet": N.XiRowSet, "XiGatherStep": N.XiGatherStep, "XiPackedFrame": N.XiPackedFrame, "XiBlock": N.XiBlock, "XiPass1Out": N.XiPass1Out,
                "XiPass2In": N.XiPass2In, "XiPass2Out": N.XiPass2Out, "XiGatherRows": N.XiGatherRows,
                "XiFrames": N.XiFrames, "XiPlanDetector": N.XiPlanDetector, "XiPredict": N.XiPredict,
                "XiPredictOut": N.XiPredictOut, "XiBoxRules": N.XiBoxRules, "XiBoxOut": N.XiBoxOut, "XiKnn": N.XiKnn,

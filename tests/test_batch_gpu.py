@@ -52,10 +52,12 @@ def test_batched_results_equal_alone():
 
 def test_admission_by_memory_keeps_results():
     """A budget that holds one sweep at a time: sweeps wait and are admitted as memory frees up, same results."""
-    from xpg_b200.batch import footprint, run_jobs
+    from xpg_b200.batch import job_footprint, run_jobs
     jobs = [_job(c) for c in ("adaptive", "binned")]
     alone = [_alone(j) for j in jobs]
-    res, stats = run_jobs(jobs, budget_bytes=1)
+    need = [job_footprint(j) for j in jobs]
+    res, stats = run_jobs(jobs, budget_bytes=max(need) + min(need) // 2)     # one at a time, none split
+    assert all(r.memory["parts"] == 1 for r in res)
     assert stats["admitted_at"][1] >= stats["admitted_at"][0]
     for c, a, b in zip(("adaptive", "binned"), alone, res):
         _same(a, b, c)

@@ -18,6 +18,7 @@ def test_config2_block_sample_matches_oracle():
     wl = bench.Workload("config2-block")
     res = wl.integrate(wl.source())
     p = wl.plan
+    assert res.memory["parts"] == 1
     np.testing.assert_array_equal(res.refl["iz0"], p.iz0)
     assert np.isfinite(res.refl["iprf"]).all()
     rows = stratified_rows(p, np.arange(p.n), n_min=500)

@@ -229,20 +229,37 @@ def test_pack_generated_frames_round_trip():
         assert torch.equal(out, ref[k]), k
 
 
-def test_integration_in_parts_under_a_memory_budget(monkeypatch):
+def test_integration_in_parts_under_a_memory_budget():
     """A device budget below the open blocks' buffers: each phi block is integrated in parts of consecutive phi
     (own profiles and widths), as XPG does when its host budget is short; as the reference's own test of that mode
     (tests/test_pipeline.py:146-177): the same reflections, median |dI| / sigma < 0.1 against one pass."""
     from xpg_b200 import memplan
-    case = "adaptive"
+    from xpg_b200.plan import IntegrationModel, plan_integration
+    case = "config1"
+    z = G.load(case)
+    spec = G.case_inputs(case)[0]
+    edges = z["edges"]
+    p = plan_integration([spec.experiment()] * (len(edges) - 1), edges, IntegrationModel(spec.sigma_d, spec.sigma_m),
+                         float(z["dmin"]), 1e9, (1, spec.nframes), 0.05, spec.n_regions_xy, True, True)
+    one, _ = memplan.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, memplan.row_bytes(p), spec.nframes)
+    wedges = 3 * 32 * spec.ny * spec.nx * 4
     a = _run(case).refl
-    monkeypatch.setenv("XPG_INTEGRATE_MEM_GB", "0.0002")
-    monkeypatch.setattr(memplan, "BLOCK_PARTS_MAX", 3)
-    res = _run(case)
+    res = _run(case, mem_budget=0.92 * one + wedges)
     b = res.refl
-    assert len(res.profiles) > 2                          # more parts than the two phi blocks
+    assert res.memory["parts"] > 1 and len(res.profiles) == res.memory["parts"]
     np.testing.assert_array_equal(a["hkl"], b["hkl"])
     ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
     assert ok.mean() > 0.9
     d = np.abs(a["iprf"][ok] - b["iprf"][ok]) / np.sqrt(a["vprf"][ok])
     assert np.median(d) < 0.1
+
+
+@pytest.mark.parametrize("case", ["binned", "adaptive"])
+def test_gather_graph_identical(case):
+    """Each wedge's gathers replayed from a CUDA graph (captured once per set of open blocks, the wedge's frames and
+    rows in a device descriptor) give the same bits as direct launches; "binned" has excluded frames, "adaptive" two
+    blocks open at once."""
+    a = _run(case, wedge_frames=8).refl
+    b = _run(case, wedge_frames=8, graphs=True).refl
+    for k in CHECK_F + ("n_over", "n_fg_masked", "isum_raw"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k

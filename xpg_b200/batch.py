@@ -57,6 +57,17 @@ def footprint(plan, n_frames, wedge_bytes, depth=3):
     return int(np.cumsum(d).max()) + depth * wedge_bytes
 
 
+def job_footprint(job, device="cuda"):
+    """Device bytes a job needs when it runs (planned here; nothing is integrated)."""
+    run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, early_pass1=False,
+                   device=device, verbose=False, mem_budget=float("inf"), **job.kwargs)
+    try:
+        wb = max(fb - fa + 1 for fa, fb in run.wedges) * run.src.ny * run.src.nx * 4
+        return footprint(run.plan, run.wedges[-1][1], wb)
+    finally:
+        run.close()
+
+
 @dataclass
 class Job:
     """One sweep to integrate: `integrate()`'s arguments (images: a frame source), an optional label, and for
@@ -116,11 +127,12 @@ def _round(active, bins, stats):
 
 
 def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, clock=time.perf_counter,
-             on_wedge=None, max_active=None):
+             on_wedge=None, max_active=None, graphs=True):
     """Integrates `jobs` (list of Job) together; returns (results in job order, stats). served: each wedge is fed no
     earlier than its arrival time (job.arrivals, seconds after the start) and the latency of every wedge (from its
     arrival to the completion of everything it triggered: its gathers and, when it completes blocks, their
-    intensities on the host) is recorded in stats["latency"]."""
+    intensities on the host) is recorded in stats["latency"]. graphs: each sweep's per-wedge gathers replayed from
+    a CUDA graph (captured once per set of open blocks)."""
     budget = budget_bytes if budget_bytes is not None else int(0.8 * torch.cuda.mem_get_info(device)[0])
     queue = list(range(len(jobs)))
     active, results = [], [None] * len(jobs)
@@ -144,7 +156,7 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 return                                       # the request has not arrived
             if i not in head:
                 run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, early_pass1=False,
-                               device=device, verbose=False, mem_budget=budget, **job.kwargs)
+                               device=device, verbose=False, mem_budget=budget, graphs=graphs, **job.kwargs)
                 wb = max(fb - fa + 1 for fa, fb in run.wedges) * run.src.ny * run.src.nx * 4
                 head[i] = (run, footprint(run.plan, run.wedges[-1][1], wb))
             run, need = head[i]

@@ -339,7 +339,7 @@ constexpr int kGatherBatch = 8;     // frames of a box pixel read together by th
 __host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * P + 15) / 16 * 16; }
 
 // resident CTAs per SM the pass kernels are compiled for (registers per thread <= 65536 / (NT * blocks))
-template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 4 : 8); }
+template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 6 : 8); }
 
 // Pass 1 of one row, by the whole CTA. `bar`: the CTA's bulk-copy barrier (initialised once per CTA), `phase`: its
 // next phase (advanced here when the row is staged by a bulk copy). The caller separates consecutive rows of a CTA
@@ -1388,9 +1388,9 @@ __device__ __forceinline__ float box_value(const XiFrames& F, const void* frame,
     return sum;
 }
 
-__global__ void k_gather(XiFrames F, XiGatherRows G, float* __restrict__ arena, int32_t* __restrict__ cnt,
-                         const int32_t* __restrict__ order) {
-    const int row = order ? order[blockIdx.x] : blockIdx.x;
+// The gather of one row's box from the frames of a wedge, by the whole CTA.
+__device__ __forceinline__ void gather_row(const XiFrames& F, const XiGatherRows& G, float* __restrict__ arena,
+                                           int32_t* __restrict__ cnt, int row) {
     const int iz0 = G.iz0[row], fb = G.fb[row], Dz = G.Dz[row], bx = G.bx[row];
     const int s = G.pxs ? G.pxs[row] : 1;
     const int ix0 = G.ix0[row], iy0 = G.iy0[row];
@@ -1455,6 +1455,22 @@ __global__ void k_gather(XiFrames F, XiGatherRows G, float* __restrict__ arena, 
         }
     }
 }
+
+__global__ void k_gather(XiFrames F, XiGatherRows G, float* __restrict__ arena, int32_t* __restrict__ cnt,
+                         const int32_t* __restrict__ order) {
+    gather_row(F, G, arena, cnt, order ? order[blockIdx.x] : blockIdx.x);
+}
+
+// The gather of one wedge with the frames and rows read from a device descriptor when the kernel runs, so that one
+// launch captured in a CUDA graph serves every wedge of a block: CTAs stride over the step's rows.
+__global__ void k_gather_step(const XiGatherStep* __restrict__ step, XiGatherRows G, float* __restrict__ arena,
+                              int32_t* __restrict__ cnt) {
+    const XiFrames F = step->frames;
+    const int n = step->n_order;
+    if (F.n_frames <= 0) return;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) gather_row(F, G, arena, cnt, step->order[k]);
+}
+
 
 __global__ void k_decode_bins(XiGatherRows G, float* __restrict__ arena, const int32_t* __restrict__ cnt) {
     const int row = G.order ? G.order[blockIdx.x] : blockIdx.x;
@@ -1666,6 +1682,7 @@ constexpr size_t kStageBudget = 190 * 1024;
 // pass 2. Larger staging overlaps the box read with the set-up but costs resident CTAs per SM.
 size_t g_stage_max[2] = {48 * 1024, 48 * 1024};
 int g_list_cap = 2048;
+int g_wide_nt = 256;          // threads per CTA of the pass kernels for boxes over 200 pixels (128 or 256)
 
 // Pass 1 stages boxes of up to g_stage_max[0] bytes when they fit beside the per-pixel tables.
 bool pass1_staged(size_t P, int max_dz) {
@@ -1724,6 +1741,11 @@ int xi_tune(int key, long long value) {
         g_stage_max[key == XI_TUNE_PASS1_STAGE_BYTES ? 0 : 1] = (size_t)value;
         return XI_OK;
     }
+    if (key == XI_TUNE_WIDE_THREADS) {
+        if (value != 128 && value != 256) return fail(XI_E_LIMIT, "xi_tune: threads per CTA (128 or 256)");
+        g_wide_nt = (int)value;
+        return XI_OK;
+    }
     if (key == XI_TUNE_PASS2_LIST_CAP) {
         if (value < 0 || value > 16384) return fail(XI_E_LIMIT, "xi_tune: list capacity");
         g_list_cap = (int)value;
@@ -1762,11 +1784,11 @@ int xi_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     const bool staged = pass1_staged(P, R->max_dz);
     if (staged) {
         if (P <= 96) return launch_pass1<64, true>(det, R, B, arena, O, s, nblk);
-        if (P <= 200) return launch_pass1<128, true>(det, R, B, arena, O, s, nblk);
+        if (P <= 200 || g_wide_nt == 128) return launch_pass1<128, true>(det, R, B, arena, O, s, nblk);
         return launch_pass1<256, true>(det, R, B, arena, O, s, nblk);
     }
     if (P <= 96) return launch_pass1<64, false>(det, R, B, arena, O, s, nblk);
-    if (P <= 200) return launch_pass1<128, false>(det, R, B, arena, O, s, nblk);
+    if (P <= 200 || g_wide_nt == 128) return launch_pass1<128, false>(det, R, B, arena, O, s, nblk);
     return launch_pass1<256, false>(det, R, B, arena, O, s, nblk);
 }
 
@@ -1786,11 +1808,11 @@ int xi_pass2(const XiDetector* det, const XiRows* R, const XiBlock* B, const flo
     if (rc) return rc;
     if (staged) {
         if (P <= 96) return launch_pass2<64, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
-        if (P <= 200) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
+        if (P <= 200 || g_wide_nt == 128) return launch_pass2<128, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
         return launch_pass2<256, true>(det, R, B, arena, prof, in, O, s, nblk, cap);
     }
     if (P <= 96) return launch_pass2<64, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
-    if (P <= 200) return launch_pass2<128, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
+    if (P <= 200 || g_wide_nt == 128) return launch_pass2<128, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
     return launch_pass2<256, false>(det, R, B, arena, prof, in, O, s, nblk, cap);
 }
 
@@ -1811,11 +1833,11 @@ int xi_pass1_batched(const XiRowSet* sets, const int64_t* items, int n_items, in
     const size_t P = (size_t)max_bx * max_bx;
     if (pass1_staged(P, max_dz)) {
         if (P <= 96) return launch_pass1_q<64, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
-        if (P <= 200) return launch_pass1_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+        if (P <= 200 || g_wide_nt == 128) return launch_pass1_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
         return launch_pass1_q<256, true>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
     }
     if (P <= 96) return launch_pass1_q<64, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
-    if (P <= 200) return launch_pass1_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
+    if (P <= 200 || g_wide_nt == 128) return launch_pass1_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
     return launch_pass1_q<256, false>(sets, items, n_items, max_bx, max_dz, max_k, queue, s);
 }
 
@@ -1831,11 +1853,11 @@ int xi_pass2_batched(const XiRowSet* sets, const int64_t* items, int n_items, in
     if (rc) return rc;
     if (staged) {
         if (P <= 96) return launch_pass2_q<64, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
-        if (P <= 200) return launch_pass2_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+        if (P <= 200 || g_wide_nt == 128) return launch_pass2_q<128, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
         return launch_pass2_q<256, true>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
     }
     if (P <= 96) return launch_pass2_q<64, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
-    if (P <= 200) return launch_pass2_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
+    if (P <= 200 || g_wide_nt == 128) return launch_pass2_q<128, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
     return launch_pass2_q<256, false>(sets, items, n_items, max_bx, max_dz, max_k, cap, queue, s);
 }
 
@@ -1846,6 +1868,14 @@ int xi_gather(const XiFrames* F, const XiGatherRows* G, float* arena, int32_t* c
     if (nblk == 0 || F->n_frames == 0) return XI_OK;
     k_gather<<<nblk, 128, 0, (cudaStream_t)stream>>>(*F, *G, arena, cnt, G->order);
     return cuda_check("xi_gather");
+}
+
+int xi_gather_step(const XiGatherStep* step, const XiGatherRows* G, float* arena, int32_t* cnt, int grid,
+                   void* stream) {
+    if (!step || !G || !arena) return fail(XI_E_ARG, "xi_gather_step: null argument");
+    if (grid <= 0 || G->n < 0) return fail(XI_E_ARG, "xi_gather_step: bad sizes");
+    k_gather_step<<<grid, 128, 0, (cudaStream_t)stream>>>(step, *G, arena, cnt);
+    return cuda_check("xi_gather_step");
 }
 
 int xi_decode_bins(const XiGatherRows* G, float* arena, const int32_t* cnt, void* stream) {

@@ -17,10 +17,12 @@ constexpr int64_t kSpan = (int64_t)kNT * 16 * 4;   // pixels per CTA: four 16-by
 
 __device__ __forceinline__ uint32_t widen(uint32_t b) { return b == XI_PACK_FLAGGED ? 0xFFFFFFFFu : b; }
 
-__global__ void __launch_bounds__(kNT) k_unpack_u8(const uint8_t* __restrict__ plane, int64_t n,
-                                                   const uint32_t* __restrict__ exc, int64_t n_exc,
-                                                   uint32_t* __restrict__ out) {
-    const int64_t a = (int64_t)blockIdx.x * kSpan;
+// One span (kSpan pixels, index `span`) of a packed run widened into out: the byte codes, then the span's
+// exception pairs.
+__device__ __forceinline__ void unpack_span(const uint8_t* __restrict__ plane, int64_t n,
+                                            const uint32_t* __restrict__ exc, int64_t n_exc,
+                                            uint32_t* __restrict__ out, int64_t span) {
+    const int64_t a = span * kSpan;
     const int64_t b = a + kSpan < n ? a + kSpan : n;
     for (int64_t p = a + (int64_t)threadIdx.x * 16; p < b; p += (int64_t)kNT * 16) {
         if (p + 16 <= b) {
@@ -53,6 +55,27 @@ __global__ void __launch_bounds__(kNT) k_unpack_u8(const uint8_t* __restrict__ p
         if (i >= b) break;
         out[i] = exc[2 * k + 1];
     }
+}
+
+__global__ void __launch_bounds__(kNT) k_unpack_u8(const uint8_t* __restrict__ plane, int64_t n,
+                                                   const uint32_t* __restrict__ exc, int64_t n_exc,
+                                                   uint32_t* __restrict__ out) {
+    unpack_span(plane, n, exc, n_exc, out, blockIdx.x);
+}
+
+// Several packed frames at once (blockIdx.y: the frame); a raw frame's plane holds its uint32 values (copied).
+__global__ void __launch_bounds__(kNT) k_unpack_u8_frames(const XiPackedFrame* __restrict__ fr, int64_t n,
+                                                          uint32_t* __restrict__ out, int64_t stride) {
+    const XiPackedFrame f = fr[blockIdx.y];
+    uint32_t* o = out + (int64_t)blockIdx.y * stride;
+    if (f.raw) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(f.plane);
+        const int64_t a = (int64_t)blockIdx.x * kSpan;
+        const int64_t b = a + kSpan < n ? a + kSpan : n;
+        for (int64_t p = a + threadIdx.x; p < b; p += kNT) o[p] = src[p];
+        return;
+    }
+    unpack_span(f.plane, n, f.exc, f.n_exc, o, blockIdx.x);
 }
 
 // byte copy from mapped host memory; the 16-byte body when both ends are 16-byte aligned, bytes otherwise
@@ -171,6 +194,18 @@ extern "C" int xi_upload(const void* src, void* dst, int64_t bytes, void* stream
     grid = grid < 1 ? 1 : (grid > 1184 ? 1184 : grid);          // 8 CTAs per SM at most
     k_upload<<<(unsigned)grid, kNT, 0, (cudaStream_t)stream>>>(s, static_cast<uint8_t*>(dst), bytes, vec);
     return xi_cuda_check("xi_upload");
+}
+
+extern "C" int xi_unpack_u8_frames(const XiPackedFrame* frames, int n_frames, int64_t n, uint32_t* out, int64_t stride,
+                                   void* stream) {
+    if (n < 0 || n_frames < 0 || stride < n || (n && n_frames && (!frames || !out)))
+        return xi_fail(XI_E_ARG, "xi_unpack_u8_frames: null pointer or bad size");
+    if (n > XI_PACK_MAX_PIXELS || n_frames > 65535) return xi_fail(XI_E_LIMIT, "xi_unpack_u8_frames: too large");
+    if (((uintptr_t)out & 15) || (stride & 3)) return xi_fail(XI_E_ARG, "xi_unpack_u8_frames: out / stride alignment");
+    if (n == 0 || n_frames == 0) return XI_OK;
+    const dim3 grid((unsigned)((n + kSpan - 1) / kSpan), (unsigned)n_frames);
+    k_unpack_u8_frames<<<grid, kNT, 0, (cudaStream_t)stream>>>(frames, n, out, stride);
+    return xi_cuda_check("xi_unpack_u8_frames");
 }
 
 extern "C" int xi_unpack_u8(const uint8_t* plane, int64_t n, const uint32_t* exc, int64_t n_exc, uint32_t* out,

@@ -505,7 +505,7 @@ class RowSetTable:
 
 
 # Size bins of a batched launch: upper bounds on the box side; a bin's launch sizes shared memory and threads for its
-# largest box (the side bucket) and depth. Chosen by xpg_b200.tune (measured) unless given.
+# largest box (the side bucket) and depth. The tuned bins of the device (xpg_b200.tune, tuned.json) replace these.
 DEFAULT_BINS = (17, 31, 41, 55, 97)
 
 
@@ -513,7 +513,10 @@ def batched_items(groups, bins=None, device="cuda"):
     """Launch bins of a batched pass. groups: (set index, local rows, their sides, their depths) per set. Returns
     [(max_bx, max_dz, items)] with items an int64 device tensor (set << 32 | row), each bin's rows largest box
     first (resident CTAs take the big rows before the small ones, which balances the launch)."""
-    bins = tuple(bins or DEFAULT_BINS)
+    if bins is None:
+        from .tune import load_bins
+        bins = load_bins() or DEFAULT_BINS
+    bins = tuple(bins)
     cols = [(np.full(len(r), s, np.int64), np.asarray(r, np.int64), np.asarray(b, np.int64), np.asarray(d, np.int64))
             for s, r, b, d in groups if len(r)]
     if not cols:
@@ -561,3 +564,37 @@ def pass2_batched(table: RowSetTable, launches, stream=None):
             N.check(lib.xi_pass2_batched(N.ptr(table.t), N.ptr(items), int(items.numel()), mbx, mdz, table.k_max,
                                          C.c_void_p(q.data_ptr() + 4 * (i % 64)), _stream(stream)),
                     "xi_pass2_batched")
+
+
+class GatherGraph:
+    """The gathers of one wedge into the open blocks, captured once as a CUDA graph and replayed for every wedge
+    while the same blocks are open: each block's launch reads the wedge's frames and rows from a device descriptor
+    (xi_gather_step), which an upload rewrites before each replay. `key`: the open blocks the graph was captured
+    for."""
+
+    GRID = 148 * 8
+
+    def __init__(self, key, grows_list, arenas, cnts, device="cuda"):
+        self.key = key
+        n = len(grows_list)
+        self.size = C.sizeof(N.XiGatherStep)
+        self.desc = torch.zeros(max(n, 1) * self.size, dtype=torch.uint8, device=device)
+        self.graph = torch.cuda.CUDAGraph()
+        self._keep = (grows_list, arenas, cnts)
+        lib = N.load()
+        base = self.desc.data_ptr()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
+            st = _stream(None)
+            for j, (g, a, c) in enumerate(zip(grows_list, arenas, cnts)):
+                N.check(lib.xi_gather_step(C.c_void_p(base + j * self.size), C.byref(g.s), N.ptr(a), N.ptr(c),
+                                           self.GRID, st), "xi_gather_step")
+
+    def replay(self, steps):
+        """steps: one XiGatherStep per block of the key, in order."""
+        arr = (N.XiGatherStep * len(steps))(*steps)
+        host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
+        if not _RING.upload(host, self.desc[:host.numel()], torch.cuda.current_stream(self.desc.device)):
+            self.desc[:host.numel()].copy_(host.pin_memory(), non_blocking=True)
+        with TIMER.span("gather", len(steps)):
+            self.graph.replay()

@@ -586,6 +586,35 @@ class PackedStore:
         segs = [s[:int(u)].to(device) for s, u in zip(self.segments, used)]
         return PackedStore(self.n_frames, self.ny, self.nx, segs, self.index.copy())
 
+    def unpack_frames(self, k0, n, out, stream, ok=None):
+        """Frames k0..k0+n-1 into out (device int32 (n, ny, nx), 16-byte aligned) with one launch on `stream`; the
+        store must be on the device; frames with ok False are skipped (left as they are)."""
+        import ctypes as C
+        from . import native
+        from .device import TIMER, h2d
+        arr = (native.XiPackedFrame * n)()
+        m = 0
+        order = []
+        for i in range(n):
+            if ok is not None and not ok[i]:
+                continue
+            seg, off, ne, raw = (int(v) for v in self.index[k0 + i])
+            base = self.segments[seg].data_ptr() + off
+            arr[m].plane, arr[m].exc, arr[m].n_exc, arr[m].raw = base, base + self.plane, ne, raw
+            order.append(i)
+            m += 1
+        if m == 0:
+            return
+        if m != n:                              # excluded frames: one launch per run of kept frames
+            for i in range(m):
+                self.unpack(k0 + order[i], out[order[i]], stream)
+            return
+        d = h2d(np.frombuffer(bytes(arr), np.uint8), None, out.device)
+        with TIMER.span("unpack"):
+            native.check(native.load().xi_unpack_u8_frames(C.c_void_p(d.data_ptr()), n, self.P,
+                                                            C.c_void_p(out.data_ptr()), self.P,
+                                                            C.c_void_p(stream.cuda_stream)), "xi_unpack_u8_frames")
+
     def unpack(self, k, out, stream):
         """Frame k into out (device uint32 / int32 frame, 16-byte aligned) on `stream`; the store must be on the
         device."""
@@ -743,8 +772,26 @@ class PackedFrames:
         self.depth = depth
         self.transfer = {}
 
+    @property
+    def on_device(self):
+        return bool(self.store.segments) and self.store.segments[0].is_cuda
+
+    @property
+    def hide_transfer(self):
+        return not self.on_device
+
     def feeder(self, wedges, oks):
+        """A transfer thread when the store is in host memory; None when it is in HBM (wedges widened in place)."""
+        if self.on_device:
+            return None
         return _PackedFeeder(self.store, self.first, wedges, oks, self.device, self.depth, self.transfer)
+
+    def wedge(self, f_a, f_b, ok=None, stream=None):
+        n = f_b - f_a + 1
+        d = torch.empty((n, self.ny, self.nx), dtype=torch.int32, device=self.device)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        self.store.unpack_frames(f_a - self.first, n, d, st, ok)
+        return d, False
 
 
 class GeneratedFrames:
@@ -763,6 +810,7 @@ class GeneratedFrames:
         self.min_valid = 0
         self.device = device
         self.resident = False
+        self.hide_transfer = False
 
     def wedge(self, f_a, f_b, ok=None, stream=None):
         from .device import TIMER

@@ -127,13 +127,16 @@ class _Block:
 def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dmax=1e9, frames=None, mask=None,
               minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
               adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
-              n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed):
+              n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed,
+              graphs=False, mem_budget=None):
     """Integrate a sweep (`xpg/integrate.py:209-999`). `exp_blocks`: one experiment per phi block, `block_edges` in
-    frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id)."""
+    frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id); graphs:
+    each wedge's gathers replayed from a CUDA graph captured once per set of open blocks; mem_budget: device bytes the
+    open blocks' buffers may use (default: memplan.budget), beyond which blocks are integrated in parts."""
     run = SweepRun(images, exp_blocks, block_edges, model, dmin, dmax, frames, mask, minimum_zeta, verbose, log,
                    n_regions_xy, learn_profiles, exclude_frames, adaptive, deconvolve_overlaps, extra_lattices,
                    bkg_template, foreign_spots, n_foreign, moments_only, wedge_frames=wedge_frames, device=device,
-                   allowed=allowed)
+                   allowed=allowed, graphs=graphs, mem_budget=mem_budget)
     try:
         for w in range(len(run.wedges)):
             for b in run.feed(w):
@@ -159,7 +162,7 @@ class SweepRun:
                  minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
                  adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
                  n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda",
-                 allowed=centring_allowed, early_pass1=True, plan=None, mem_budget=None):
+                 allowed=centring_allowed, early_pass1=True, plan=None, mem_budget=None, graphs=False):
         N.require_cuda()
         self.t0 = time.time()
         lattice_of = [0] * len(exp_blocks)
@@ -238,7 +241,11 @@ class SweepRun:
         ok_parts = [ok.astype(np.uint8) for ok in self.oks if not ok.all()]
         self.ok_dev = D.h2d(np.concatenate(ok_parts), None, device) if ok_parts else None
         self.ok_off = 0
-        self.early_rows = EARLY_PASS1_ROWS if (early_pass1 and not resident) else 0
+        # (sources whose frames are produced in HBM have no transfer to hide)
+        hide = bool(getattr(src, "hide_transfer", True))
+        self.early_rows = EARLY_PASS1_ROWS if (early_pass1 and not resident and hide) else 0
+        self.graphs = graphs and not resident     # per-wedge gathers replayed from a CUDA graph (GatherGraph)
+        self._gg = None
 
     # ---- device constants
     def detector(self, g):
@@ -311,7 +318,28 @@ class SweepRun:
             ok_t = self.ok_dev[self.ok_off:self.ok_off + ok.size]
             self.ok_off += ok.size
         src = self.src
-        if ok.any() and self.opened:
+        if ok.any() and self.opened and self.graphs:
+            data, is_f = (self.feeder.get(w), False) if self.feeder is not None else src.wedge(f, f_b, ok)
+            slots = tuple(b for b in self.open_order if b in self.opened)
+            if self._gg is None or self._gg.key != slots:
+                blks = [self.opened[b] for b in slots]
+                self._gg = D.GatherGraph(slots, [k.grows for k in blks], [k.arena for k in blks],
+                                         [k.cnt for k in blks], self.device)
+            steps = []
+            for b in slots:
+                blk = self.opened[b]
+                stp = N.XiGatherStep()
+                if w in blk.w_gather:
+                    nf = min(fi_b, self.eff_hi[b]) - fi_a + 1
+                    stp.frames = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload,
+                                                 0 if is_f else src.min_valid, self.mask_t,
+                                                 ok_t[:nf] if ok_t is not None else None)
+                    order = blk.sched(blk.w_gather[w])
+                    stp.order = N.ptr(order)
+                    stp.n_order = int(order.numel())
+                steps.append(stp)
+            self._gg.replay(steps)
+        elif ok.any() and self.opened:
             data, is_f = (self.feeder.get(w), False) if self.feeder is not None else src.wedge(f, f_b, ok)
             for b in self.open_order:
                 blk = self.opened.get(b)
@@ -455,6 +483,8 @@ class SweepRun:
                                                                            gpu=self.t_dev))
         res.block_params = self.block_params
         res.block_widths = self.block_widths  # (sigma_D, sigma_M in radians, rocking-curve weights) of each pass
+        res.plan = self.plan                  # the plan integrated (blocks split in parts when memory was short)
+        res.memory = self.mem
         return res
 
     def close(self):

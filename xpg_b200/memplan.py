@@ -16,7 +16,7 @@ from dataclasses import replace
 import numpy as np
 
 BLOCK_PARTS_MAX = 8          # parts per phi block at most (xpg/integrate.py:55)
-DEVICE_FRACTION = 0.85       # share of the device memory free at the start that the run's buffers may use
+DEVICE_FRACTION = 0.95       # share of the device memory free at the start that the run's buffers may use
 
 
 def row_bytes(plan):

@@ -138,6 +138,14 @@ class XiSpotParams(C.Structure):
 XI_SPOT_MAX_HALF = 8
 
 
+class XiPackedFrame(C.Structure):
+    _fields_ = [("plane", _fp), ("exc", _fp), ("n_exc", C.c_int64), ("raw", C.c_int)]
+
+
+class XiGatherStep(C.Structure):
+    _fields_ = [("frames", XiFrames), ("order", _fp), ("n_order", C.c_int)]
+
+
 class XiRowSet(C.Structure):
     _fields_ = [("det", XiDetector), ("rows", XiRows), ("blk", XiBlock), ("arena", _fp), ("p1", XiPass1Out),
                 ("prof", _fp), ("p2", XiPass2Out)]
@@ -150,7 +158,7 @@ class XiHklRows(C.Structure):
                 ("alf1", C.c_void_p), ("bet1", C.c_void_p), ("alf0", C.c_double), ("bet0", C.c_double)]
 
 
-XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP = 1, 2, 3
+XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP, XI_TUNE_WIDE_THREADS = 1, 2, 3, 4
 XI_PACK_ESCAPE, XI_PACK_FLAGGED = 254, 255
 
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
@@ -158,7 +166,7 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
            "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
            "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong", "xi_spot_workspace", "xi_pass1_batched",
-           "xi_pass2_batched")
+           "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames")
 
 _LIB = None
 
@@ -216,6 +224,9 @@ def load(path=None):
     lib.xi_finalize_profiles.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.xi_pass2.argtypes = [C.POINTER(XiDetector), C.POINTER(XiRows), C.POINTER(XiBlock), C.c_void_p, C.c_void_p,
                              C.POINTER(XiPass2In), C.POINTER(XiPass2Out), C.c_void_p]
+    lib.xi_unpack_u8_frames.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
+    lib.xi_gather_step.argtypes = [C.c_void_p, C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_int,
+                                   C.c_void_p]
     for name in ("xi_pass1_batched", "xi_pass2_batched"):
         getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                        C.c_void_p]
@@ -254,9 +265,11 @@ def require_cuda():
     load()
 
 
-def tune(pass1_stage_bytes=None, pass2_stage_bytes=None, pass2_list_cap=None):
+def tune(pass1_stage_bytes=None, pass2_stage_bytes=None, pass2_list_cap=None, wide_threads=None):
     """Launch tuning of the pass kernels (results are independent of it)."""
     lib = load()
+    if wide_threads is not None:
+        check(lib.xi_tune(XI_TUNE_WIDE_THREADS, int(wide_threads)), "xi_tune")
     if pass1_stage_bytes is not None:
         check(lib.xi_tune(XI_TUNE_PASS1_STAGE_BYTES, int(pass1_stage_bytes)), "xi_tune")
     if pass2_stage_bytes is not None:

@@ -1,0 +1,129 @@
+"""Autotuner of the batched pass launches: which box sides share a persistent launch (the size bins).
+
+A batched launch sizes its shared memory, threads per CTA and staging for the largest box of its bin: wide bins
+put small boxes in CTAs sized for large ones (fewer resident CTAs), narrow bins make more launches (more tails). The
+tuner times pass 1 and pass 2 of real blocks for candidate bin edges (subsets of the box-side buckets present, at
+most `max_bins` bins) and keeps the fastest; results are stored per device name in `tuned.json` beside this file,
+which `device.DEFAULT_BINS` reads.
+
+    python -m xpg_b200.tune [--workload config4|config2] [--max-bins 4]      (on the GPU)
+"""
+from __future__ import annotations
+
+import itertools
+import json
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import device as D
+
+TUNED = Path(__file__).resolve().parent / "tuned.json"
+XY_BUCKETS = (9, 13, 17, 23, 31, 41, 55, 73, 97)
+
+
+def candidates(sides, max_bins=4):
+    """Bin edge tuples over the box sides present: the largest side always closes the last bin."""
+    present = sorted(set(int(s) for s in sides))
+    top = present[-1]
+    inner = present[:-1]
+    out = []
+    for k in range(0, max_bins):
+        for c in itertools.combinations(inner, k):
+            out.append(tuple(c) + (top,))
+    return out
+
+
+def _time(fn, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps * 1e-3
+
+
+def tune_round(picks, max_bins=4, reps=3, device="cuda"):
+    """Times every candidate bin set on one batched round of completed blocks. picks: list of (SweepRun, block)
+    whose pass 1 and learning are done (their set entries valid). Returns [(seconds, bins)] fastest first."""
+    sets1, sets2, groups = [], [], []
+    for k, (run, b) in enumerate(picks):
+        blk = run.live[b]
+        rs = blk.rowset
+        det = run.detector(run.exp_blocks[b].geom)
+        sets1.append(D.rowset_entry(det, rs, blk.c1[3], blk.arena, blk.p1))
+        sets2.append(D.rowset_entry(det, rs, blk.c2[0], blk.arena, blk.p1, blk.prof, blk.p2))
+        groups.append((k, np.arange(rs.n), rs.bx, rs.Dz))
+    t1, t2 = D.RowSetTable(sets1, device), D.RowSetTable(sets2, device)
+    sides = np.concatenate([g[2] for g in groups])
+    out = []
+    for bins in candidates(sides, max_bins):
+        launches = D.batched_items(groups, bins, device)
+        t = _time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps)
+        out.append((t, bins))
+    out.sort()
+    return out
+
+
+def save(device_name, bins, table):
+    data = json.loads(TUNED.read_text()) if TUNED.exists() else {}
+    data[device_name] = {"bins": list(bins), "measured": [{"seconds": round(t, 5), "bins": list(b)}
+                                                          for t, b in table[:12]]}
+    TUNED.write_text(json.dumps(data, indent=1) + "\n")
+
+
+def load_bins(device_name=None):
+    """Tuned bins of this device (None when not tuned)."""
+    if not TUNED.exists():
+        return None
+    try:
+        name = device_name or torch.cuda.get_device_name()
+    except Exception:
+        return None
+    entry = json.loads(TUNED.read_text()).get(name)
+    return tuple(entry["bins"]) if entry else None
+
+
+def main():
+    import argparse
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    import bench
+    from .batch import run_jobs  # noqa: F401
+    from .integrate import SweepRun
+    from . import synth
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="config4", choices=("config4", "config2"))
+    ap.add_argument("--max-bins", type=int, default=4)
+    args = ap.parse_args()
+    specs = synth.config4()[:6] if args.workload == "config4" else [synth.config2(nframes=480)]
+    jobs = bench._jobs_of(specs, bench.WEDGE_FRAMES)
+    runs = [SweepRun(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, early_pass1=False, verbose=False,
+                     **j.kwargs) for j in jobs]
+    picks = []
+    for run in runs:                      # the first completed block of every sweep
+        done = []
+        for w in range(len(run.wedges)):
+            done = run.feed(w)
+            if done:
+                break
+        done = done or run.remaining()
+        b = done[0]
+        run.pass1_stage(b)
+        run.learn(b)
+        picks.append((run, b))
+    table = tune_round(picks, args.max_bins)
+    name = torch.cuda.get_device_name()
+    save(name, table[0][1], table)
+    print(json.dumps({"device": name, "best": list(table[0][1]), "seconds": round(table[0][0], 5),
+                      "worst": [round(table[-1][0], 5), list(table[-1][1])], "candidates": len(table)}))
+    for run in runs:
+        run.close()
+
+
+if __name__ == "__main__":
+    main()
