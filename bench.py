@@ -221,6 +221,7 @@ class Workload:
         from xpg_b200 import synth
         from xpg_b200.plan import plan_integration
         self.name, self.device = name, device
+        self.overlap = os.environ.get("XPG_BENCH_OVERLAP", "0") == "1"
         (self.spec, self.exp, self.model, self.edges, self.n_frames,
          self.plan) = plan_workload(name, seed_offset, plan_integration)
         s = self.spec
@@ -243,7 +244,7 @@ class Workload:
         nb = len(self.edges) - 1
         return integrate(frames, [self.exp] * nb, self.edges, self.model, self.spec.resolution_limit(),
                          frames=(1, self.n_frames), verbose=False, n_regions_xy=self.spec.n_regions_xy,
-                         wedge_frames=WEDGE_FRAMES)
+                         wedge_frames=WEDGE_FRAMES, overlap=self.overlap)
 
     def source(self):
         """Frames resident in HBM."""

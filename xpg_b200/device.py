@@ -583,12 +583,18 @@ class GatherGraph:
         self._keep = (grows_list, arenas, cnts)
         lib = N.load()
         base = self.desc.data_ptr()
-        torch.cuda.synchronize()
-        with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
-            st = _stream(None)
-            for j, (g, a, c) in enumerate(zip(grows_list, arenas, cnts)):
-                N.check(lib.xi_gather_step(C.c_void_p(base + j * self.size), C.byref(g.s), N.ptr(a), N.ptr(c),
-                                           self.GRID, st), "xi_gather_step")
+        # captured on a side stream (nothing runs; no device-wide synchronisation, the allocator's cache is kept)
+        cap = torch.cuda.Stream(device=self.desc.device)
+        cap.wait_stream(torch.cuda.current_stream(self.desc.device))
+        with torch.cuda.stream(cap):
+            self.graph.capture_begin(capture_error_mode="thread_local")
+            try:
+                st = _stream(cap)
+                for j, (g, a, c) in enumerate(zip(grows_list, arenas, cnts)):
+                    N.check(lib.xi_gather_step(C.c_void_p(base + j * self.size), C.byref(g.s), N.ptr(a), N.ptr(c),
+                                               self.GRID, st), "xi_gather_step")
+            finally:
+                self.graph.capture_end()
 
     def replay(self, steps):
         """steps: one XiGatherStep per block of the key, in order."""

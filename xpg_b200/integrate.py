@@ -31,6 +31,7 @@ PROFILE_GRID = 41
 MAX_DZ = max(DZ_BUCKETS)
 WEDGE_FRAMES = 32                     # frames per upload / gather launch
 EARLY_PASS1_ROWS = 16384              # completed rows worth an early pass-1 launch (uploaded frames)
+LOOKAHEAD = 2                         # wedges gathered (overlap mode) before the passes of a block they completed
 OUT_F64 = ("bg", "isum", "vsum", "vsum0", "iprf", "vprf", "vprf0", "corr", "xo", "yo", "zo", "p_valid", "p_total",
            "frac_rec", "rho", "m_d", "m_m", "p_fg")
 
@@ -83,6 +84,12 @@ class _Block:
         self.p1 = None                                    # pass-1 buffers and constants, made at the first pass 1
         self.c1 = None
         self.p1_done = np.zeros(rows.size, bool)
+        # gather order: rows by 128-pixel detector tile (row-major), plan order within a tile, so that the boxes the
+        # resident CTAs gather at one time overlap on the detector and share their frame pixels in L2
+        pxs_h = p.pxs[rows].astype(np.int64)
+        tile = ((p.iy0[rows] * pxs_h) // 128 + 64) * 4096 + (p.ix0[rows] * pxs_h) // 128 + 64
+        self.by_tile = np.argsort(tile, kind="stable").astype(np.int32)
+        self.z_lo_t, self.z_hi_t = self.z_lo[self.by_tile], self.z_hi[self.by_tile]
 
     def rows_in(self, fi_a, fi_b):
         """Local rows whose box frame range meets [fi_a, fi_b]."""
@@ -107,7 +114,8 @@ class _Block:
         for w, (fa, fb) in enumerate(wedges):
             fi_a, fi_b = fa - 1, fb - 1
             if eff_hi >= fi_a:
-                loc = self.rows_in(fi_a, min(fi_b, eff_hi))
+                hi = min(fi_b, eff_hi)
+                loc = self.by_tile[(self.z_lo_t <= hi) & (self.z_hi_t >= fi_a)]     # in gather (tile) order
                 if loc.size:
                     self.w_gather[w] = add(loc)
             if early_rows:
@@ -128,20 +136,26 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
               minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
               adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
               n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed,
-              graphs=False, mem_budget=None):
+              graphs=False, mem_budget=None, overlap=False):
     """Integrate a sweep (`xpg/integrate.py:209-999`). `exp_blocks`: one experiment per phi block, `block_edges` in
     frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id); graphs:
     each wedge's gathers replayed from a CUDA graph captured once per set of open blocks; mem_budget: device bytes the
-    open blocks' buffers may use (default: memplan.budget), beyond which blocks are integrated in parts."""
+    open blocks' buffers may use (default: memplan.budget), beyond which blocks are integrated in parts; overlap: the
+    gathers on a stream of their own, LOOKAHEAD wedges ahead of the passes of the blocks they completed."""
     run = SweepRun(images, exp_blocks, block_edges, model, dmin, dmax, frames, mask, minimum_zeta, verbose, log,
                    n_regions_xy, learn_profiles, exclude_frames, adaptive, deconvolve_overlaps, extra_lattices,
                    bkg_template, foreign_spots, n_foreign, moments_only, wedge_frames=wedge_frames, device=device,
-                   allowed=allowed, graphs=graphs, mem_budget=mem_budget)
+                   allowed=allowed, graphs=graphs, mem_budget=mem_budget, overlap=overlap)
     try:
+        ahead = LOOKAHEAD if run.gs is not None else 0
+        done = []                                    # (block, wedge that completed it), in processing order
         for w in range(len(run.wedges)):
-            for b in run.feed(w):
-                run.process(b)
+            done += [(b, w) for b in run.feed(w)]
+            while done and w - done[0][1] >= ahead:  # later wedges' gathers are queued before a block's passes
+                run.process(done.pop(0)[0])
             run.early_pass1(w)
+        for b, _ in done:
+            run.process(b)
         for b in run.remaining():
             run.process(b)
         return run.result()
@@ -162,7 +176,8 @@ class SweepRun:
                  minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
                  adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
                  n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda",
-                 allowed=centring_allowed, early_pass1=True, plan=None, mem_budget=None, graphs=False):
+                 allowed=centring_allowed, early_pass1=True, plan=None, mem_budget=None, graphs=False,
+                 overlap=False):
         N.require_cuda()
         self.t0 = time.time()
         lattice_of = [0] * len(exp_blocks)
@@ -246,6 +261,13 @@ class SweepRun:
         self.early_rows = EARLY_PASS1_ROWS if (early_pass1 and not resident and hide) else 0
         self.graphs = graphs and not resident     # per-wedge gathers replayed from a CUDA graph (GatherGraph)
         self._gg = None
+        self.reported = set()                     # completed blocks handed out by feed / remaining
+        # overlap: gathers on a stream of their own, so that they run beside the passes and the host's work on
+        # completed blocks (which then wait for their blocks' gathers only); blocks' pass-1 widths are taken when
+        # their pass 1 runs, so early pass 1 (which takes them at block opening) is off
+        self.gs = torch.cuda.Stream(device=device) if (overlap and not resident) else None
+        if self.gs is not None:
+            self.early_rows = 0
 
     # ---- device constants
     def detector(self, g):
@@ -281,6 +303,7 @@ class SweepRun:
 
     def decode_rows(self, b, blk: _Block, idx, binned_t=None):
         self.block_pass1_consts(b, blk)
+        self._wait_gathers(blk)
         if binned_t is None:
             binned = idx[blk.grows.binned[idx]]
             binned_t = D.h2d(binned.astype(np.int32), None, self.device) if binned.size else None
@@ -317,6 +340,36 @@ class SweepRun:
         if not ok.all():
             ok_t = self.ok_dev[self.ok_off:self.ok_off + ok.size]
             self.ok_off += ok.size
+        if self.gs is None:
+            self._gather_wedge(w, ok, ok_t, fi_a, fi_b)
+        else:
+            # the gathers go to the gather stream, after everything queued so far on the compute stream (block
+            # openings, uploads); passes wait for the event of the wedge that completed their block
+            ev = torch.cuda.Event()
+            ev.record()
+            self.gs.wait_event(ev)
+            with torch.cuda.stream(self.gs):
+                self._gather_wedge(w, ok, ok_t, fi_a, fi_b)
+                ev_w = torch.cuda.Event()
+                ev_w.record(self.gs)
+            for b in self.opened:
+                if w in self.opened[b].w_gather:
+                    self.opened[b].gathered = ev_w
+        if self.feeder is not None:
+            self.feeder.done_with(w)
+        done = sorted((b for b in self.open_order if b in self.opened and self.eff_hi[b] <= fi_b
+                       and b not in self.reported), key=lambda b: (self.eff_hi[b], self.open_order.index(b)))
+        self.reported.update(done)
+        return done
+
+    def _wait_gathers(self, blk):
+        """The compute stream waits for the block's gathers (two-stream mode)."""
+        ev = getattr(blk, "gathered", None)
+        if ev is not None:
+            torch.cuda.current_stream().wait_event(ev)
+
+    def _gather_wedge(self, w, ok, ok_t, fi_a, fi_b):
+        f, f_b = self.wedges[w]
         src = self.src
         if ok.any() and self.opened and self.graphs:
             data, is_f = (self.feeder.get(w), False) if self.feeder is not None else src.wedge(f, f_b, ok)
@@ -349,14 +402,12 @@ class SweepRun:
                 fs = D.frames_struct(data[:nf], fi_a, None if is_f else src.overload, 0 if is_f else src.min_valid,
                                      self.mask_t, ok_t[:nf] if ok_t is not None else None)
                 D.gather(fs, blk.grows, blk.sched(blk.w_gather[w]), blk.arena, blk.cnt)
-        if self.feeder is not None:
-            self.feeder.done_with(w)
-        return sorted((b for b in self.open_order if b in self.opened and self.eff_hi[b] <= fi_b),
-                      key=lambda b: (self.eff_hi[b], self.open_order.index(b)))
 
     def remaining(self):
         """The open blocks left after the last wedge, in processing order."""
-        return [b for b in self.open_order if b in self.opened]
+        out = [b for b in self.open_order if b in self.opened and b not in self.reported]
+        self.reported.update(out)
+        return out
 
     def early_pass1(self, w):
         """Pass 1 of the next block's rows whose last frame arrived with wedge w (uploaded frames only; after the
@@ -382,6 +433,7 @@ class SweepRun:
         for a batched launch (the caller launches, then calls learn)."""
         blk = self.opened.pop(b)
         self.live[b] = blk
+        self._wait_gathers(blk)
         self.tg = time.time()
         self.processed.append(b)
         rem = np.flatnonzero(~blk.p1_done)

@@ -236,7 +236,24 @@ def load(path=None):
     lib.xi_synth_last_error.restype = C.c_char_p
     if path is None:
         _LIB = lib
+        _apply_tuned(lib)
     return lib
+
+
+def _apply_tuned(lib):
+    """The launch shape measured best on this device by xpg_b200.tune (tuned.json), when there is one."""
+    try:
+        from .tune import load_shape
+        shape = load_shape()
+    except Exception:
+        shape = None
+    if not shape:
+        return
+    keys = {"wide_threads": XI_TUNE_WIDE_THREADS, "pass1_stage_bytes": XI_TUNE_PASS1_STAGE_BYTES,
+            "pass2_stage_bytes": XI_TUNE_PASS2_STAGE_BYTES, "pass2_list_cap": XI_TUNE_PASS2_LIST_CAP}
+    for k, v in shape.items():
+        if k in keys:
+            lib.xi_tune(keys[k], int(v))
 
 
 def check(rc, what):

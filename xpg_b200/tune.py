@@ -1,10 +1,12 @@
-"""Autotuner of the batched pass launches: which box sides share a persistent launch (the size bins).
+"""Autotuner of the pass launches: which box sides share a persistent launch (the size bins) and the CTA shape.
 
 A batched launch sizes its shared memory, threads per CTA and staging for the largest box of its bin: wide bins
 put small boxes in CTAs sized for large ones (fewer resident CTAs), narrow bins make more launches (more tails). The
-tuner times pass 1 and pass 2 of real blocks for candidate bin edges (subsets of the box-side buckets present, at
-most `max_bins` bins) and keeps the fastest; results are stored per device name in `tuned.json` beside this file,
-which `device.DEFAULT_BINS` reads.
+CTA shape of large boxes (128 threads at 6 CTAs per SM, or 256 at 3) and the largest box staged in shared memory by
+a bulk copy trade resident reflections per SM against work per CTA. The tuner times pass 1 and pass 2 of real blocks
+for candidate bin edges (subsets of the box-side buckets present, at most `max_bins` bins) and launch shapes, and
+keeps the fastest; results are stored per device name in `tuned.json` beside this file, which the library applies
+when it loads (`native.load`) and `device.batched_items` reads.
 
     python -m xpg_b200.tune [--workload config4|config2] [--max-bins 4]      (on the GPU)
 """
@@ -47,9 +49,16 @@ def _time(fn, reps=3):
     return e0.elapsed_time(e1) / reps * 1e-3
 
 
-def tune_round(picks, max_bins=4, reps=3, device="cuda"):
-    """Times every candidate bin set on one batched round of completed blocks. picks: list of (SweepRun, block)
-    whose pass 1 and learning are done (their set entries valid). Returns [(seconds, bins)] fastest first."""
+SHAPES = ({"wide_threads": 256, "pass1_stage_bytes": 48 * 1024}, {"wide_threads": 128, "pass1_stage_bytes": 48 * 1024},
+          {"wide_threads": 256, "pass1_stage_bytes": 0}, {"wide_threads": 128, "pass1_stage_bytes": 0},
+          {"wide_threads": 128, "pass1_stage_bytes": 96 * 1024})
+
+
+def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES):
+    """Times the candidate launch shapes and bin sets on one batched round of completed blocks. picks: list of
+    (SweepRun, block) whose pass 1 and learning are done (their set entries valid). Returns [(seconds, bins, shape)]
+    fastest first."""
+    from . import native as N
     sets1, sets2, groups = [], [], []
     for k, (run, b) in enumerate(picks):
         blk = run.live[b]
@@ -61,19 +70,40 @@ def tune_round(picks, max_bins=4, reps=3, device="cuda"):
     t1, t2 = D.RowSetTable(sets1, device), D.RowSetTable(sets2, device)
     sides = np.concatenate([g[2] for g in groups])
     out = []
-    for bins in candidates(sides, max_bins):
+    base = candidates(sides, 1)[0]
+    for shape in shapes:                 # launch shape first, on one bin of all sides
+        N.tune(**shape)
+        launches = D.batched_items(groups, base, device)
+        out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base, shape))
+    best_shape = min(out, key=lambda r: r[0])[2]
+    N.tune(**best_shape)
+    for bins in candidates(sides, max_bins)[1:]:
         launches = D.batched_items(groups, bins, device)
         t = _time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps)
-        out.append((t, bins))
-    out.sort()
+        out.append((t, bins, best_shape))
+    out.sort(key=lambda r: r[0])
     return out
 
 
-def save(device_name, bins, table):
+def save(device_name, table, workload):
     data = json.loads(TUNED.read_text()) if TUNED.exists() else {}
-    data[device_name] = {"bins": list(bins), "measured": [{"seconds": round(t, 5), "bins": list(b)}
-                                                          for t, b in table[:12]]}
+    t, bins, shape = table[0]
+    data[device_name] = {"bins": list(bins), "shape": shape, "workload": workload,
+                         "measured": [{"seconds": round(t_, 5), "bins": list(b), "shape": sh}
+                                      for t_, b, sh in table[:16]]}
     TUNED.write_text(json.dumps(data, indent=1) + "\n")
+
+
+def load_shape(device_name=None):
+    """Tuned launch shape of this device (xi_tune arguments), or None."""
+    if not TUNED.exists():
+        return None
+    try:
+        name = device_name or torch.cuda.get_device_name()
+    except Exception:
+        return None
+    entry = json.loads(TUNED.read_text()).get(name)
+    return entry.get("shape") if entry else None
 
 
 def load_bins(device_name=None):
@@ -118,9 +148,11 @@ def main():
         picks.append((run, b))
     table = tune_round(picks, args.max_bins)
     name = torch.cuda.get_device_name()
-    save(name, table[0][1], table)
-    print(json.dumps({"device": name, "best": list(table[0][1]), "seconds": round(table[0][0], 5),
-                      "worst": [round(table[-1][0], 5), list(table[-1][1])], "candidates": len(table)}))
+    save(name, table, args.workload)
+    print(json.dumps({"device": name, "best": {"bins": list(table[0][1]), "shape": table[0][2]},
+                      "seconds": round(table[0][0], 5), "worst": [round(table[-1][0], 5), list(table[-1][1]),
+                                                                  table[-1][2]], "candidates": len(table),
+                      "shapes": [{"seconds": round(t, 5), "shape": sh} for t, b, sh in table if len(b) == 1]}))
     for run in runs:
         run.close()
 
