@@ -43,8 +43,6 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
-# large shoebox arenas are freed and allocated block after block: segments that grow avoid fragmenting HBM
-os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 
 METRICS = {"config2-sweep": "integrated reflections/s (the 16M-pixel, 3600-frame sweep per step)",
            "config2-block": "integrated reflections/s (one 360-frame phi block of the 16M-pixel sweep per step)",

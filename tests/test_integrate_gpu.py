@@ -233,9 +233,10 @@ def test_integration_in_parts_under_a_memory_budget():
     """A device budget below the open blocks' buffers: each phi block is integrated in parts of consecutive phi
     (own profiles and widths), as XPG does when its host budget is short (its own test of split integration,
     tests/test_pipeline.py:146-177, asks for the same reflections and a small median |dI| / sigma). Here the
-    100-frame sweep goes in 8 parts of ~170 reflections: too few strong ones to adapt the widths, so pass 1 is the
-    one-pass run's bit for bit; the profiles are learnt from each part's few strong spots, so the profile-fitted
-    intensities move by a fraction of sigma (median < 0.25)."""
+    100-frame sweep goes in 8 parts of ~170 reflections: the first part's pass 1 uses the model's widths, as the
+    one-pass run does, bit for bit; later parts take the widths adapted by the parts before them and each part learns
+    its profiles from its own few strong spots, so the profile-fitted intensities move by a fraction of sigma
+    (median < 0.25)."""
     from xpg_b200 import memplan
     from xpg_b200.plan import IntegrationModel, plan_integration
     case = "config1"
@@ -253,8 +254,9 @@ def test_integration_in_parts_under_a_memory_budget():
     np.testing.assert_array_equal(a["hkl"], b["hkl"])
     ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
     assert ok.mean() > 0.9
+    first = res.plan.blocks_refl[0]                       # the first part: pass 1 with the model's widths, as one pass
     for k in ("isum", "vsum", "bg", "isum_raw"):
-        assert np.array_equal(a[k], b[k], equal_nan=True), k
+        assert np.array_equal(a[k][first], b[k][first], equal_nan=True), k
     d = np.abs(a["iprf"][ok] - b["iprf"][ok]) / np.sqrt(a["vprf"][ok])
     assert np.median(d) < 0.25
 
@@ -269,3 +271,27 @@ def test_gather_graph_and_overlap_identical(case, mode):
     b = _run(case, wedge_frames=8, **mode).refl
     for k in CHECK_F + ("n_over", "n_fg_masked", "isum_raw"):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
+
+
+def test_integration_in_passes_over_the_frames():
+    """A budget that even the 8-part split cannot meet: the blocks go in passes over the frames (XPG's grouping of
+    blocks m apart in phi); every reflection is integrated, and the first block's pass 1 is the one-pass run's."""
+    from xpg_b200 import memplan
+    from xpg_b200.plan import IntegrationModel, plan_integration
+    case = "adaptive"
+    z = G.load(case)
+    spec = G.case_inputs(case)[0]
+    edges = z["edges"]
+    p = plan_integration([spec.experiment()] * (len(edges) - 1), edges, IntegrationModel(spec.sigma_d, spec.sigma_m),
+                         float(z["dmin"]), 1e9, (1, spec.nframes), 0.05, spec.n_regions_xy, True, True)
+    one, _ = memplan.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, memplan.row_bytes(p), spec.nframes)
+    wedges = 3 * 32 * spec.ny * spec.nx * 4
+    a = _run(case).refl
+    res = _run(case, mem_budget=0.55 * one + wedges)
+    b = res.refl
+    assert len(res.memory.get("passes", [])) > 1
+    np.testing.assert_array_equal(a["hkl"], b["hkl"])
+    assert np.isfinite(b["iprf"]).sum() >= 0.99 * np.isfinite(a["iprf"]).sum()
+    ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
+    d = np.abs(a["iprf"][ok] - b["iprf"][ok]) / np.sqrt(a["vprf"][ok])
+    assert np.median(d) < 0.25

@@ -57,3 +57,18 @@ def test_split_blocks_matches_the_reference_rule():
     cuts = [0] + [int(np.searchsorted(c, c[-1] * f, side="right")) for f in (1 / 3, 2 / 3)] + [o.size]
     for k in range(3):
         np.testing.assert_array_equal(parts[k], np.sort(o[cuts[k]:cuts[k + 1]]))
+
+
+def test_passes_group_blocks_m_apart_when_parts_do_not_fit():
+    """Blocks whose boxes are deeper than the blocks themselves stay open together even in parts: then the blocks
+    go in passes over the frames, m apart in phi (XPG's `_plan_passes` grouping), the fewest that fit."""
+    p, exps, nf = _plan("adaptive")
+    w = M.row_bytes(p)
+    one, big = M.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, w, nf)
+    passes, pk = M.split_passes(p, w, nf, big)
+    assert len(passes) == 2 and sorted(sum(passes, [])) == [0, 1] and pk <= big
+    q, e, info = M.fit(p, exps, nf, 0, 0.55 * one)
+    assert "passes" in info and info["peak"] < one
+    assert sorted(sum(info["passes"], [])) == list(range(len(q.blocks_refl)))
+    q2, e2, info2 = M.fit(p, exps, nf, 0, 0.55 * one, allow_passes=False)
+    assert "passes" not in info2

@@ -28,17 +28,13 @@ import numpy as np
 import torch
 
 from . import device as D
+from . import memplan
 from .integrate import SweepRun
 
+
 def block_bytes(plan, rows):
-    """Device bytes a block holds while open: its shoebox arena (value + 3 encoding, rows aligned to 16 bytes), bin
-    counters, per-pixel pass-1 tables (img2, J, u1, u2 float32 and all_valid2), per-frame fz, per-row scalars and
-    pass-2 outputs."""
-    Dz = plan.Dz[rows].astype(np.int64)
-    bx = plan.bx[rows].astype(np.int64)
-    vox = ((Dz * bx * bx + 3) & ~3).sum()
-    pix = (bx * bx).sum()
-    return int(4 * vox + 4 * Dz[plan.fb[rows] > 1].sum() + 17 * pix + 4 * Dz.sum() + 400 * rows.size)
+    """Device bytes a block holds while open (memplan.row_bytes of its rows)."""
+    return int(memplan.row_bytes(plan)[rows].sum())
 
 
 def footprint(plan, n_frames, wedge_bytes, depth=3):
@@ -155,10 +151,11 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
             if served and job.arrivals is not None and clock() - t0 < job.arrivals[0]:
                 return                                       # the request has not arrived
             if i not in head:
+                if served:
+                    job.images.rereadable = False            # live frames arrive once: no second pass over them
                 run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, early_pass1=False,
                                device=device, verbose=False, mem_budget=budget, graphs=graphs, **job.kwargs)
-                wb = max(fb - fa + 1 for fa, fb in run.wedges) * run.src.ny * run.src.nx * 4
-                head[i] = (run, footprint(run.plan, run.wedges[-1][1], wb))
+                head[i] = (run, int(run.mem["peak"]))              # parts and passes included
             run, need = head[i]
             if active and used + need > budget:
                 return                                       # waits for memory to free up
@@ -183,6 +180,11 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 progressed = True
             if a.w >= len(a.run.wedges) and not a.pend and a.run.opened:
                 a.pend += a.run.remaining()
+            if (a.w >= len(a.run.wedges) and not a.pend and not a.run.opened and not a.run.live
+                    and a.run.pass_index + 1 < a.run.n_passes):
+                a.run.start_pass(a.run.pass_index + 1)       # blocks that did not fit in one pass over the frames
+                a.w = 0
+                progressed = True
         while any(a.pend for a in active):
             _round(active, bins, stats)
             progressed = True
@@ -193,7 +195,8 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 stats["latency"].append((a.i, w, now - float(a.job.arrivals[w]) if a.job.arrivals is not None else 0.0))
                 if on_wedge is not None:
                     on_wedge(a.i, w, now)
-        for a in [a for a in active if a.w >= len(a.run.wedges) and not a.pend and not a.run.opened]:
+        for a in [a for a in active if a.w >= len(a.run.wedges) and not a.pend and not a.run.opened
+                  and a.run.pass_index + 1 >= a.run.n_passes]:
             results[a.i] = a.run.result()
             a.run.close()
             used -= a.nbytes

@@ -112,6 +112,56 @@ class _UploadRing:
 _RING = _UploadRing()
 
 
+class BufferPool:
+    """Large device buffers kept across uses: the shoebox arenas of successive blocks (tens of GB each) and frame
+    wedges. The caching allocator splits and fragments such blocks when they are freed and allocated block after
+    block; here a request takes the smallest kept buffer that holds it (a view of its first elements), else a new one
+    allocated 5% larger than asked (so that later blocks of about the same size fit), and `give` returns it. A
+    buffer is given back only once no queued work uses it any more, or when the next user writes it on the same
+    stream (stream order)."""
+
+    SLACK = 1.05
+    KEEP = 3
+
+    def __init__(self):
+        self.free = {}                 # (device index, dtype) -> [tensor]
+
+    def take(self, n, dtype, device):
+        dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        key = (dev.index, dtype)
+        pool = self.free.setdefault(key, [])
+        fits = [t for t in pool if t.numel() >= n]
+        if fits:
+            t = min(fits, key=lambda x: x.numel())
+            pool.remove(t)
+            return t[:n]
+        size = max(int(n * self.SLACK), 1)
+        try:
+            return torch.empty(size, dtype=dtype, device=dev)[:n]
+        except torch.OutOfMemoryError:
+            pool.clear()                # the kept buffers are too small: let the allocator have their memory
+            torch.cuda.empty_cache()
+            return torch.empty(n, dtype=dtype, device=dev)
+
+    def give(self, t):
+        if t is None:
+            return
+        base = t._base if t._base is not None else t
+        key = (base.device.index, base.dtype)
+        pool = self.free.setdefault(key, [])
+        pool.append(base)
+        pool.sort(key=lambda x: -x.numel())
+        del pool[self.KEEP:]
+
+    def clear(self):
+        self.free.clear()
+
+
+POOL = BufferPool()
+
+
 def h2d(a, dtype=None, device="cuda"):
     """Host array -> device tensor on the current stream without blocking the host: staged through the upload ring
     and read by a kernel (large arrays: through torch's pinned staging and the copy engine). A pageable copy would

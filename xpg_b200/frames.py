@@ -771,6 +771,7 @@ class PackedFrames:
         self.resident = False
         self.depth = depth
         self.transfer = {}
+        self._buf = None
 
     @property
     def on_device(self):
@@ -787,8 +788,14 @@ class PackedFrames:
         return _PackedFeeder(self.store, self.first, wedges, oks, self.device, self.depth, self.transfer)
 
     def wedge(self, f_a, f_b, ok=None, stream=None):
+        """Frames f_a..f_b widened into the source's wedge buffer (reused wedge after wedge: the next wedge's unpack
+        is queued on the stream after the kernels that read this one)."""
+        from .device import POOL
         n = f_b - f_a + 1
-        d = torch.empty((n, self.ny, self.nx), dtype=torch.int32, device=self.device)
+        if self._buf is None or self._buf.numel() < n * self.ny * self.nx:
+            POOL.give(self._buf)
+            self._buf = POOL.take(n * self.ny * self.nx, torch.int32, self.device)
+        d = self._buf[:n * self.ny * self.nx].view(n, self.ny, self.nx)
         st = stream if stream is not None else torch.cuda.current_stream()
         self.store.unpack_frames(f_a - self.first, n, d, st, ok)
         return d, False
@@ -811,10 +818,16 @@ class GeneratedFrames:
         self.device = device
         self.resident = False
         self.hide_transfer = False
+        self._buf = None
 
     def wedge(self, f_a, f_b, ok=None, stream=None):
-        from .device import TIMER
-        d = torch.empty((f_b - f_a + 1, self.ny, self.nx), dtype=torch.int32, device=self.device)
+        """Frames f_a..f_b rendered into the source's wedge buffer (reused wedge after wedge, in stream order)."""
+        from .device import POOL, TIMER
+        n = f_b - f_a + 1
+        if self._buf is None or self._buf.numel() < n * self.ny * self.nx:
+            POOL.give(self._buf)
+            self._buf = POOL.take(n * self.ny * self.nx, torch.int32, self.device)
+        d = self._buf[:n * self.ny * self.nx].view(n, self.ny, self.nx)
         with TIMER.span("generate", 2):
             self.spots.render(f_a, f_b - f_a + 1, d, stream)
         return d, False

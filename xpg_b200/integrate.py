@@ -70,7 +70,7 @@ class _Block:
             pphi=rad(dv["phi"].index_select(0, pj)), pxs=pxs, Dz=p.Dz[rows], bx=p.bx[rows], nb=nb, device=device,
             sb_bias=3.0)
         self.grows = D.GatherRows(self.rowset, ix0, iy0, iz0, p.fb[rows], pxs, device)
-        self.arena = torch.zeros(max(self.rowset.n_vox, 1), dtype=torch.float32, device=device)
+        self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device).zero_()
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
         ident = bool((rows[1:] > rows[:-1]).all())         # local rows by global row: outputs leave in plan order
         order = None if ident else np.argsort(rows, kind="stable")
@@ -158,6 +158,13 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
             run.process(b)
         for b in run.remaining():
             run.process(b)
+        for k in range(1, run.n_passes):             # blocks that did not fit in one pass over the frames
+            run.start_pass(k)
+            for w in range(len(run.wedges)):
+                for b in run.feed(w):
+                    run.process(b)
+            for b in run.remaining():
+                run.process(b)
         return run.result()
     finally:
         run.close()
@@ -207,15 +214,16 @@ class SweepRun:
         # device memory: blocks split into parts of consecutive phi when their open buffers exceed the budget
         wedge_bytes = 0 if resident else 3 * W * src.ny * src.nx * 4
         limit = mem_budget if mem_budget is not None else memplan.budget(device)
-        self.plan, exp_blocks, self.mem = memplan.fit(p, exp_blocks, f_last, wedge_bytes, limit)
+        self.plan, exp_blocks, self.mem = memplan.fit(p, exp_blocks, f_last, wedge_bytes, limit,
+                                                      allow_passes=getattr(src, "rereadable", True))
         p = self.plan
         self.exp_blocks = exp_blocks
         self.refl = p.refl
         n = p.n
-        if verbose and self.mem["parts"] > 1:
+        if verbose and (self.mem["parts"] > 1 or "passes" in self.mem):
             log(f"  INTEGRATE: open shoebox buffers ~{self.mem['one'] / 2 ** 30:.1f} GB > the device budget "
-                f"{limit / 2 ** 30:.1f} GB: each phi block in {self.mem['parts']} parts, peak "
-                f"~{self.mem['peak'] / 2 ** 30:.1f} GB")
+                f"{limit / 2 ** 30:.1f} GB: each phi block in {self.mem['parts']} parts, "
+                f"{len(self.mem.get('passes', [1]))} passes over the frames, peak ~{self.mem['peak'] / 2 ** 30:.1f} GB")
         if verbose:
             log(f"  INTEGRATE: {p.info['n_predicted']} predicted reflections, box {p.box}x{p.box} px, sigma_D "
                 f"{model.sigma_d:.4f} sigma_M {model.sigma_m:.4f} deg; {p.info['n_wide']} wide in phi (> {MAX_DZ} "
@@ -240,7 +248,11 @@ class SweepRun:
             if p.blocks_refl[b].size:
                 k = np.searchsorted(read_fi, p.need_hi[b], "left")
                 self.eff_hi[b] = int(read_fi[min(k, len(read_fi) - 1)]) if len(read_fi) else -1
-        self.pending = sorted((b for b in range(nblocks) if p.blocks_refl[b].size), key=lambda b: p.need_lo[b])
+        # passes over the frames (memplan, when the open blocks do not fit even in parts): each reads every frame
+        self.passes = self.mem.get("passes") or [[b for b in range(nblocks) if p.blocks_refl[b].size]]
+        self.n_passes = len(self.passes)
+        self.pass_index = 0
+        self.pending = sorted(self.passes[0], key=lambda b: p.need_lo[b])
         self.opened, self.open_order = {}, []
         self.det_cache = {}
         self.bkg_template = bkg_template
@@ -403,6 +415,18 @@ class SweepRun:
                                      self.mask_t, ok_t[:nf] if ok_t is not None else None)
                 D.gather(fs, blk.grows, blk.sched(blk.w_gather[w]), blk.arena, blk.cnt)
 
+    def start_pass(self, k):
+        """Starts pass k over the frames (k >= 1; the blocks of the passes before it are all processed)."""
+        if self.opened or self.live:
+            raise RuntimeError("a pass starts after every block of the previous pass is processed")
+        self.pass_index = k
+        self.pending = sorted(self.passes[k], key=lambda b: self.plan.need_lo[b])
+        self.ok_off = 0
+        self._gg = None
+        if self.feeder is not None:
+            self.feeder.close()
+            self.feeder = self.src.feeder(self.wedges, self.oks)
+
     def remaining(self):
         """The open blocks left after the last wedge, in processing order."""
         out = [b for b in self.open_order if b in self.opened and b not in self.reported]
@@ -492,7 +516,8 @@ class SweepRun:
         return None
 
     def collect(self, b):
-        """The block's results to the host, into the run's output columns."""
+        """The block's results to the host, into the run's output columns; the block's arena goes back to the pool
+        (every kernel that reads it has run once the results are on the host)."""
         blk = self.live.pop(b)
         p1, rs = blk.p1, blk.rowset
         cols = {k: p1.t[k] for k in P1_OUT}
@@ -506,6 +531,9 @@ class SweepRun:
             self.out[k][dst] = v
         if self.fz_out is not None:
             self.fz_out[blk.rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
+        if self._gg is None or b not in self._gg.key:      # a captured gather graph may still name the arena
+            D.POOL.give(blk.arena)
+            blk.arena = None
         self.t_dev += time.time() - self.tg
 
     def result(self):
@@ -543,6 +571,11 @@ class SweepRun:
         if self.feeder is not None:
             self.feeder.close()
             self.feeder = None
+        self._gg = None
+        if self.src is not None and getattr(self.src, "_buf", None) is not None:
+            D.POOL.give(self.src._buf)
+            self.src._buf = None
+        D.POOL.clear()                        # the kept arenas go back to the allocator between runs
 
 
 ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")

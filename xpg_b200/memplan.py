@@ -20,17 +20,19 @@ DEVICE_FRACTION = 0.95       # share of the device memory free at the start that
 
 
 def row_bytes(plan):
-    """Device bytes of every row while its block is open: the shoebox (value + 3 floats, rows on 16 bytes), bin
-    counters of binned rows, the per-pixel pass-1 tables (img2, J, u1, u2, all_valid2), per-frame fz, per-row
-    scalars of both passes."""
+    """Device bytes of every row while its block is open: the shoebox (value + 3 floats, rows on 16 bytes, and the
+    buffer pool's 5% slack), bin counters of binned rows, the per-pixel pass-1 tables (img2, J, u1, u2,
+    all_valid2), per-frame fz, per-row scalars of both passes."""
     Dz = plan.Dz.astype(np.int64)
     bx = plan.bx.astype(np.int64)
-    return (4 * ((Dz * bx * bx + 3) & ~3) + np.where(plan.fb > 1, 4 * Dz, 0) + 17 * bx * bx + 4 * Dz + 400)
+    arena = 4 * ((Dz * bx * bx + 3) & ~3)
+    return (arena + arena // 20 + np.where(plan.fb > 1, 4 * Dz, 0) + 17 * bx * bx + 4 * Dz + 400)   # + the pool's 5%
 
 
 def budget(device="cuda"):
     """Bytes the run's shoebox buffers may use: XPG_INTEGRATE_MEM_GB (the reference's knob for the same buffers), else
-    DEVICE_FRACTION of the device memory free now (the caching allocator's free blocks counted as free)."""
+    DEVICE_FRACTION of the device memory free now (the caching allocator's free blocks and the buffer pool's kept
+    buffers counted as free)."""
     gb = os.environ.get("XPG_INTEGRATE_MEM_GB")
     if gb:
         return float(gb) * 2 ** 30
@@ -38,7 +40,10 @@ def budget(device="cuda"):
     dev = torch.device(device)
     if dev.index is None:
         dev = torch.device("cuda", torch.cuda.current_device())
-    free = torch.cuda.mem_get_info(dev)[0] + torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+    from .device import POOL
+    kept = sum(t.numel() * t.element_size() for (d, _), ts in POOL.free.items() if d == dev.index for t in ts)
+    free = (torch.cuda.mem_get_info(dev)[0] + torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+            + kept)
     return DEVICE_FRACTION * free
 
 
@@ -73,9 +78,11 @@ def split_blocks(blocks_refl, z, w_row, k):
     return parts, parent
 
 
-def fit(plan, exp_blocks, n_frames, wedge_bytes, limit):
+def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
     """The plan (and per-block experiments) whose open blocks fit `limit` bytes with the wedge buffers: unchanged
-    when it fits, else every block split into the fewest parts (2..8) that fit, or the split with the lowest peak.
+    when it fits, else every block split into the fewest parts (2..8) that fit, or the split with the lowest peak;
+    when that still does not fit (boxes deeper than a block: parts of a block stay open together) and the frames can
+    be read again (allow_passes), the blocks go in several passes over the frames (info["passes"]).
     Returns (plan, exp_blocks, info)."""
     w_row = row_bytes(plan)
     one, big = peak_bytes(plan.blocks_refl, plan.need_lo, plan.need_hi, w_row, n_frames)
@@ -93,8 +100,30 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit):
         if pk + wedge_bytes <= limit:
             break
     pk, k, parts, parent, lo, hi = best
-    if pk >= one:
-        return plan, exp_blocks, info
-    new = replace(plan, blocks_refl=parts, need_lo=lo, need_hi=hi)
-    info.update(peak=pk + wedge_bytes, parts=k, parent=parent)
-    return new, [exp_blocks[b] for b in parent], info
+    if pk < one:
+        plan = replace(plan, blocks_refl=parts, need_lo=lo, need_hi=hi)
+        exp_blocks = [exp_blocks[b] for b in parent]
+        info.update(peak=pk + wedge_bytes, parts=k, parent=parent)
+    if info["peak"] > limit and allow_passes:
+        passes, ppk = split_passes(plan, w_row, n_frames, limit - wedge_bytes)
+        if len(passes) > 1:
+            info.update(peak=ppk + wedge_bytes, passes=passes)
+    return plan, exp_blocks, info
+
+
+def split_passes(plan, w_row, n_frames, limit, max_passes=16):
+    """Passes over the frames, each integrating the blocks m apart in phi (XPG's grouping along phi,
+    `_plan_passes`, xpg/shoebox.py:134-196): the fewest passes whose open blocks fit `limit`, else the lowest peak.
+    Returns (passes: block lists, their peak)."""
+    blocks = [b for b in range(len(plan.blocks_refl)) if plan.blocks_refl[b].size]
+    best = None
+    for m in range(2, max_passes + 1):
+        passes = [[b for k, b in enumerate(blocks) if k % m == r] for r in range(m)]
+        passes = [q for q in passes if q]
+        pk = max(peak_bytes([plan.blocks_refl[b] for b in q], [plan.need_lo[b] for b in q],
+                            [plan.need_hi[b] for b in q], w_row, n_frames)[0] for q in passes)
+        if best is None or pk < best[1]:
+            best = (passes, pk)
+        if pk <= limit:
+            break
+    return best
