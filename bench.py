@@ -219,7 +219,7 @@ class Workload:
         from xpg_b200 import synth
         from xpg_b200.plan import plan_integration
         self.name, self.device = name, device
-        self.overlap = os.environ.get("XPG_BENCH_OVERLAP", "0") == "1"
+        self.overlap = os.environ.get("XPG_BENCH_OVERLAP", "1") == "1"      # gathers on a stream of their own
         (self.spec, self.exp, self.model, self.edges, self.n_frames,
          self.plan) = plan_workload(name, seed_offset, plan_integration)
         s = self.spec

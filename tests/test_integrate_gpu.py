@@ -254,7 +254,7 @@ def test_integration_in_parts_under_a_memory_budget():
     np.testing.assert_array_equal(a["hkl"], b["hkl"])
     ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
     assert ok.mean() > 0.9
-    first = res.plan.blocks_refl[0]                       # the first part: pass 1 with the model's widths, as one pass
+    first = res.plan.blocks_refl[res.block_order[0]]      # the first part processed: pass 1 with the model's widths
     for k in ("isum", "vsum", "bg", "isum_raw"):
         assert np.array_equal(a[k][first], b[k][first], equal_nan=True), k
     d = np.abs(a["iprf"][ok] - b["iprf"][ok]) / np.sqrt(a["vprf"][ok])

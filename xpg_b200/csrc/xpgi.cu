@@ -525,37 +525,28 @@ __device__ __forceinline__ void pass1_row(const XiDetector& det_g, const XiRows&
                 if (32 * w >= Dz) break;
                 const int zn = min(32, Dz - 32 * w);
                 const unsigned fw = fgw[w], nw = nbw[w];
-                const unsigned fgm = fg2 ? fw : 0u;       // foreground voxels of this column
-                unsigned rw = 0u;
+                // per voxel only its value's tests are taken (valid, recorded, overloaded bits) and the two sums it
+                // may join; the counts follow from the word's bit masks
+                unsigned vm = 0u, rm = 0u, om = 0u;
+                unsigned icm = fw & ~nw;                   // foreground frames not a neighbour's (shifted per batch)
+                unsigned bgm = ring ? ~nw : 0u;            // background voxels not a neighbour's (shifted per batch)
                 const float* col = (STAGED ? stage : sb) + (size_t)32 * w * P + p;
                 for (int t0 = 0; t0 < zn; t0 += kZBatch) {
                   float vv[kZBatch];                     // independent loads in flight before any is used
 #pragma unroll
                   for (int u = 0; u < kZBatch; ++u) vv[u] = t0 + u < zn ? col[(size_t)(t0 + u) * P] : 0.0f;
+                  unsigned bv = 0u, br = 0u, bo = 0u;
 #pragma unroll
                   for (int u = 0; u < kZBatch; ++u) {
-                    const int t = t0 + u;
-                    if (t >= zn) break;
+                    if (t0 + u >= zn) break;
                     const float v = vv[u] - R.sb_bias;
-                    if (STAGED) stage[(size_t)(32 * w + t) * P + p] = v;
-                    const bool valid = v >= 0.0f, recd = v > -2.5f;
-                    const bool fgzz = (fw >> t) & 1u, nbz = (nw >> t) & 1u, fg = (fgm >> t) & 1u;
-                    const bool clean = valid && !nbz;
-                    rw |= (unsigned)recd << t;
-                    if (fg) {
-                        t_over += (v == -2.0f);
-                        t_fgm += (!valid && recd);
-                        t_fgnb += nbz;
-                    }
-                    if (fgzz) {
-                        if (clean) {
-                            ic += v;
-                            ++in_;
-                        } else {
-                            okall = false;
-                        }
-                    }
-                    if (clean && ring) {                 // background (the ring excludes the foreground ellipse)
+                    if (STAGED) stage[(size_t)(32 * w + t0 + u) * P + p] = v;
+                    const bool valid = v >= 0.0f;
+                    bv |= (unsigned)valid << u;
+                    br |= (unsigned)(v > -2.5f) << u;
+                    bo |= (unsigned)(v == -2.0f) << u;
+                    if (valid && ((icm >> u) & 1u)) ic += v;
+                    if (valid && ((bgm >> u) & 1u)) {    // background (the ring excludes the foreground ellipse)
                         if (v <= clip_floor) {
                             cs0 += v;
                             ++cn0;
@@ -572,8 +563,20 @@ __device__ __forceinline__ void pass1_row(const XiDetector& det_g, const XiRows&
                         }
                     }
                   }
+                  vm |= bv << t0;
+                  rm |= br << t0;
+                  om |= bo << t0;
+                  icm >>= kZBatch;
+                  bgm >>= kZBatch;
                 }
-                recw[w] |= rw;
+                recw[w] |= rm;
+                const unsigned fgm = fg2 ? fw : 0u;     // foreground voxels of this column
+                t_over += __popc(fgm & om);
+                t_fgm += __popc(fgm & ~vm & rm);
+                t_fgnb += __popc(fgm & nw);
+                const unsigned clean_fg = fw & vm & ~nw; // foreground-frame voxels valid and not a neighbour's
+                in_ += __popc(clean_fg);
+                if (clean_fg != fw) okall = false;
             }
             double csd = (double)cs;
             if (cs >= 16777216.0f) {                     // float32 may have rounded: this column again in float64

@@ -121,7 +121,7 @@ class BufferPool:
     stream (stream order)."""
 
     SLACK = 1.05
-    KEEP = 3
+    KEEP = 2
 
     def __init__(self):
         self.free = {}                 # (device index, dtype) -> [tensor]
@@ -132,11 +132,11 @@ class BufferPool:
             dev = torch.device("cuda", torch.cuda.current_device())
         key = (dev.index, dtype)
         pool = self.free.setdefault(key, [])
-        fits = [t for t in pool if t.numel() >= n]
+        fits = [i for i, t in enumerate(pool) if t.numel() >= n]
         if fits:
-            t = min(fits, key=lambda x: x.numel())
-            pool.remove(t)
-            return t[:n]
+            i = min(fits, key=lambda j: pool[j].numel())
+            return pool.pop(i)[:n]
+        pool.clear()                    # kept buffers too small for this request: their memory goes back first
         size = max(int(n * self.SLACK), 1)
         try:
             return torch.empty(size, dtype=dtype, device=dev)[:n]
@@ -151,7 +151,8 @@ class BufferPool:
         base = t._base if t._base is not None else t
         key = (base.device.index, base.dtype)
         pool = self.free.setdefault(key, [])
-        pool.append(base)
+        if not any(x is base for x in pool):
+            pool.append(base)
         pool.sort(key=lambda x: -x.numel())
         del pool[self.KEEP:]
 
@@ -572,9 +573,9 @@ def batched_items(groups, bins=None, device="cuda"):
     if not cols:
         return []
     st, rw, bx, dz = (np.concatenate([c[k] for c in cols]) for k in range(4))
+    if int(bx.max()) > bins[-1]:                 # sides beyond the bins (tuned on another workload): one more bin
+        bins = bins + (int(bx.max()),)
     which = np.searchsorted(np.asarray(bins), bx, side="left")
-    if (which >= len(bins)).any():
-        raise ValueError("a box side beyond the largest size bin")
     out = []
     for k in np.unique(which):
         m = np.flatnonzero(which == k)

@@ -564,6 +564,7 @@ class SweepRun:
         res.block_params = self.block_params
         res.block_widths = self.block_widths  # (sigma_D, sigma_M in radians, rocking-curve weights) of each pass
         res.plan = self.plan                  # the plan integrated (blocks split in parts when memory was short)
+        res.block_order = list(self.processed)  # blocks (of res.plan) in the order they were processed
         res.memory = self.mem
         return res
 
