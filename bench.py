@@ -700,13 +700,14 @@ def served_bench(args):
     from xpg_b200.csrc import build
     if build.stale():
         build.build()
-    specs = synth.config5(nframes=args.served_frames)
+    specs = synth.config5(nframes=args.served_frames, n_sweeps=args.served_sweeps)
     rng = np.random.default_rng(55)
     wedge = 50
+    rate = float(args.served_rate)
     jobs = _jobs_of(specs, wedge)
     for j in jobs:
         nw = len(range(1, j.kwargs["frames"][1] + 1, wedge))
-        j.arrivals = np.cumsum(rng.exponential(wedge / 500.0, nw))
+        j.arrivals = np.cumsum(rng.exponential(wedge / rate, nw))
     run_jobs(_jobs_of(specs[:1], wedge), bins=args.bins)           # warm-up: kernels loaded, allocator primed
     torch.cuda.synchronize()
     res, stats = run_jobs(jobs, bins=args.bins, served=True)
@@ -715,7 +716,7 @@ def served_bench(args):
     last_arrival = max(float(j.arrivals[-1]) for j in jobs)
     line = {"metric": "served: wedge-to-intensities latency and sustained reflections/s (config 5)", "unit": "s",
             "p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4),
-            "max": round(float(lat.max()), 4), "wedge_acquisition_s": wedge / 500.0,
+            "max": round(float(lat.max()), 4), "wedge_acquisition_s": wedge / rate, "frame_rate_hz": rate,
             "sustained_refl_per_s": round(n / stats["seconds"], 1), "seconds": round(stats["seconds"], 3),
             "last_arrival_s": round(last_arrival, 3), "wedges": int(lat.size), "reflections": n,
             "sweeps": [{"frames": s.nframes, "cell": s.space_group, "reflections": len(r.refl["x"])}
@@ -851,6 +852,8 @@ def main():
     ap.add_argument("--bins", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
                     help="size bins (box sides) of the batched pass launches, e.g. 17,31,55,97")
     ap.add_argument("--served-frames", type=int, default=720, help="frames per sweep of the served workload")
+    ap.add_argument("--served-rate", type=float, default=500.0, help="frames per second of each served sweep")
+    ap.add_argument("--served-sweeps", type=int, default=4, help="concurrent sweeps of the served workload")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

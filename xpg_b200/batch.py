@@ -168,8 +168,9 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
             active.append(a)
             stats["peak_bytes"] = max(stats["peak_bytes"], used)
 
+    waiting = []                                             # (job, wedge, event, arrival) of fed wedges
     admit()
-    while active or queue:
+    while active or queue or waiting:
         progressed = False
         fed = []
         for a in active:
@@ -189,12 +190,23 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
             _round(active, bins, stats)
             progressed = True
         if served and fed:
-            torch.cuda.synchronize()
-            now = clock() - t0
+            # a wedge is done when the work queued for it (its gathers, and the blocks it completed, whose results
+            # are on the host already) has run: an event after it, polled without stopping the loop
             for a, w in fed:
-                stats["latency"].append((a.i, w, now - float(a.job.arrivals[w]) if a.job.arrivals is not None else 0.0))
-                if on_wedge is not None:
-                    on_wedge(a.i, w, now)
+                ev = torch.cuda.Event()
+                ev.record()
+                waiting.append((a.i, w, ev, float(a.job.arrivals[w]) if a.job.arrivals is not None else 0.0))
+        if waiting:
+            now = clock() - t0
+            left = []
+            for i, w, ev, arr in waiting:
+                if ev.query():
+                    stats["latency"].append((i, w, now - arr))
+                    if on_wedge is not None:
+                        on_wedge(i, w, now)
+                else:
+                    left.append((i, w, ev, arr))
+            waiting[:] = left
         for a in [a for a in active if a.w >= len(a.run.wedges) and not a.pend and not a.run.opened
                   and a.run.pass_index + 1 >= a.run.n_passes]:
             results[a.i] = a.run.result()

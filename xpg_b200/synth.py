@@ -383,7 +383,7 @@ class DeviceSpots:
     table. The noise of a spot's pixels is keyed by the spot's index in the table and the frame: any partition of the
     frames into wedges renders the same frames."""
 
-    BUCKET = 8
+    BUCKET = 32
 
     def __init__(self, spec: SweepSpec, table, device="cuda"):
         import torch
@@ -397,10 +397,10 @@ class DeviceSpots:
         n_b = int(np.ceil((spec.nframes + 1) / self.BUCKET)) + 1
         lo, hi = np.clip(lo, 0, n_b - 1), np.clip(hi, 0, n_b - 1)
         cnt = hi - lo + 1
-        idx = np.repeat(np.arange(z.size, dtype=np.int64), cnt)
-        bk = np.repeat(lo, cnt) + (np.arange(idx.size) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+        idx = np.repeat(np.arange(z.size, dtype=np.int32), cnt)
+        bk = (np.repeat(lo, cnt) + (np.arange(idx.size) - np.repeat(np.cumsum(cnt) - cnt, cnt))).astype(np.int32)
         o = np.argsort(bk, kind="stable")
-        self.idx = idx[o].astype(np.int32)
+        self.idx = idx[o]
         self.start = np.searchsorted(bk[o], np.arange(n_b + 1))
         self.device = device
         self.bg = (spec.background, spec.ramp, float(g.orgx), float(g.orgy),
