@@ -111,8 +111,11 @@ class _Block:
             return o, parts[-1].size
         self.w_gather, self.w_early = {}, {}
         acc = np.zeros(0, np.int64)
+        first = int(self.z_lo.min()) if self.z_lo.size else 0
         for w, (fa, fb) in enumerate(wedges):
             fi_a, fi_b = fa - 1, fb - 1
+            if fi_b < first or fi_a > eff_hi:              # wedges before or after the block's frames
+                continue
             if eff_hi >= fi_a:
                 hi = min(fi_b, eff_hi)
                 loc = self.by_tile[(self.z_lo_t <= hi) & (self.z_hi_t >= fi_a)]     # in gather (tile) order
