@@ -644,15 +644,17 @@ def batched_bench(args):
     from xpg_b200.integrate import integrate
     if build.stale():
         build.build()
+    from xpg_b200 import memplan
     specs = synth.config4()
     jobs = _jobs_of(specs, WEDGE_FRAMES)
+    budget = memplan.budget()          # one device budget for both forms: the same parts and passes, the same results
 
     def plain():
-        return [integrate(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, verbose=False, **j.kwargs)
-                for j in jobs]
+        return [integrate(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, verbose=False, mem_budget=budget,
+                          **j.kwargs) for j in jobs]
 
     def batched():
-        return run_jobs(jobs, bins=args.bins)
+        return run_jobs(jobs, budget_bytes=budget, bins=args.bins)
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -681,7 +683,10 @@ def batched_bench(args):
             "seconds": {"plain": [round(t, 3) for t in tp], "batched": [round(t, 3) for t in tb]},
             "reflections": n, "same_results": bool(same),
             "sweeps": [{"frames": s.nframes, "detector": [s.nx, s.ny], "cell": s.space_group,
-                        "sigma_m": round(s.sigma_m, 3), "reflections": len(r.refl["x"])} for s, r in zip(specs, rp)],
+                        "sigma_m": round(s.sigma_m, 3), "reflections": len(r.refl["x"]),
+                        "block_parts": int(r.memory["parts"]), "passes": len(r.memory.get("passes", [1])),
+                        "planned_peak_gib": round(r.memory["peak"] / 2 ** 30, 1)} for s, r in zip(specs, rp)],
+            "budget_gib": round(budget / 2 ** 30, 1),
             "batched_stats": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "pass1_launches",
                                                                       "peak_bytes")},
             "data": "synthetic, frames rendered on the device inside the timed region (both forms)"}
@@ -708,18 +713,30 @@ def served_bench(args):
     for j in jobs:
         nw = len(range(1, j.kwargs["frames"][1] + 1, wedge))
         j.arrivals = np.cumsum(rng.exponential(wedge / rate, nw))
-    run_jobs(_jobs_of(specs[:1], wedge), bins=args.bins)           # warm-up: kernels loaded, allocator primed
+    budget = args.served_budget_gb * 2 ** 30
+    slots = len(jobs)
+    warm = _jobs_of(specs[:1], wedge)
+    warm[0].images.rereadable = False
+    run_jobs(warm, budget_bytes=budget, bins=args.bins, slots=slots)    # warm-up: kernels loaded, allocator primed
     torch.cuda.synchronize()
-    res, stats = run_jobs(jobs, bins=args.bins, served=True)
+    res, stats = run_jobs(jobs, budget_bytes=budget, bins=args.bins, served=True, slots=slots)
     lat = np.array([x[2] for x in stats["latency"]])
+    comp = np.array([(x[0], x[1]) in stats["completing"] for x in stats["latency"]], bool)
     n = sum(len(r.refl["x"]) for r in res)
     last_arrival = max(float(j.arrivals[-1]) for j in jobs)
+
+    def pct(v):
+        return {"p50": round(float(np.percentile(v, 50)), 4), "p99": round(float(np.percentile(v, 99)), 4),
+                "n": int(v.size)} if v.size else None
     line = {"metric": "served: wedge-to-intensities latency and sustained reflections/s (config 5)", "unit": "s",
             "p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4),
             "max": round(float(lat.max()), 4), "wedge_acquisition_s": wedge / rate, "frame_rate_hz": rate,
             "sustained_refl_per_s": round(n / stats["seconds"], 1), "seconds": round(stats["seconds"], 3),
             "last_arrival_s": round(last_arrival, 3), "wedges": int(lat.size), "reflections": n,
-            "sweeps": [{"frames": s.nframes, "cell": s.space_group, "reflections": len(r.refl["x"])}
+            "latency_block_completing": pct(lat[comp]), "latency_other": pct(lat[~comp]),
+            "budget_gib": args.served_budget_gb, "slots": slots,
+            "sweeps": [{"frames": s.nframes, "cell": s.space_group, "reflections": len(r.refl["x"]),
+                        "block_parts": int(r.memory["parts"]), "planned_peak_gib": round(r.memory["peak"] / 2 ** 30, 1)}
                        for s, r in zip(specs, res)],
             "scheduler": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "peak_bytes", "waits")},
             "data": "synthetic; wedges rendered on the device at their arrival"}
@@ -854,6 +871,8 @@ def main():
     ap.add_argument("--served-frames", type=int, default=720, help="frames per sweep of the served workload")
     ap.add_argument("--served-rate", type=float, default=500.0, help="frames per second of each served sweep")
     ap.add_argument("--served-sweeps", type=int, default=4, help="concurrent sweeps of the served workload")
+    ap.add_argument("--served-budget-gb", type=float, default=80.0,
+                    help="device memory (GiB) the served sweeps are admitted under, one slot per sweep")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

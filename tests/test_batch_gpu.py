@@ -79,3 +79,29 @@ def test_served_results_equal_alone_and_latency_recorded():
     assert all(lat >= 0 for _, _, lat in stats["latency"])
     for c, a, b in zip(CASES, alone, res):
         _same(a, b, c)
+
+
+def test_served_slots_plan_each_sweep_in_its_share():
+    """slots: every sweep is planned for budget / slots (its blocks in parts when its open blocks exceed that share;
+    live frames take no second pass), so that the sweeps run together; each result is the same as the sweep
+    integrated alone under that share."""
+    from xpg_b200.batch import job_footprint, serve
+    from xpg_b200.integrate import integrate
+    cases = ("adaptive", "crowded")
+    jobs = [_job(c) for c in cases]
+    need = [job_footprint(j) for j in jobs]
+    share = 0.7 * min(need)
+    for j in jobs:
+        j.images.rereadable = False
+    alone = [integrate(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, verbose=False, mem_budget=share,
+                       **j.kwargs) for j in jobs]
+    assert any(a.memory["parts"] > 1 for a in alone)
+    rng = np.random.default_rng(5)
+    for k, j in enumerate(jobs):
+        nw = len(range(1, j.kwargs["frames"][1] + 1, j.kwargs["wedge_frames"]))
+        j.arrivals = 0.005 * k + np.cumsum(rng.exponential(0.004, nw))
+    res, stats = serve(jobs, budget_bytes=2 * share, slots=2)
+    assert stats["admitted_at"][1] <= j.arrivals[0] + 0.5            # both sweeps ran at once
+    for c, a, b in zip(cases, alone, res):
+        assert b.memory["parts"] == a.memory["parts"] and "passes" not in b.memory
+        _same(a, b, c)

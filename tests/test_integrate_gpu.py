@@ -233,9 +233,9 @@ def test_integration_in_parts_under_a_memory_budget():
     """A device budget below the open blocks' buffers: each phi block is integrated in parts of consecutive phi
     (own profiles and widths), as XPG does when its host budget is short (its own test of split integration,
     tests/test_pipeline.py:146-177, asks for the same reflections and a small median |dI| / sigma). Here the
-    100-frame sweep goes in 8 parts of ~170 reflections, each with the widths adapted by the parts before it and the
-    profiles learnt from its own few strong spots: summation intensities move by a small fraction of sigma (median
-    < 0.1), profile-fitted ones by more (median < 0.35)."""
+    100-frame sweep's single block goes in parts (with passes over the frames where the parts overlap), each with
+    the widths adapted by the parts before it and the profiles learnt from its own strong spots: summation
+    intensities move by a small fraction of sigma (median < 0.1), profile-fitted ones by more (median < 0.35)."""
     from xpg_b200 import memplan
     from xpg_b200.plan import IntegrationModel, plan_integration
     case = "config1"
@@ -251,7 +251,7 @@ def test_integration_in_parts_under_a_memory_budget():
     b = res.refl
     assert res.memory["parts"] > 1 and len(res.profiles) == res.memory["parts"]
     np.testing.assert_array_equal(a["hkl"], b["hkl"])
-    ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0)
+    ok = np.isfinite(a["iprf"]) & np.isfinite(b["iprf"]) & (a["vprf"] > 0) & (a["vsum"] > 0)
     assert ok.mean() > 0.9
     ds = np.abs(a["isum"][ok] - b["isum"][ok]) / np.sqrt(a["vsum"][ok])
     assert np.median(ds) < 0.1
@@ -272,9 +272,9 @@ def test_gather_graph_and_overlap_identical(case, mode):
 
 
 def test_integration_in_passes_over_the_frames():
-    """A budget that even the 8-part split cannot meet: the blocks go in passes over the frames (XPG's grouping of
-    blocks m apart in phi, here of the blocks' parts); every reflection is integrated, the same reflections as one
-    pass, profile-fitted intensities within a fraction of sigma."""
+    """A budget below the two open blocks: the blocks go in passes over the frames (XPG's grouping of blocks m apart
+    in phi); every reflection is integrated, the same reflections as one pass, profile-fitted intensities within a
+    fraction of sigma."""
     from xpg_b200 import memplan
     from xpg_b200.plan import IntegrationModel, plan_integration
     case = "adaptive"

@@ -30,8 +30,8 @@ def test_fit_splits_blocks_into_parts_of_consecutive_phi():
     p, exps, nf = _plan("adaptive")
     w = M.row_bytes(p)
     one, big = M.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, w, nf)
-    q, e, info = M.fit(p, exps, nf, 0, 0.6 * one)
-    assert info["parts"] >= 2 and info["peak"] < one
+    q, e, info = M.fit(p, exps, nf, 0, 0.6 * one, allow_passes=False)     # frames read once: parts only
+    assert info["parts"] >= 2 and info["peak"] < one and "passes" not in info
     assert len(e) == len(q.blocks_refl) == len(info["parent"])
     rows = np.concatenate(q.blocks_refl)
     assert np.array_equal(np.sort(rows), np.arange(p.n))               # every row in exactly one part
@@ -59,16 +59,61 @@ def test_split_blocks_matches_the_reference_rule():
         np.testing.assert_array_equal(parts[k], np.sort(o[cuts[k]:cuts[k + 1]]))
 
 
-def test_passes_group_blocks_m_apart_when_parts_do_not_fit():
-    """Blocks whose boxes are deeper than the blocks themselves stay open together even in parts: then the blocks
-    go in passes over the frames, m apart in phi (XPG's `_plan_passes` grouping), the fewest that fit."""
+def test_passes_group_blocks_m_apart():
+    """Blocks open together that do not fit go in passes over the frames, m apart in phi (XPG's `_plan_passes`
+    grouping), the fewest that fit, before any block is split (xpg/integrate.py:598-622)."""
     p, exps, nf = _plan("adaptive")
     w = M.row_bytes(p)
     one, big = M.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, w, nf)
-    passes, pk = M.split_passes(p, w, nf, big)
+    passes, pk = M.split_passes(p.blocks_refl, p.need_lo, p.need_hi, [0, 0], w, nf, big)
     assert len(passes) == 2 and sorted(sum(passes, [])) == [0, 1] and pk <= big
     q, e, info = M.fit(p, exps, nf, 0, 0.55 * one)
     assert "passes" in info and info["peak"] < one
+    assert info["parts"] == 1 and q is p          # XPG's order: whole blocks in passes before any split
     assert sorted(sum(info["passes"], [])) == list(range(len(q.blocks_refl)))
     q2, e2, info2 = M.fit(p, exps, nf, 0, 0.55 * one, allow_passes=False)
     assert "passes" not in info2
+
+
+def test_passes_over_parts_when_rows_wide_in_phi_keep_every_part_open():
+    """One phi block whose rows include some wide in phi (binned boxes spanning the whole sweep): every part of the
+    block then reaches from the first frame to the last, so no split lowers the peak; the parts go in passes over
+    the frames instead, the fewest parts whose passes fit, every row in exactly one part of one pass."""
+    from dataclasses import replace
+    p, exps, nf = _plan("config1")
+    assert len(p.blocks_refl) == 1
+    zs, ze = p.zstart.copy(), p.zend.copy()
+    z = p.refl["z"]
+    o = np.argsort(z, kind="stable")
+    wide = o[::50]                                              # a few rows in every part span the sweep
+    zs[wide], ze[wide] = 0, nf - 1
+    p = replace(p, zstart=zs, zend=ze, need_lo=[0], need_hi=[nf - 1])
+    w = M.row_bytes(p)
+    one, _ = M.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, w, nf)
+    parts, parent = M.split_blocks(p.blocks_refl, z, w, 8)
+    lo = [int(zs[r].min()) for r in parts]
+    hi = [int(ze[r].max()) for r in parts]
+    assert M.peak_bytes(parts, lo, hi, w, nf)[0] == one                # parts alone do not help
+    q, e, info = M.fit(p, exps, nf, 0, 0.6 * one)
+    assert info["parts"] >= 2 and len(info["passes"]) >= 2 and info["peak"] <= 0.6 * one
+    assert sorted(sum(info["passes"], [])) == list(range(len(q.blocks_refl)))
+    rows = np.concatenate(q.blocks_refl)
+    assert np.array_equal(np.sort(rows), np.arange(p.n))
+    q2, e2, info2 = M.fit(p, exps, nf, 0, 0.6 * one, allow_passes=False)
+    assert "passes" not in info2 and info2["parts"] == 1          # no split lowers the peak: the plan stays whole
+
+
+def test_passes_by_lattice_first():
+    """Blocks of two lattices over the same frames: the first pass grouping tried after one pass is by lattice
+    (xpg/shoebox.py:163-170), then m apart in phi within each lattice."""
+    rng = np.random.default_rng(3)
+    blocks = [np.arange(10 * b, 10 * b + 10) for b in range(6)]          # lattice 0: blocks 0-2, lattice 1: 3-5
+    lo = [0, 100, 200, 0, 100, 200]
+    hi = [150, 250, 299, 150, 250, 299]
+    w = rng.uniform(1, 2, 60)
+    one = M.peak_bytes(blocks, lo, hi, w, 300)[0]
+    passes, pk = M.split_passes(blocks, lo, hi, [0, 0, 0, 1, 1, 1], w, 300, 0.6 * one)
+    assert passes == [[0, 1, 2], [3, 4, 5]] and pk <= 0.6 * one
+    passes, pk = M.split_passes(blocks, lo, hi, [0, 0, 0, 1, 1, 1], w, 300, 0.3 * one)
+    assert len(passes) == 4 and sorted(sum(passes, [])) == list(range(6))
+    assert all(len({b // 3 for b in q}) == 1 for q in passes)           # each pass holds one lattice

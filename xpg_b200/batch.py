@@ -123,17 +123,21 @@ def _round(active, bins, stats):
 
 
 def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, clock=time.perf_counter,
-             on_wedge=None, max_active=None, graphs=True):
+             on_wedge=None, max_active=None, graphs=True, slots=None):
     """Integrates `jobs` (list of Job) together; returns (results in job order, stats). served: each wedge is fed no
     earlier than its arrival time (job.arrivals, seconds after the start) and the latency of every wedge (from its
     arrival to the completion of everything it triggered: its gathers and, when it completes blocks, their
     intensities on the host) is recorded in stats["latency"]. graphs: each sweep's per-wedge gathers replayed from
-    a CUDA graph (captured once per set of open blocks)."""
+    a CUDA graph (captured once per set of open blocks). slots: each sweep is planned (blocks in parts, memplan.fit)
+    for budget_bytes / slots, so that `slots` sweeps run at once; by default each is planned for the whole budget
+    and sweeps wait for the memory the running ones hold."""
     budget = budget_bytes if budget_bytes is not None else int(0.8 * torch.cuda.mem_get_info(device)[0])
+    plan_budget = budget / slots if slots else budget
     queue = list(range(len(jobs)))
     active, results = [], [None] * len(jobs)
     used = 0
-    stats = dict(rounds=0, blocks=0, pass1_launches=0, latency=[], admitted_at={}, peak_bytes=0, waits=0)
+    stats = dict(rounds=0, blocks=0, pass1_launches=0, latency=[], admitted_at={}, peak_bytes=0, waits=0,
+                 completing=set())
     t0 = clock()
 
     def arrived(a, w):
@@ -154,7 +158,7 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 if served:
                     job.images.rereadable = False            # live frames arrive once: no second pass over them
                 run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, early_pass1=False,
-                               device=device, verbose=False, mem_budget=budget, graphs=graphs, **job.kwargs)
+                               device=device, verbose=False, mem_budget=plan_budget, graphs=graphs, **job.kwargs)
                 head[i] = (run, int(run.mem["peak"]))              # parts and passes included
             run, need = head[i]
             if active and used + need > budget:
@@ -175,7 +179,10 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
         fed = []
         for a in active:
             if a.w < len(a.run.wedges) and arrived(a, a.w):
-                a.pend += a.run.feed(a.w)
+                got = a.run.feed(a.w)
+                if got:
+                    stats["completing"].add((a.i, a.w))     # the wedge completed blocks: its latency has their passes
+                a.pend += got
                 fed.append((a, a.w))
                 a.w += 1
                 progressed = True
@@ -230,6 +237,7 @@ def integrate_batch(jobs, budget_bytes=None, bins=None, device="cuda"):
     return res
 
 
-def serve(jobs, budget_bytes=None, bins=None, device="cuda"):
-    """Request loop over jobs whose wedges arrive at job.arrivals: (results, stats) with the per-wedge latency."""
-    return run_jobs(jobs, budget_bytes, bins, device, served=True)
+def serve(jobs, budget_bytes=None, bins=None, device="cuda", slots=None):
+    """Request loop over jobs whose wedges arrive at job.arrivals: (results, stats) with the per-wedge latency.
+    slots: sweeps planned to run at once within budget_bytes (run_jobs)."""
+    return run_jobs(jobs, budget_bytes, bins, device, served=True, slots=slots)

@@ -115,12 +115,14 @@ _RING = _UploadRing()
 class BufferPool:
     """Large device buffers kept across uses: the shoebox arenas of successive blocks (tens of GB each) and frame
     wedges. The caching allocator splits and fragments such blocks when they are freed and allocated block after
-    block; here a request takes the smallest kept buffer that holds it (a view of its first elements), else a new one
-    allocated 5% larger than asked (so that later blocks of about the same size fit), and `give` returns it. A
-    buffer is given back only once no queued work uses it any more, or when the next user writes it on the same
-    stream (stream order)."""
+    block; here a request takes the smallest kept buffer that holds it (a view of its first elements) if that is at
+    most FIT times the request (a small block holding a large buffer would leave the next large block to allocate
+    anew, beyond what the memory plan counts), else a new one allocated SLACK larger than asked (so that later blocks
+    of about the same size fit), and `give` returns it. A buffer is given back only once no queued work uses it any
+    more, or when the next user writes it on the same stream (stream order)."""
 
     SLACK = 1.05
+    FIT = 1.3
     KEEP = 2
 
     def __init__(self):
@@ -128,20 +130,20 @@ class BufferPool:
 
     def take(self, n, dtype, device):
         dev = torch.device(device)
-        if dev.index is None:
+        if dev.type == "cuda" and dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
         key = (dev.index, dtype)
         pool = self.free.setdefault(key, [])
-        fits = [i for i, t in enumerate(pool) if t.numel() >= n]
+        fits = [i for i, t in enumerate(pool) if n <= t.numel() <= self.FIT * n + 4096]
         if fits:
             i = min(fits, key=lambda j: pool[j].numel())
             return pool.pop(i)[:n]
-        pool.clear()                    # kept buffers too small for this request: their memory goes back first
+        pool[:] = [t for t in pool if t.numel() > n]     # kept buffers too small for this request: memory back first
         size = max(int(n * self.SLACK), 1)
         try:
             return torch.empty(size, dtype=dtype, device=dev)[:n]
         except torch.OutOfMemoryError:
-            pool.clear()                # the kept buffers are too small: let the allocator have their memory
+            pool.clear()                # the kept buffers: let the allocator have their memory
             torch.cuda.empty_cache()
             return torch.empty(n, dtype=dtype, device=dev)
 

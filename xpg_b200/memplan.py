@@ -79,51 +79,77 @@ def split_blocks(blocks_refl, z, w_row, k):
 
 
 def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
-    """The plan (and per-block experiments) whose open blocks fit `limit` bytes with the wedge buffers: unchanged
-    when it fits, else every block split into the fewest parts (2..8) that fit, or the split with the lowest peak;
-    when that still does not fit (boxes deeper than a block: parts of a block stay open together) and the frames can
-    be read again (allow_passes), the blocks go in several passes over the frames (info["passes"]).
-    Returns (plan, exp_blocks, info)."""
+    """The plan (and per-block experiments) whose open blocks fit `limit` bytes with the wedge buffers, in XPG's
+    order (xpg/integrate.py:598-622): unchanged when one pass over the frames fits; else, when the frames can be read
+    again (allow_passes), the whole blocks in several passes over the frames (`split_passes`); else every block split
+    into the fewest parts of consecutive phi (2..8) that fit, each split with its own passes (allow_passes), or the
+    split with the lowest peak when none fits and it is below the whole blocks'. Returns (plan, exp_blocks, info);
+    info["passes"]: the block lists of the passes when there are several."""
     w_row = row_bytes(plan)
     one, big = peak_bytes(plan.blocks_refl, plan.need_lo, plan.need_hi, w_row, n_frames)
     info = dict(peak=one + wedge_bytes, one=one + wedge_bytes, parts=1, budget=limit)
     if limit is None or one + wedge_bytes <= limit:
+        return plan, exp_blocks, info
+    room = limit - wedge_bytes
+    lat = plan.refl.get("lattice")
+
+    def passes_of(blocks, lo, hi):
+        lattice = [int(lat[r[0]]) if lat is not None and r.size else 0 for r in blocks]
+        return split_passes(blocks, lo, hi, lattice, w_row, n_frames, room) if allow_passes else ([], None)
+
+    base, base_pk = passes_of(plan.blocks_refl, plan.need_lo, plan.need_hi)
+    whole = base_pk if base_pk is not None else one
+    if base_pk is not None and base_pk <= room:
+        info.update(peak=base_pk + wedge_bytes, passes=base)
         return plan, exp_blocks, info
     best = None
     for k in range(2, BLOCK_PARTS_MAX + 1):
         parts, parent = split_blocks(plan.blocks_refl, plan.refl["z"], w_row, k)
         lo = [int(plan.zstart[r].min()) for r in parts]
         hi = [int(plan.zend[r].max()) for r in parts]
-        pk, _ = peak_bytes(parts, lo, hi, w_row, n_frames)
+        passes, pk = passes_of(parts, lo, hi)
+        if pk is None:
+            pk = peak_bytes(parts, lo, hi, w_row, n_frames)[0]
         if best is None or pk < best[0]:
-            best = (pk, k, parts, parent, lo, hi)
-        if pk + wedge_bytes <= limit:
+            best = (pk, k, parts, parent, lo, hi, passes)
+        if pk <= room:
             break
-    pk, k, parts, parent, lo, hi = best
-    if pk < one:
+    pk, k, parts, parent, lo, hi, passes = best
+    if pk < whole:
         plan = replace(plan, blocks_refl=parts, need_lo=lo, need_hi=hi)
         exp_blocks = [exp_blocks[b] for b in parent]
         info.update(peak=pk + wedge_bytes, parts=k, parent=parent)
-    if info["peak"] > limit and allow_passes:
-        passes, ppk = split_passes(plan, w_row, n_frames, limit - wedge_bytes)
         if len(passes) > 1:
-            info.update(peak=ppk + wedge_bytes, passes=passes)
+            info["passes"] = passes
+    elif base_pk is not None and base_pk < one:
+        info.update(peak=base_pk + wedge_bytes, passes=base)
     return plan, exp_blocks, info
 
 
-def split_passes(plan, w_row, n_frames, limit, max_passes=16):
-    """Passes over the frames, each integrating the blocks m apart in phi (XPG's grouping along phi,
-    `_plan_passes`, xpg/shoebox.py:134-196): the fewest passes whose open blocks fit `limit`, else the lowest peak.
-    Returns (passes: block lists, their peak)."""
-    blocks = [b for b in range(len(plan.blocks_refl)) if plan.blocks_refl[b].size]
-    best = None
-    for m in range(2, max_passes + 1):
-        passes = [[b for k, b in enumerate(blocks) if k % m == r] for r in range(m)]
+def split_passes(blocks, need_lo, need_hi, lattice, w_row, n_frames, limit, max_passes=16):
+    """Passes over the frames whose open blocks fit `limit` bytes, XPG's candidates in its order (`_plan_passes`,
+    xpg/shoebox.py:134-183): one pass, then by lattice (blocks of other lattices cover the same frames), then within
+    each lattice the blocks m apart in phi; the first that fits, else the fewest passes within 5% of the lowest peak.
+    blocks: row lists (empty ones take no pass). Returns (passes: block index lists in phi order, their peak)."""
+    order = sorted((b for b in range(len(blocks)) if blocks[b].size), key=lambda b: need_lo[b])
+    lat = [lattice[b] for b in order]
+    lats = sorted(set(lat))
+    rank, seen = [], {}
+    for l_ in lat:
+        rank.append(seen.get(l_, 0))
+        seen[l_] = rank[-1] + 1
+    cands = [[0] * len(order)]
+    cands += [[lats.index(l_) % k for l_ in lat] for k in range(2, len(lats) + 1)]
+    cands += [[lats.index(l_) * m + r % m for l_, r in zip(lat, rank)] for m in range(2, max_passes // len(lats) + 1)]
+    tried = []
+    for key in cands:
+        passes = [[b for b, k_ in zip(order, key) if k_ == q] for q in range(max(key) + 1)]
         passes = [q for q in passes if q]
-        pk = max(peak_bytes([plan.blocks_refl[b] for b in q], [plan.need_lo[b] for b in q],
-                            [plan.need_hi[b] for b in q], w_row, n_frames)[0] for q in passes)
-        if best is None or pk < best[1]:
-            best = (passes, pk)
+        pk = max(peak_bytes([blocks[b] for b in q], [need_lo[b] for b in q], [need_hi[b] for b in q], w_row,
+                            n_frames)[0] for q in passes)
+        tried.append((passes, pk))
         if pk <= limit:
-            break
-    return best
+            return passes, pk
+    low = min(t[1] for t in tried)
+    cut = low + 0.05 * (tried[0][1] - low)
+    return next(t for t in tried if t[1] <= cut)
