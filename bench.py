@@ -677,6 +677,16 @@ def batched_bench(args):
     n = sum(len(r.refl["x"]) for r in rp)
     same = all(np.array_equal(a.refl[k], b.refl[k], equal_nan=True) for a, b in zip(rp, rb)
                for k in ("isum", "iprf", "vprf", "bg", "isum_raw"))
+    spans = {}
+    if args.spans:                       # one more step of each, untimed, with device-time spans per kernel
+        for name, fn in (("plain", plain), ("batched", batched)):
+            D.TIMER.enabled = True
+            D.TIMER.reset()
+            _, t = timed(fn)
+            torch.cuda.synchronize()
+            spans[name] = {"seconds": round(t, 3), "device_s": {k: round(v[1], 4) for k, v in
+                                                                D.TIMER.summary().items()}}
+            D.TIMER.enabled = False
     line = {"metric": "integrated reflections/s, 12 sweeps (config 4), batched vs plain", "unit": "refl/s",
             "value": round(n / np.median(tb), 1), "plain": round(n / np.median(tp), 1),
             "speedup": round(float(np.median(tp) / np.median(tb)), 3), "steps": args.steps, "warmup": args.warmup,
@@ -686,9 +696,10 @@ def batched_bench(args):
                         "sigma_m": round(s.sigma_m, 3), "reflections": len(r.refl["x"]),
                         "block_parts": int(r.memory["parts"]), "passes": len(r.memory.get("passes", [1])),
                         "planned_peak_gib": round(r.memory["peak"] / 2 ** 30, 1)} for s, r in zip(specs, rp)],
-            "budget_gib": round(budget / 2 ** 30, 1),
-            "batched_stats": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "pass1_launches",
-                                                                      "peak_bytes")},
+            "budget_gib": round(budget / 2 ** 30, 1), "spans": spans or None,
+            "batched_stats": {k: (v if k != "host_s" else {a: round(b, 3) for a, b in v.items()})
+                              for k, v in stats.items() if k in ("rounds", "blocks", "pass1_launches", "peak_bytes",
+                                                                 "host_s")},
             "data": "synthetic, frames rendered on the device inside the timed region (both forms)"}
     print(json.dumps(line), flush=True)
 
@@ -738,7 +749,8 @@ def served_bench(args):
             "sweeps": [{"frames": s.nframes, "cell": s.space_group, "reflections": len(r.refl["x"]),
                         "block_parts": int(r.memory["parts"]), "planned_peak_gib": round(r.memory["peak"] / 2 ** 30, 1)}
                        for s, r in zip(specs, res)],
-            "scheduler": {k: v for k, v in stats.items() if k in ("rounds", "blocks", "peak_bytes", "waits")},
+            "scheduler": {k: (v if k != "host_s" else {a: round(b, 3) for a, b in v.items()})
+                          for k, v in stats.items() if k in ("rounds", "blocks", "peak_bytes", "waits", "host_s")},
             "data": "synthetic; wedges rendered on the device at their arrival"}
     print(json.dumps(line), flush=True)
 
@@ -877,6 +889,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the post-check of the results against the oracle")
+    ap.add_argument("--spans", action="store_true", help="config4: one more untimed step of each form with per-kernel "
+                                                          "device-time spans")
     ap.add_argument("--decode", action="store_true", help="time the bitshuffle-LZ4 frame decode instead")
     ap.add_argument("--spots", action="store_true", help="time the spot-finding classifier instead")
     args = ap.parse_args()

@@ -147,6 +147,10 @@ int xi_version(void);
 /* Synchronises the stream and reports (then clears) the kernels' status word: XI_E_SHAPE when a row was skipped
  * because its shape exceeded its call's max_bx / max_dz. */
 int xi_status(void *stream);
+/* Queues a copy of the kernels' status word into host_dst (pinned host memory) on the stream, without waiting: the
+ * caller reads it once the stream has passed that point; nonzero: a row was skipped (xi_status then reports and
+ * clears it). */
+int xi_status_copy(int *host_dst, void *stream);
 
 /* Launch tuning (process-wide; no counterpart in XPG, whose torch kernels have no launch shape): the largest
  * shoebox (bytes) pass 1 / pass 2 stage in shared memory, pass 2's fit-list capacity (voxels) and the CTA width of

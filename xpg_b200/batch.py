@@ -137,7 +137,8 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
     active, results = [], [None] * len(jobs)
     used = 0
     stats = dict(rounds=0, blocks=0, pass1_launches=0, latency=[], admitted_at={}, peak_bytes=0, waits=0,
-                 completing=set())
+                 completing=set(), host_s=dict(feed=0.0, rounds=0.0, admit=0.0, finish=0.0))
+    hs = stats["host_s"]
     t0 = clock()
 
     def arrived(a, w):
@@ -179,7 +180,9 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
         fed = []
         for a in active:
             if a.w < len(a.run.wedges) and arrived(a, a.w):
+                t_ = time.perf_counter()
                 got = a.run.feed(a.w)
+                hs["feed"] += time.perf_counter() - t_
                 if got:
                     stats["completing"].add((a.i, a.w))     # the wedge completed blocks: its latency has their passes
                 a.pend += got
@@ -193,9 +196,11 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 a.run.start_pass(a.run.pass_index + 1)       # blocks that did not fit in one pass over the frames
                 a.w = 0
                 progressed = True
+        t_ = time.perf_counter()
         while any(a.pend for a in active):
             _round(active, bins, stats)
             progressed = True
+        hs["rounds"] += time.perf_counter() - t_
         if served and fed:
             # a wedge is done when the work queued for it (its gathers, and the blocks it completed, whose results
             # are on the host already) has run: an event after it, polled without stopping the loop
@@ -216,13 +221,17 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
             waiting[:] = left
         for a in [a for a in active if a.w >= len(a.run.wedges) and not a.pend and not a.run.opened
                   and a.run.pass_index + 1 >= a.run.n_passes]:
+            t_ = time.perf_counter()
             results[a.i] = a.run.result()
+            hs["finish"] += time.perf_counter() - t_
             a.run.close()
             used -= a.nbytes
             active.remove(a)
             progressed = True
         n_before = len(active)
+        t_ = time.perf_counter()
         admit()
+        hs["admit"] += time.perf_counter() - t_
         progressed = progressed or len(active) != n_before
         if not progressed:
             stats["waits"] += 1

@@ -1775,6 +1775,16 @@ int xi_status(void* stream) {
 }
 
 
+int xi_status_copy(int* host_dst, void* stream) {
+    int* p = status_ptr();
+    if (!p) return fail(XI_E_CUDA, "status word unavailable");
+    if (!host_dst) return fail(XI_E_ARG, "xi_status_copy: null destination");
+    if (cudaMemcpyAsync(host_dst, p, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream) != cudaSuccess)
+        return cuda_check("xi_status_copy");
+    return XI_OK;
+}
+
+
 int xi_pass1(const XiDetector* det, const XiRows* R, const XiBlock* B, const float* arena, XiPass1Out* O,
              void* stream) {
     if (!det || !B || !arena || !O) return fail(XI_E_ARG, "xi_pass1: null argument");

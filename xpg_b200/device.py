@@ -169,7 +169,10 @@ def h2d(a, dtype=None, device="cuda"):
     """Host array -> device tensor on the current stream without blocking the host: staged through the upload ring
     and read by a kernel (large arrays: through torch's pinned staging and the copy engine). A pageable copy would
     wait for every kernel queued before it."""
-    t = torch.as_tensor(np.ascontiguousarray(a), dtype=dtype)
+    a = np.ascontiguousarray(a)
+    if not a.flags.writeable:                 # torch does not wrap read-only arrays (a broadcast view, a plan column)
+        a = a.copy()
+    t = torch.as_tensor(a, dtype=dtype)
     if t.numel() == 0:
         return t.to(device)
     t = t.contiguous()

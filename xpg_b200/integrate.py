@@ -263,6 +263,7 @@ class SweepRun:
         if mask is not None and not np.asarray(mask).all():
             self.mask_t = D.h2d(np.asarray(mask, np.uint8), None, device)
         self.processed = []
+        self.collects = []                # blocks whose results are on their way to the host (collect -> finish)
         self.live = {}                    # completed blocks between pass1_stage and collect
         # when frames are uploaded, rows of the next block to complete whose last frame has arrived get their pass 1
         # as soon as their wedge is in: it overlaps the transfer of the later wedges (their widths are fixed: every
@@ -519,27 +520,50 @@ class SweepRun:
         return None
 
     def collect(self, b):
-        """The block's results to the host, into the run's output columns; the block's arena goes back to the pool
-        (every kernel that reads it has run once the results are on the host)."""
+        """The block's results to the host: copies into pinned host memory queued behind pass 2 (the host goes on with
+        the next wedges while pass 2 runs), put into the run's output columns once they have landed (`finish`). The
+        block's arena goes back to the pool now: its next user writes it on this stream, after every kernel that
+        reads it (unless a captured gather graph still names it)."""
         blk = self.live.pop(b)
         p1, rs = blk.p1, blk.rowset
         cols = {k: p1.t[k] for k in P1_OUT}
         if blk.p2 is not None:
             cols.update({k: blk.p2.t[k] for k in P2_OUT})
-        D.status()
-        self.prof_by_block[b] = blk.prof.cpu().numpy()
-        h = _host_rows(cols, tuple(cols), blk.perm_t)     # in plan (global row) order
-        dst = slice(*blk.span) if blk.span is not None else blk.rows_sorted
-        for k, v in h.items():
-            self.out[k][dst] = v
+        c = _Collected(b, blk.rows, blk.span, blk.rows_sorted, self.tg)     # no device buffer kept past the copies
+        c.host = _host_rows_async(cols, tuple(cols), blk.perm_t)
+        c.prof = _pinned_copy(blk.prof)
         if self.fz_out is not None:
-            self.fz_out[blk.rows] = _fz_rows(p1, rs, np.arange(rs.n)).float().cpu().numpy()
-        if self._gg is None or b not in self._gg.key:      # a captured gather graph may still name the arena
+            c.fz = _pinned_copy(_fz_rows(p1, rs, np.arange(rs.n)).float())
+        c.status = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        N.check(N.load().xi_status_copy(c.status.data_ptr(), N.stream_handle()), "xi_status_copy")
+        c.ev = torch.cuda.Event()
+        c.ev.record()
+        self.collects.append(c)
+        if self._gg is None or b not in self._gg.key:
             D.POOL.give(blk.arena)
             blk.arena = None
-        self.t_dev += time.time() - self.tg
+        self.finish(wait=False)
+
+    def finish(self, wait=True):
+        """Collected blocks whose copies have landed (every one: wait) into the run's output columns, in order."""
+        while self.collects:
+            c = self.collects[0]
+            if not wait and not c.ev.query():
+                return
+            c.ev.synchronize()
+            self.collects.pop(0)
+            if int(c.status[0]):
+                D.status()                                  # reports (raises) and clears the status word
+            self.prof_by_block[c.b] = c.prof.numpy()
+            dst = slice(*c.span) if c.span is not None else c.rows_sorted
+            for k, v in c.host.items():
+                self.out[k][dst] = v.numpy()
+            if c.fz is not None:
+                self.fz_out[c.rows] = c.fz.numpy()
+            self.t_dev += time.time() - c.tg
 
     def result(self):
+        self.finish()
         p, out, refl = self.plan, self.out, self.refl
         unfilled = np.ones(p.n, bool)                     # rows of blocks never processed: NaN, as XPG leaves them
         for b in self.processed:
@@ -586,6 +610,38 @@ ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")
 P1_OUT = ("bg", "isum", "vsum", "vsum0", "xo", "yo", "zo", "frac_rec", "m_d", "m_m", "n_over", "n_fg_masked",
           "isum_raw")
 P2_OUT = ("iprf", "vprf", "vprf0", "corr", "p_valid", "p_total", "rho", "p_fg")
+
+
+class _Collected:
+    """A block's results on their way to the host: pinned copies queued on the compute stream, the kernels' status
+    word, and an event after them."""
+
+    def __init__(self, b, rows, span, rows_sorted, tg):
+        self.b, self.rows, self.span, self.rows_sorted, self.tg = b, rows, span, rows_sorted, tg
+        self.host, self.prof, self.fz, self.status, self.ev = {}, None, None, None, None
+
+
+def _pinned_copy(t):
+    """Queues a copy of device tensor t into new pinned host memory on the current stream (read after a sync)."""
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    return h
+
+
+def _host_rows_async(t, keys, perm=None):
+    """`_host_rows` without waiting: one stacked pinned copy per dtype queued on the current stream; values are host
+    tensor rows, valid once the stream has passed the copies."""
+    out = {}
+    for dt in (torch.float32, torch.int64):
+        ks = [k for k in keys if t[k].dtype == dt]
+        if not ks:
+            continue
+        st = torch.stack([t[k] for k in ks])
+        if perm is not None:
+            st = st.index_select(1, perm)
+        h = _pinned_copy(st)
+        out.update({k: h[i] for i, k in enumerate(ks)})
+    return out
 
 
 def _host_rows(t, keys, perm=None):

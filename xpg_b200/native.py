@@ -161,12 +161,12 @@ class XiHklRows(C.Structure):
 XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP, XI_TUNE_WIDE_THREADS = 1, 2, 3, 4
 XI_PACK_ESCAPE, XI_PACK_FLAGGED = 254, 255
 
-EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_tune", "xi_gather", "xi_decode_bins", "xi_pass1",
-           "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
-           "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram", "xi_predict_workspace",
-           "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8", "xi_upload", "xi_bslz4_lz4_stage",
-           "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong", "xi_spot_workspace", "xi_pass1_batched",
-           "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames")
+EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_status_copy", "xi_tune", "xi_gather", "xi_decode_bins",
+           "xi_pass1", "xi_accumulate", "xi_finalize_profiles", "xi_pass2", "xi_predict_count", "xi_predict_write",
+           "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram",
+           "xi_predict_workspace", "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8",
+           "xi_upload", "xi_bslz4_lz4_stage", "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong",
+           "xi_spot_workspace", "xi_pass1_batched", "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames")
 
 _LIB = None
 
@@ -214,6 +214,7 @@ def load(path=None):
     lib.xi_format_integrate_hkl.argtypes = [C.POINTER(XiHklRows), C.c_void_p, C.c_int64, C.c_int,
                                             C.POINTER(C.c_int64)]
     lib.xi_status.argtypes = [C.c_void_p]
+    lib.xi_status_copy.argtypes = [C.c_void_p, C.c_void_p]
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_decode_bins.argtypes = [C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
