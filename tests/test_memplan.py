@@ -100,7 +100,10 @@ def test_passes_over_parts_when_rows_wide_in_phi_keep_every_part_open():
     rows = np.concatenate(q.blocks_refl)
     assert np.array_equal(np.sort(rows), np.arange(p.n))
     q2, e2, info2 = M.fit(p, exps, nf, 0, 0.6 * one, allow_passes=False)
-    assert "passes" not in info2 and info2["parts"] == 1          # no split lowers the peak: the plan stays whole
+    # frames read once: the wide rows go in a part of their own, the others in parts of consecutive phi
+    assert "passes" not in info2 and info2.get("wide_apart") and info2["peak"] <= 0.6 * one
+    assert np.array_equal(np.sort(np.concatenate(q2.blocks_refl)), np.arange(p.n))
+    assert any(np.isin(wide, r).all() for r in q2.blocks_refl)     # every planted wide row in the wide part
 
 
 def test_passes_by_lattice_first():

@@ -17,6 +17,7 @@ import numpy as np
 
 BLOCK_PARTS_MAX = 8          # parts per phi block at most (xpg/integrate.py:55)
 DEVICE_FRACTION = 0.95       # share of the device memory free at the start that the run's buffers may use
+WIDE_SPANS = 4.0             # rows deeper in phi than this many median spans: a part of their own (frames read once)
 
 
 def row_bytes(plan):
@@ -83,8 +84,10 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
     order (xpg/integrate.py:598-622): unchanged when one pass over the frames fits; else, when the frames can be read
     again (allow_passes), the whole blocks in several passes over the frames (`split_passes`); else every block split
     into the fewest parts of consecutive phi (2..8) that fit, each split with its own passes (allow_passes), or the
-    split with the lowest peak when none fits and it is below the whole blocks'. Returns (plan, exp_blocks, info);
-    info["passes"]: the block lists of the passes when there are several."""
+    split with the lowest peak when none fits and it is below the whole blocks'. Frames read once (no passes) and no
+    such split fits: the rows far deeper in phi than the others in a part of their own (`split_wide`, info
+    ["wide_apart"]). Returns (plan, exp_blocks, info); info["passes"]: the block lists of the passes when there are
+    several; info["parts"]: parts per block of the consecutive-phi split."""
     w_row = row_bytes(plan)
     one, big = peak_bytes(plan.blocks_refl, plan.need_lo, plan.need_hi, w_row, n_frames)
     info = dict(peak=one + wedge_bytes, one=one + wedge_bytes, parts=1, budget=limit)
@@ -111,19 +114,56 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
         if pk is None:
             pk = peak_bytes(parts, lo, hi, w_row, n_frames)[0]
         if best is None or pk < best[0]:
-            best = (pk, k, parts, parent, lo, hi, passes)
+            best = (pk, k, parts, parent, lo, hi, passes, False)
         if pk <= room:
             break
-    pk, k, parts, parent, lo, hi, passes = best
+    if not allow_passes and best[0] > room:
+        # frames read once and no split by XPG's rule fits: a few rows far deeper in phi than a part (binned, near
+        # the rotation axis) keep every part of their block open; those rows go in a part of their own
+        for k in range(2, BLOCK_PARTS_MAX + 1):
+            parts, parent = split_wide(plan.blocks_refl, plan.refl["z"], plan.zstart, plan.zend, w_row, k)
+            lo = [int(plan.zstart[r].min()) for r in parts]
+            hi = [int(plan.zend[r].max()) for r in parts]
+            pk = peak_bytes(parts, lo, hi, w_row, n_frames)[0]
+            if pk < best[0]:
+                best = (pk, k, parts, parent, lo, hi, [], True)
+            if pk <= room:
+                break
+    pk, k, parts, parent, lo, hi, passes, wide = best
     if pk < whole:
         plan = replace(plan, blocks_refl=parts, need_lo=lo, need_hi=hi)
         exp_blocks = [exp_blocks[b] for b in parent]
         info.update(peak=pk + wedge_bytes, parts=k, parent=parent)
+        if wide:
+            info["wide_apart"] = True
         if len(passes) > 1:
             info["passes"] = passes
     elif base_pk is not None and base_pk < one:
         info.update(peak=base_pk + wedge_bytes, passes=base)
     return plan, exp_blocks, info
+
+
+def split_wide(blocks_refl, z, zstart, zend, w_row, k):
+    """Every block's rows whose frame span exceeds WIDE_SPANS times the median span in a part of their own (after the
+    block's other parts), the other rows in k parts by XPG's rule (`split_blocks`): (parts, the block of each part).
+    No counterpart in XPG, which can always read the frames again instead."""
+    span = np.asarray(zend, np.int64) - np.asarray(zstart, np.int64) + 1
+    nonempty = [r for r in blocks_refl if r.size]
+    if not nonempty:
+        return [], []
+    limit = max(8.0, WIDE_SPANS * float(np.median(span[np.concatenate(nonempty)])))
+    parts, parent = [], []
+    for b, rows in enumerate(blocks_refl):
+        if not rows.size:
+            continue
+        wide = span[rows] > limit
+        sub, _ = split_blocks([rows[~wide]], z, w_row, k)
+        parts += sub
+        parent += [b] * len(sub)
+        if wide.any():
+            parts.append(rows[wide])
+            parent.append(b)
+    return parts, parent
 
 
 def split_passes(blocks, need_lo, need_hi, lattice, w_row, n_frames, limit, max_passes=16):
