@@ -516,6 +516,7 @@ def run(args):
                 "memory": {"block_parts": int(res_timed.memory["parts"]),
                            "open_buffers_gb": round(res_timed.memory["peak"] / 1e9, 1),
                            "budget_gb": round(res_timed.memory["budget"] / 1e9, 1)},
+                "host_s_last_step": {k: round(v, 3) for k, v in res_timed.timing.get("host_s", {}).items()},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "parity": parity}
         print(json.dumps(line), flush=True)

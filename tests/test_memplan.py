@@ -65,7 +65,7 @@ def test_passes_group_blocks_m_apart():
     p, exps, nf = _plan("adaptive")
     w = M.row_bytes(p)
     one, big = M.peak_bytes(p.blocks_refl, p.need_lo, p.need_hi, w, nf)
-    passes, pk = M.split_passes(p.blocks_refl, p.need_lo, p.need_hi, [0, 0], w, nf, big)
+    passes, pk = M.split_passes([w[r].sum() for r in p.blocks_refl], p.need_lo, p.need_hi, [0, 0], nf, big)
     assert len(passes) == 2 and sorted(sum(passes, [])) == [0, 1] and pk <= big
     q, e, info = M.fit(p, exps, nf, 0, 0.55 * one)
     assert "passes" in info and info["peak"] < one
@@ -115,8 +115,9 @@ def test_passes_by_lattice_first():
     hi = [150, 250, 299, 150, 250, 299]
     w = rng.uniform(1, 2, 60)
     one = M.peak_bytes(blocks, lo, hi, w, 300)[0]
-    passes, pk = M.split_passes(blocks, lo, hi, [0, 0, 0, 1, 1, 1], w, 300, 0.6 * one)
+    nbytes = [w[r].sum() for r in blocks]
+    passes, pk = M.split_passes(nbytes, lo, hi, [0, 0, 0, 1, 1, 1], 300, 0.6 * one)
     assert passes == [[0, 1, 2], [3, 4, 5]] and pk <= 0.6 * one
-    passes, pk = M.split_passes(blocks, lo, hi, [0, 0, 0, 1, 1, 1], w, 300, 0.3 * one)
+    passes, pk = M.split_passes(nbytes, lo, hi, [0, 0, 0, 1, 1, 1], 300, 0.3 * one)
     assert len(passes) == 4 and sorted(sum(passes, [])) == list(range(6))
     assert all(len({b // 3 for b in q}) == 1 for q in passes)           # each pass holds one lattice

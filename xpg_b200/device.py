@@ -358,19 +358,37 @@ class Pass1Buffers:
                "seff")
     COUNTS = ("n_over", "n_fg_masked", "n_fg_nb", "isum_raw")
 
-    def __init__(self, rows: RowSet):
+    def __init__(self, rows: RowSet, pooled=False):
+        """pooled: the per-pixel tables (17 bytes a pixel, GBs for a block) as views of one buffer from POOL, given
+        back by `release` (the caching allocator would otherwise split the large blocks it keeps for them)."""
         d = rows.device
         n = rows.n
         self.t = {k: torch.empty(n, dtype=F32, device=d) for k in self.SCALARS}
         self.t.update({k: torch.empty(n, dtype=torch.int64, device=d) for k in self.COUNTS})
         self.t["fz"] = torch.empty(rows.n_frm, dtype=F32, device=d)
-        for k in ("img2", "J", "u1", "u2"):
-            self.t[k] = torch.empty(rows.n_pix, dtype=F32, device=d)
-        self.t["all_valid2"] = torch.empty(rows.n_pix, dtype=torch.uint8, device=d)
+        self.base = None
+        if pooled:
+            step = (rows.n_pix * 4 + 255) // 256 * 256              # each table on 256 bytes
+            self.base = POOL.take(4 * step + max(rows.n_pix, 1), torch.uint8, d)
+            for i, k in enumerate(("img2", "J", "u1", "u2")):
+                self.t[k] = self.base[i * step:i * step + rows.n_pix * 4].view(F32)
+            self.t["all_valid2"] = self.base[4 * step:4 * step + rows.n_pix]
+        else:
+            for k in ("img2", "J", "u1", "u2"):
+                self.t[k] = torch.empty(rows.n_pix, dtype=F32, device=d)
+            self.t["all_valid2"] = torch.empty(rows.n_pix, dtype=torch.uint8, device=d)
         o = N.XiPass1Out()
         for k, v in self.t.items():
             setattr(o, k, N.ptr(v))
         self.s = o
+
+    def release(self):
+        """The pooled per-pixel tables back to POOL (their next user writes them in stream order)."""
+        if self.base is not None:
+            POOL.give(self.base)
+            self.base = None
+            for k in ("img2", "J", "u1", "u2", "all_valid2"):
+                self.t.pop(k, None)
 
     def pass2_in(self):
         i = N.XiPass2In()

@@ -139,12 +139,13 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
               minimum_zeta=0.05, verbose=True, log=print, n_regions_xy=3, learn_profiles=True, exclude_frames=(),
               adaptive=True, deconvolve_overlaps=True, extra_lattices=None, bkg_template=None, foreign_spots=None,
               n_foreign=4, moments_only=False, *, wedge_frames=WEDGE_FRAMES, device="cuda", allowed=centring_allowed,
-              graphs=False, mem_budget=None, overlap=False):
+              graphs=False, mem_budget=None, overlap=True):
     """Integrate a sweep (`xpg/integrate.py:209-999`). `exp_blocks`: one experiment per phi block, `block_edges` in
     frame-coordinate units; `extra_lattices`: further lattices integrated together (refl['lattice'] = id); graphs:
     each wedge's gathers replayed from a CUDA graph captured once per set of open blocks; mem_budget: device bytes the
-    open blocks' buffers may use (default: memplan.budget), beyond which blocks are integrated in parts; overlap: the
-    gathers on a stream of their own, LOOKAHEAD wedges ahead of the passes of the blocks they completed."""
+    open blocks' buffers may use (default: memplan.budget), beyond which blocks are integrated in parts; overlap (on
+    by default; results are the same bits either way): the gathers on a stream of their own, LOOKAHEAD wedges ahead
+    of the passes of the blocks they completed."""
     run = SweepRun(images, exp_blocks, block_edges, model, dmin, dmax, frames, mask, minimum_zeta, verbose, log,
                    n_regions_xy, learn_profiles, exclude_frames, adaptive, deconvolve_overlaps, extra_lattices,
                    bkg_template, foreign_spots, n_foreign, moments_only, wedge_frames=wedge_frames, device=device,
@@ -242,6 +243,7 @@ class SweepRun:
         self.state = dict(sd=self.sd, sm=self.sm, rcw=A.rc_default_weights())
         self.block_params, self.prof_by_block, self.block_widths = {}, {}, {}
         self.t_dev = 0.0
+        self.host_s = {}                  # host seconds per stage (waits for the device included)
         nblocks = len(exp_blocks)
         self.read_fi = read_fi = np.array([f - 1 for f in range(f_first, f_last + 1) if f not in excl], np.int64)
         # a block takes every frame read up to the first frame read at or after its last needed frame
@@ -306,7 +308,7 @@ class SweepRun:
             sd_b, sm_b, rcw_b = self.widths()
             blk.c1 = (sd_b, sm_b, rcw_b) + D.block_consts(self.exp_blocks[b].geom, sd_b, sm_b, self.model.gain,
                                                           rcw_b, self.device)
-            blk.p1 = D.Pass1Buffers(blk.rowset)
+            blk.p1 = D.Pass1Buffers(blk.rowset, pooled=True)
 
     def pass1_rows(self, b, blk: _Block, idx, groups=None, binned_t=None):
         """Bin decode and pass 1 of the block's local rows idx, whose frames have all been gathered (launch groups
@@ -343,6 +345,7 @@ class SweepRun:
         p = self.plan
         f, f_b = self.wedges[w]
         fi_a, fi_b = f - 1, f_b - 1
+        t0 = time.perf_counter()
         while self.pending and p.need_lo[self.pending[0]] <= fi_b:
             b = self.pending.pop(0)
             blk = _Block(b, p.blocks_refl[b], p, self.device)
@@ -351,6 +354,7 @@ class SweepRun:
                 self.block_pass1_consts(b, blk)
             self.opened[b] = blk
             self.open_order.append(b)
+        t0 = self._clock("open", t0)
         ok = self.oks[w]
         ok_t = None
         if not ok.all():
@@ -373,6 +377,7 @@ class SweepRun:
                     self.opened[b].gathered = ev_w
         if self.feeder is not None:
             self.feeder.done_with(w)
+        self._clock("gather_launch", t0)
         done = sorted((b for b in self.open_order if b in self.opened and self.eff_hi[b] <= fi_b
                        and b not in self.reported), key=lambda b: (self.eff_hi[b], self.open_order.index(b)))
         self.reported.update(done)
@@ -459,6 +464,7 @@ class SweepRun:
     def pass1_stage(self, b, batched=False):
         """Bin decode and pass 1 of the block's rows not done yet; batched: no launch, returns (set entry, local rows)
         for a batched launch (the caller launches, then calls learn)."""
+        t0 = time.perf_counter()
         blk = self.opened.pop(b)
         self.live[b] = blk
         self._wait_gathers(blk)
@@ -468,15 +474,18 @@ class SweepRun:
         if not batched:
             if rem.size:
                 self.pass1_rows(b, blk, rem)
+            self._clock("pass1_stage", t0)
             return None
         self.decode_rows(b, blk, rem)
         blk.p1_done[rem] = True
         det = self.detector(self.exp_blocks[b].geom)
+        self._clock("pass1_stage", t0)
         return D.rowset_entry(det, blk.rowset, blk.c1[3], blk.arena, blk.p1), rem
 
     def learn(self, b):
         """Profiles and widths of a block whose pass 1 is complete: accumulation, the host adaptation (sigma_M,
         rocking-curve weights for this block's pass 2, sigma_D for the next block), finalisation."""
+        t0 = time.perf_counter()
         blk = self.live[b]
         p, rs, device = self.plan, blk.rowset, self.device
         g = self.exp_blocks[b].geom
@@ -487,7 +496,9 @@ class SweepRun:
         den = torch.zeros_like(num)
         if self.learn_profiles:
             D.accumulate(rs, p1, self.nreg, num, den)
+        t0 = self._clock("learn_other", t0)
         h1 = _host_rows(p1.t, ADAPT_KEYS)
+        t0 = self._clock("learn_wait", t0)                 # pass 1 of the block runs meanwhile
         rows = blk.rows
         if self.adaptive:
             st = _adapt_rows(h1, p, rows)
@@ -501,12 +512,14 @@ class SweepRun:
             if sd_next is not None:
                 self.state.update(sd=sd_next, sm=float(sm_b), rcw=np.asarray(rcw_b, np.float32))
             self.block_params[b] = params
+        t0 = self._clock("adapt", t0)
         blk.prof = torch.empty((self.nreg, PROFILE_GRID, PROFILE_GRID), dtype=torch.float32, device=device)
         D.finalize_profiles(num, den, blk.prof)
         self.block_widths[b] = dict(pass1=widths_p1,
                                     pass2=(float(sd_b), float(sm_b), np.asarray(rcw_b, np.float32).copy()))
         blk.c2 = D.block_consts(g, sd_b, sm_b, self.model.gain, rcw_b, device)
         blk.p2 = None if self.moments_only else D.Pass2Buffers(rs)
+        self._clock("learn_other", t0)
 
     def pass2_stage(self, b, batched=False):
         """Pass 2 of the block (none for moments-only runs); batched: its set entry for a batched launch."""
@@ -516,7 +529,9 @@ class SweepRun:
         det = self.detector(self.exp_blocks[b].geom)
         if batched:
             return D.rowset_entry(det, blk.rowset, blk.c2[0], blk.arena, blk.p1, blk.prof, blk.p2)
+        t0 = time.perf_counter()
         D.pass2(det, blk.rowset, blk.c2[0], blk.arena, blk.prof, blk.p1, blk.p2)
+        self._clock("pass2_stage", t0)
         return None
 
     def collect(self, b):
@@ -524,6 +539,7 @@ class SweepRun:
         the next wedges while pass 2 runs), put into the run's output columns once they have landed (`finish`). The
         block's arena goes back to the pool now: its next user writes it on this stream, after every kernel that
         reads it (unless a captured gather graph still names it)."""
+        t0 = time.perf_counter()
         blk = self.live.pop(b)
         p1, rs = blk.p1, blk.rowset
         cols = {k: p1.t[k] for k in P1_OUT}
@@ -542,6 +558,8 @@ class SweepRun:
         if self._gg is None or b not in self._gg.key:
             D.POOL.give(blk.arena)
             blk.arena = None
+        p1.release()
+        self._clock("collect", t0)
         self.finish(wait=False)
 
     def finish(self, wait=True):
@@ -550,6 +568,7 @@ class SweepRun:
             c = self.collects[0]
             if not wait and not c.ev.query():
                 return
+            t0 = time.perf_counter()
             c.ev.synchronize()
             self.collects.pop(0)
             if int(c.status[0]):
@@ -561,6 +580,13 @@ class SweepRun:
             if c.fz is not None:
                 self.fz_out[c.rows] = c.fz.numpy()
             self.t_dev += time.time() - c.tg
+            self._clock("finish", t0)
+
+    def _clock(self, stage, t0):
+        """Adds the host seconds since t0 to the stage's total; returns the time now."""
+        t = time.perf_counter()
+        self.host_s[stage] = self.host_s.get(stage, 0.0) + t - t0
+        return t
 
     def result(self):
         self.finish()
@@ -587,7 +613,8 @@ class SweepRun:
             self.log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - self.t0:.1f}s "
                      f"(device {self.t_dev:.1f}s)")
         res = IntegrationResult(refl, self.model, self.prof_by_block, dict(total=time.time() - self.t0,
-                                                                           gpu=self.t_dev))
+                                                                           gpu=self.t_dev,
+                                                                           host_s=dict(self.host_s)))
         res.block_params = self.block_params
         res.block_widths = self.block_widths  # (sigma_D, sigma_M in radians, rocking-curve weights) of each pass
         res.plan = self.plan                  # the plan integrated (blocks split in parts when memory was short)
@@ -604,6 +631,7 @@ class SweepRun:
             D.POOL.give(self.src._buf)
             self.src._buf = None
         D.POOL.clear()                        # the kept arenas go back to the allocator between runs
+        torch.cuda.empty_cache()              # and to the device: the next run's small buffers must not split them
 
 
 ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")

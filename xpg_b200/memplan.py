@@ -62,21 +62,73 @@ def peak_bytes(blocks_refl, need_lo, need_hi, w_row, n_frames):
     return float(np.cumsum(d).max()), big
 
 
+def peak_of(nbytes, lo, hi, n_frames):
+    """Largest sum over the frames of `nbytes[i]` for the parts open at the frame (part i over frame indices
+    lo[i]..hi[i])."""
+    nbytes = np.asarray(nbytes, np.float64)
+    if not nbytes.size:
+        return 0.0
+    d = np.zeros(n_frames + 2)
+    np.add.at(d, np.clip(np.asarray(lo, np.int64), 0, n_frames), nbytes)
+    np.add.at(d, np.clip(np.asarray(hi, np.int64) + 1, 0, n_frames + 1), -nbytes)
+    return float(np.cumsum(d).max())
+
+
+class _Cuts:
+    """A split's parts without their row lists: per part its bytes, first and last frame, block, and where its rows
+    lie in its block's z order (`rows()` makes the row lists of the chosen split only)."""
+
+    def __init__(self):
+        self.nbytes, self.lo, self.hi, self.parent, self.slices = [], [], [], [], []
+
+    def add(self, nbytes, lo, hi, parent, sl):
+        self.nbytes.append(nbytes)
+        self.lo.append(int(lo))
+        self.hi.append(int(hi))
+        self.parent.append(parent)
+        self.slices.append(sl)
+
+    def peak(self, n_frames):
+        return peak_of(self.nbytes, self.lo, self.hi, n_frames)
+
+    def rows(self):
+        return [np.sort(o[a:e]) for o, a, e in self.slices]
+
+
+class _ZOrders:
+    """Every block's rows (optionally a subset) in z order, with their cumulative bytes and frame bounds: sorted once,
+    cut for every k."""
+
+    def __init__(self, blocks_refl, z, w_row, zstart, zend, keep=None):
+        self.items = []
+        for b, rows in enumerate(blocks_refl):
+            r = rows if keep is None else rows[keep[rows]]
+            if not r.size:
+                continue
+            o = r[np.argsort(z[r], kind="stable")]
+            c = np.concatenate([[0.0], np.cumsum(w_row[o], dtype=np.float64)])
+            self.items.append((b, o, c, np.asarray(zstart)[o], np.asarray(zend)[o]))
+
+    def cut(self, k, out=None):
+        """Every block in k parts of consecutive z with about equal bytes (XPG's `_split_blocks` rule: cuts where the
+        cumulative bytes pass k equal shares; empty parts dropped)."""
+        out = out if out is not None else _Cuts()
+        for b, o, c, zs, ze in self.items:
+            cuts = np.searchsorted(c[1:], c[-1] * np.arange(1, k) / k, side="right")
+            edges = np.unique(np.concatenate([[0], cuts, [o.size]]))
+            a, e = edges[:-1], edges[1:]
+            lo, hi = np.minimum.reduceat(zs, a), np.maximum.reduceat(ze, a)
+            for i in range(a.size):
+                out.add(float(c[e[i]] - c[a[i]]), lo[i], hi[i], b, (o, int(a[i]), int(e[i])))
+        return out
+
+
 def split_blocks(blocks_refl, z, w_row, k):
     """Every block's rows in k parts of consecutive z with about equal bytes (rows in index order within a part;
     empty parts dropped): (parts, the block of each part)."""
-    parts, parent = [], []
-    for b, rows in enumerate(blocks_refl):
-        if not rows.size:
-            continue
-        o = rows[np.argsort(z[rows], kind="stable")]
-        c = np.cumsum(w_row[o])
-        cuts = np.searchsorted(c, c[-1] * np.arange(1, k) / k, side="right")
-        for part in np.split(o, cuts):
-            if part.size:
-                parts.append(np.sort(part))
-                parent.append(b)
-    return parts, parent
+    n = int(max((int(r.max()) + 1 for r in blocks_refl if r.size), default=0))
+    cuts = _ZOrders(blocks_refl, z, w_row, np.zeros(n, np.int64), np.zeros(n, np.int64)).cut(k)
+    return cuts.rows(), cuts.parent
 
 
 def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
@@ -89,51 +141,55 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
     ["wide_apart"]). Returns (plan, exp_blocks, info); info["passes"]: the block lists of the passes when there are
     several; info["parts"]: parts per block of the consecutive-phi split."""
     w_row = row_bytes(plan)
-    one, big = peak_bytes(plan.blocks_refl, plan.need_lo, plan.need_hi, w_row, n_frames)
+    nb = [float(w_row[r].sum()) if r.size else 0.0 for r in plan.blocks_refl]
+    one = peak_of(nb, plan.need_lo, plan.need_hi, n_frames)
     info = dict(peak=one + wedge_bytes, one=one + wedge_bytes, parts=1, budget=limit)
     if limit is None or one + wedge_bytes <= limit:
         return plan, exp_blocks, info
     room = limit - wedge_bytes
     lat = plan.refl.get("lattice")
 
-    def passes_of(blocks, lo, hi):
-        lattice = [int(lat[r[0]]) if lat is not None and r.size else 0 for r in blocks]
-        return split_passes(blocks, lo, hi, lattice, w_row, n_frames, room) if allow_passes else ([], None)
+    def passes_of(nbytes, lo, hi, first_rows):
+        if not allow_passes:
+            return [], None
+        lattice = [int(lat[r]) if lat is not None and r >= 0 else 0 for r in first_rows]
+        return split_passes(nbytes, lo, hi, lattice, n_frames, room)
 
-    base, base_pk = passes_of(plan.blocks_refl, plan.need_lo, plan.need_hi)
+    base, base_pk = passes_of(nb, plan.need_lo, plan.need_hi, [int(r[0]) if r.size else -1 for r in plan.blocks_refl])
     whole = base_pk if base_pk is not None else one
     if base_pk is not None and base_pk <= room:
         info.update(peak=base_pk + wedge_bytes, passes=base)
         return plan, exp_blocks, info
+    zo = _ZOrders(plan.blocks_refl, plan.refl["z"], w_row, plan.zstart, plan.zend)
     best = None
     for k in range(2, BLOCK_PARTS_MAX + 1):
-        parts, parent = split_blocks(plan.blocks_refl, plan.refl["z"], w_row, k)
-        lo = [int(plan.zstart[r].min()) for r in parts]
-        hi = [int(plan.zend[r].max()) for r in parts]
-        passes, pk = passes_of(parts, lo, hi)
+        cuts = zo.cut(k)
+        passes, pk = passes_of(cuts.nbytes, cuts.lo, cuts.hi, [int(o[a]) for o, a, _ in cuts.slices])
         if pk is None:
-            pk = peak_bytes(parts, lo, hi, w_row, n_frames)[0]
+            pk = cuts.peak(n_frames)
         if best is None or pk < best[0]:
-            best = (pk, k, parts, parent, lo, hi, passes, False)
+            best = (pk, k, cuts, passes, False)
         if pk <= room:
             break
     if not allow_passes and best[0] > room:
         # frames read once and no split by XPG's rule fits: a few rows far deeper in phi than a part (binned, near
         # the rotation axis) keep every part of their block open; those rows go in a part of their own
+        wide = wide_rows(plan.blocks_refl, plan.zstart, plan.zend)
+        zn = _ZOrders(plan.blocks_refl, plan.refl["z"], w_row, plan.zstart, plan.zend, keep=~wide)
+        zw = _ZOrders(plan.blocks_refl, plan.refl["z"], w_row, plan.zstart, plan.zend, keep=wide)
         for k in range(2, BLOCK_PARTS_MAX + 1):
-            parts, parent = split_wide(plan.blocks_refl, plan.refl["z"], plan.zstart, plan.zend, w_row, k)
-            lo = [int(plan.zstart[r].min()) for r in parts]
-            hi = [int(plan.zend[r].max()) for r in parts]
-            pk = peak_bytes(parts, lo, hi, w_row, n_frames)[0]
+            cuts = _wide_cut(zn, zw, k)
+            pk = cuts.peak(n_frames)
             if pk < best[0]:
-                best = (pk, k, parts, parent, lo, hi, [], True)
+                best = (pk, k, cuts, [], True)
             if pk <= room:
                 break
-    pk, k, parts, parent, lo, hi, passes, wide = best
+    pk, k, cuts, passes, wide = best
     if pk < whole:
-        plan = replace(plan, blocks_refl=parts, need_lo=lo, need_hi=hi)
-        exp_blocks = [exp_blocks[b] for b in parent]
-        info.update(peak=pk + wedge_bytes, parts=k, parent=parent)
+        lo, hi = list(cuts.lo), list(cuts.hi)
+        plan = replace(plan, blocks_refl=cuts.rows(), need_lo=lo, need_hi=hi)
+        exp_blocks = [exp_blocks[b] for b in cuts.parent]
+        info.update(peak=pk + wedge_bytes, parts=k, parent=list(cuts.parent))
         if wide:
             info["wide_apart"] = True
         if len(passes) > 1:
@@ -143,35 +199,53 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
     return plan, exp_blocks, info
 
 
+def wide_rows(blocks_refl, zstart, zend):
+    """Rows whose frame span exceeds WIDE_SPANS times the median span of the plan's rows (a boolean per row)."""
+    span = np.asarray(zend, np.int64) - np.asarray(zstart, np.int64) + 1
+    nonempty = [r for r in blocks_refl if r.size]
+    if not nonempty:
+        return np.zeros(span.size, bool)
+    return span > max(8.0, WIDE_SPANS * float(np.median(span[np.concatenate(nonempty)])))
+
+
+def _wide_cut(z_narrow, z_wide, k):
+    """Each block's other rows in k parts by XPG's rule, then its wide rows as one part (`split_wide`)."""
+    narrow = z_narrow.cut(k)
+    wide = z_wide.cut(1)
+    out = _Cuts()
+    by_block = {}
+    for i, b in enumerate(wide.parent):
+        by_block[b] = i
+    blocks = sorted(set(narrow.parent) | set(wide.parent))
+    for b in blocks:
+        for i, pb in enumerate(narrow.parent):
+            if pb == b:
+                out.add(narrow.nbytes[i], narrow.lo[i], narrow.hi[i], b, narrow.slices[i])
+        if b in by_block:
+            i = by_block[b]
+            out.add(wide.nbytes[i], wide.lo[i], wide.hi[i], b, wide.slices[i])
+    return out
+
+
 def split_wide(blocks_refl, z, zstart, zend, w_row, k):
     """Every block's rows whose frame span exceeds WIDE_SPANS times the median span in a part of their own (after the
     block's other parts), the other rows in k parts by XPG's rule (`split_blocks`): (parts, the block of each part).
     No counterpart in XPG, which can always read the frames again instead."""
-    span = np.asarray(zend, np.int64) - np.asarray(zstart, np.int64) + 1
-    nonempty = [r for r in blocks_refl if r.size]
-    if not nonempty:
-        return [], []
-    limit = max(8.0, WIDE_SPANS * float(np.median(span[np.concatenate(nonempty)])))
-    parts, parent = [], []
-    for b, rows in enumerate(blocks_refl):
-        if not rows.size:
-            continue
-        wide = span[rows] > limit
-        sub, _ = split_blocks([rows[~wide]], z, w_row, k)
-        parts += sub
-        parent += [b] * len(sub)
-        if wide.any():
-            parts.append(rows[wide])
-            parent.append(b)
-    return parts, parent
+    wide = wide_rows(blocks_refl, zstart, zend)
+    cuts = _wide_cut(_ZOrders(blocks_refl, z, w_row, zstart, zend, keep=~wide),
+                     _ZOrders(blocks_refl, z, w_row, zstart, zend, keep=wide), k)
+    return cuts.rows(), cuts.parent
 
 
-def split_passes(blocks, need_lo, need_hi, lattice, w_row, n_frames, limit, max_passes=16):
+def split_passes(nbytes, need_lo, need_hi, lattice, n_frames, limit, max_passes=16):
     """Passes over the frames whose open blocks fit `limit` bytes, XPG's candidates in its order (`_plan_passes`,
     xpg/shoebox.py:134-183): one pass, then by lattice (blocks of other lattices cover the same frames), then within
     each lattice the blocks m apart in phi; the first that fits, else the fewest passes within 5% of the lowest peak.
-    blocks: row lists (empty ones take no pass). Returns (passes: block index lists in phi order, their peak)."""
-    order = sorted((b for b in range(len(blocks)) if blocks[b].size), key=lambda b: need_lo[b])
+    nbytes: each block's bytes (empty blocks, 0, take no pass). Returns (passes: block index lists in phi order, their
+    peak)."""
+    nbytes = np.asarray(nbytes, np.float64)
+    lo_a, hi_a = np.asarray(need_lo, np.int64), np.asarray(need_hi, np.int64)
+    order = sorted((b for b in range(nbytes.size) if nbytes[b] > 0), key=lambda b: lo_a[b])
     lat = [lattice[b] for b in order]
     lats = sorted(set(lat))
     rank, seen = [], {}
@@ -185,8 +259,7 @@ def split_passes(blocks, need_lo, need_hi, lattice, w_row, n_frames, limit, max_
     for key in cands:
         passes = [[b for b, k_ in zip(order, key) if k_ == q] for q in range(max(key) + 1)]
         passes = [q for q in passes if q]
-        pk = max(peak_bytes([blocks[b] for b in q], [need_lo[b] for b in q], [need_hi[b] for b in q], w_row,
-                            n_frames)[0] for q in passes)
+        pk = max(peak_of(nbytes[q], lo_a[q], hi_a[q], n_frames) for q in passes)
         tried.append((passes, pk))
         if pk <= limit:
             return passes, pk
