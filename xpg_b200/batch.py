@@ -123,12 +123,13 @@ def _round(active, bins, stats):
 
 
 def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, clock=time.perf_counter,
-             on_wedge=None, max_active=None, graphs=True, slots=None):
+             on_wedge=None, max_active=None, graphs=False, slots=None, overlap=True):
     """Integrates `jobs` (list of Job) together; returns (results in job order, stats). served: each wedge is fed no
     earlier than its arrival time (job.arrivals, seconds after the start) and the latency of every wedge (from its
     arrival to the completion of everything it triggered: its gathers and, when it completes blocks, their
     intensities on the host) is recorded in stats["latency"]. graphs: each sweep's per-wedge gathers replayed from
-    a CUDA graph (captured once per set of open blocks). slots: each sweep is planned (blocks in parts, memplan.fit)
+    a CUDA graph (captured once per set of open blocks). overlap: each sweep's gathers on a stream of its own, beside
+    the passes of every sweep's completed blocks. slots: each sweep is planned (blocks in parts, memplan.fit)
     for budget_bytes / slots, so that `slots` sweeps run at once; by default each is planned for the whole budget
     and sweeps wait for the memory the running ones hold."""
     budget = budget_bytes if budget_bytes is not None else int(0.8 * torch.cuda.mem_get_info(device)[0])
@@ -159,7 +160,8 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
                 if served:
                     job.images.rereadable = False            # live frames arrive once: no second pass over them
                 run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, early_pass1=False,
-                               device=device, verbose=False, mem_budget=plan_budget, graphs=graphs, **job.kwargs)
+                               device=device, verbose=False, mem_budget=plan_budget, graphs=graphs,
+                               overlap=overlap, **job.kwargs)
                 head[i] = (run, int(run.mem["peak"]))              # parts and passes included
             run, need = head[i]
             if active and used + need > budget:
@@ -207,12 +209,13 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
             for a, w in fed:
                 ev = torch.cuda.Event()
                 ev.record()
-                waiting.append((a.i, w, ev, float(a.job.arrivals[w]) if a.job.arrivals is not None else 0.0))
+                evs = (ev,) if a.run.last_gathered is None else (ev, a.run.last_gathered)
+                waiting.append((a.i, w, evs, float(a.job.arrivals[w]) if a.job.arrivals is not None else 0.0))
         if waiting:
             now = clock() - t0
             left = []
             for i, w, ev, arr in waiting:
-                if ev.query():
+                if all(e.query() for e in ev):
                     stats["latency"].append((i, w, now - arr))
                     if on_wedge is not None:
                         on_wedge(i, w, now)

@@ -45,7 +45,8 @@ class IntegrationResult:
 
 
 class _Block:
-    """Device state of one open phi block."""
+    """Device state of one phi block: its row tables and schedule (made ahead, while the host waits for the device),
+    then its shoebox arena (`allocate`, when the block opens)."""
 
     def __init__(self, b, rows, plan, device):
         self.b = b
@@ -70,8 +71,8 @@ class _Block:
             pphi=rad(dv["phi"].index_select(0, pj)), pxs=pxs, Dz=p.Dz[rows], bx=p.bx[rows], nb=nb, device=device,
             sb_bias=3.0)
         self.grows = D.GatherRows(self.rowset, ix0, iy0, iz0, p.fb[rows], pxs, device)
-        self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device).zero_()
-        self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
+        self.arena = None
+        self.cnt = None
         ident = bool((rows[1:] > rows[:-1]).all())         # local rows by global row: outputs leave in plan order
         order = None if ident else np.argsort(rows, kind="stable")
         self.perm_t = None if ident else D.h2d(order, None, device)
@@ -90,6 +91,11 @@ class _Block:
         tile = ((p.iy0[rows] * pxs_h) // 128 + 64) * 4096 + (p.ix0[rows] * pxs_h) // 128 + 64
         self.by_tile = np.argsort(tile, kind="stable").astype(np.int32)
         self.z_lo_t, self.z_hi_t = self.z_lo[self.by_tile], self.z_hi[self.by_tile]
+
+    def allocate(self, device):
+        """The zeroed shoebox arena (from the buffer pool) and bin counters: the block opens."""
+        self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device).zero_()
+        self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
 
     def rows_in(self, fi_a, fi_b):
         """Local rows whose box frame range meets [fi_a, fi_b]."""
@@ -259,6 +265,7 @@ class SweepRun:
         self.pass_index = 0
         self.pending = sorted(self.passes[0], key=lambda b: p.need_lo[b])
         self.opened, self.open_order = {}, []
+        self.prepared = {}                # blocks made ahead of their opening (prepare_ahead)
         self.det_cache = {}
         self.bkg_template = bkg_template
         self.mask_t = None
@@ -284,6 +291,7 @@ class SweepRun:
         # completed blocks (which then wait for their blocks' gathers only); blocks' pass-1 widths are taken when
         # their pass 1 runs, so early pass 1 (which takes them at block opening) is off
         self.gs = torch.cuda.Stream(device=device) if (overlap and not resident) else None
+        self.last_gathered = None
         if self.gs is not None:
             self.early_rows = 0
 
@@ -300,6 +308,20 @@ class SweepRun:
         sd_b = st["sd"] if self.adaptive else self.sd
         sm_b, rcw_b = (st["sm"], st["rcw"]) if self.adaptive else (self.sm, A.rc_default_weights())
         return sd_b, sm_b, rcw_b
+
+    def _prepare(self, b):
+        blk = _Block(b, self.plan.blocks_refl[b], self.plan, self.device)
+        blk.schedule(self.wedges, self.eff_hi[b], self.early_rows, self.device)
+        return blk
+
+    def prepare_ahead(self, n=1):
+        """Row tables and schedules of the next n blocks to open, made while the host would otherwise wait for the
+        device (their opening then only takes the arena)."""
+        t0 = time.perf_counter()
+        for b in self.pending[:n]:
+            if b not in self.prepared:
+                self.prepared[b] = self._prepare(b)
+        self._clock("prepare", t0)
 
     def block_pass1_consts(self, b, blk: _Block):
         """The block's pass-1 constants from the current widths (those adapted by every block processed before it),
@@ -348,8 +370,8 @@ class SweepRun:
         t0 = time.perf_counter()
         while self.pending and p.need_lo[self.pending[0]] <= fi_b:
             b = self.pending.pop(0)
-            blk = _Block(b, p.blocks_refl[b], p, self.device)
-            blk.schedule(self.wedges, self.eff_hi[b], self.early_rows, self.device)
+            blk = self.prepared.pop(b, None) or self._prepare(b)
+            blk.allocate(self.device)
             if self.early_rows and self.next_block(extra=b) == b:
                 self.block_pass1_consts(b, blk)
             self.opened[b] = blk
@@ -372,6 +394,7 @@ class SweepRun:
                 self._gather_wedge(w, ok, ok_t, fi_a, fi_b)
                 ev_w = torch.cuda.Event()
                 ev_w.record(self.gs)
+            self.last_gathered = ev_w             # the wedge's gathers (a scheduler's latency clock waits for them)
             for b in self.opened:
                 if w in self.opened[b].w_gather:
                     self.opened[b].gathered = ev_w
@@ -430,6 +453,7 @@ class SweepRun:
             raise RuntimeError("a pass starts after every block of the previous pass is processed")
         self.pass_index = k
         self.pending = sorted(self.passes[k], key=lambda b: self.plan.need_lo[b])
+        self.prepared = {}
         self.ok_off = 0
         self._gg = None
         if self.feeder is not None:
@@ -497,6 +521,8 @@ class SweepRun:
         if self.learn_profiles:
             D.accumulate(rs, p1, self.nreg, num, den)
         t0 = self._clock("learn_other", t0)
+        self.prepare_ahead()                               # host work while pass 1 of the block runs
+        t0 = time.perf_counter()
         h1 = _host_rows(p1.t, ADAPT_KEYS)
         t0 = self._clock("learn_wait", t0)                 # pass 1 of the block runs meanwhile
         rows = blk.rows

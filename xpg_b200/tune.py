@@ -2,10 +2,11 @@
 
 A batched launch sizes its shared memory, threads per CTA and staging for the largest box of its bin: wide bins
 put small boxes in CTAs sized for large ones (fewer resident CTAs), narrow bins make more launches (more tails). The
-CTA shape of large boxes (128 threads at 6 CTAs per SM, or 256 at 3) and the largest box staged in shared memory by
-a bulk copy trade resident reflections per SM against work per CTA. The tuner times pass 1 and pass 2 of real blocks
-for candidate bin edges (subsets of the box-side buckets present, at most `max_bins` bins) and launch shapes, and
-keeps the fastest; results are stored per device name in `tuned.json` beside this file, which the library applies
+CTA shape of large boxes (128 threads at 6 CTAs per SM, or 256 at 3), the largest box staged in shared memory by
+a bulk copy, and pass 2's fit-list capacity (the fitted voxels kept in shared memory for its six IRLS iterations;
+a row with more fits from the box each time) trade resident reflections per SM against work per CTA. The tuner
+times pass 1 and pass 2 of real blocks for launch shapes, then list capacities, then candidate bin edges (subsets of
+the box-side buckets present, at most `max_bins` bins), and keeps the fastest; results are stored per device name in `tuned.json` beside this file, which the library applies
 when it loads (`native.load`) and `device.batched_items` reads.
 
     python -m xpg_b200.tune [--workload config4|config2] [--max-bins 4]      (on the GPU)
@@ -54,10 +55,13 @@ SHAPES = ({"wide_threads": 256, "pass1_stage_bytes": 48 * 1024}, {"wide_threads"
           {"wide_threads": 128, "pass1_stage_bytes": 96 * 1024})
 
 
-def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES):
-    """Times the candidate launch shapes and bin sets on one batched round of completed blocks. picks: list of
-    (SweepRun, block) whose pass 1 and learning are done (their set entries valid). Returns [(seconds, bins, shape)]
-    fastest first."""
+LIST_CAPS = (2048, 4096, 8192, 12288, 16384)
+
+
+def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES, caps=LIST_CAPS):
+    """Times the candidate launch shapes, then pass 2's fit-list capacities, then bin sets on one batched round of
+    completed blocks. picks: list of (SweepRun, block) whose pass 1 and learning are done (their set entries valid).
+    Returns [(seconds, bins, shape)] fastest first."""
     from . import native as N
     sets1, sets2, groups = [], [], []
     for k, (run, b) in enumerate(picks):
@@ -75,7 +79,14 @@ def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES):
         N.tune(**shape)
         launches = D.batched_items(groups, base, device)
         out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base, shape))
-    best_shape = min(out, key=lambda r: r[0])[2]
+    best_shape = dict(min(out, key=lambda r: r[0])[2])
+    N.tune(**best_shape)
+    for cap in caps:                     # pass 2's fit-list capacity (rows whose list overflows fit from the box)
+        shape = dict(best_shape, pass2_list_cap=cap)
+        N.tune(**shape)
+        launches = D.batched_items(groups, base, device)
+        out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base, shape))
+    best_shape = dict(min(out, key=lambda r: r[0])[2])
     N.tune(**best_shape)
     for bins in candidates(sides, max_bins)[1:]:
         launches = D.batched_items(groups, bins, device)
