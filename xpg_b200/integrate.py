@@ -249,7 +249,7 @@ class SweepRun:
         self.state = dict(sd=self.sd, sm=self.sm, rcw=A.rc_default_weights())
         self.block_params, self.prof_by_block, self.block_widths = {}, {}, {}
         self.t_dev = 0.0
-        self.host_s = {}                  # host seconds per stage (waits for the device included)
+        self.host_s = {"plan": time.time() - self.t0}     # host seconds per stage (waits for the device included)
         nblocks = len(exp_blocks)
         self.read_fi = read_fi = np.array([f - 1 for f in range(f_first, f_last + 1) if f not in excl], np.int64)
         # a block takes every frame read up to the first frame read at or after its last needed frame
@@ -616,6 +616,7 @@ class SweepRun:
 
     def result(self):
         self.finish()
+        t0 = time.perf_counter()
         p, out, refl = self.plan, self.out, self.refl
         unfilled = np.ones(p.n, bool)                     # rows of blocks never processed: NaN, as XPG leaves them
         for b in self.processed:
@@ -638,6 +639,7 @@ class SweepRun:
             okk = np.isfinite(refl["iprf"])
             self.log(f"  INTEGRATE: {okk.sum()} reflections integrated in {time.time() - self.t0:.1f}s "
                      f"(device {self.t_dev:.1f}s)")
+        self._clock("result", t0)
         res = IntegrationResult(refl, self.model, self.prof_by_block, dict(total=time.time() - self.t0,
                                                                            gpu=self.t_dev,
                                                                            host_s=dict(self.host_s)))

@@ -141,10 +141,21 @@ def main():
     ap.add_argument("--workload", default="config4", choices=("config4", "config2"))
     ap.add_argument("--max-bins", type=int, default=4)
     args = ap.parse_args()
-    specs = synth.config4()[:6] if args.workload == "config4" else [synth.config2(nframes=480)]
+    specs = synth.config4() if args.workload == "config4" else [synth.config2(nframes=480)]
     jobs = bench._jobs_of(specs, bench.WEDGE_FRAMES)
-    runs = [SweepRun(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, early_pass1=False, verbose=False,
-                     **j.kwargs) for j in jobs]
+    from . import memplan
+    room = 0.9 * memplan.budget()
+    runs = []
+    for j in jobs:                        # up to 6 sweeps whose planned peaks fit the device together
+        run = SweepRun(j.images, j.exp_blocks, j.block_edges, j.model, j.dmin, early_pass1=False, verbose=False,
+                       mem_budget=room, **j.kwargs)
+        if run.mem["peak"] > room or "passes" in run.mem or run.mem["parts"] > 1:
+            run.close()
+            continue
+        room -= run.mem["peak"]
+        runs.append(run)
+        if len(runs) == 6:
+            break
     picks = []
     for run in runs:                      # the first completed block of every sweep
         done = []
