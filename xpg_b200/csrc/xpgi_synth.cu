@@ -31,12 +31,10 @@ __device__ __forceinline__ double unit_double(uint64_t h) {
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
-__device__ __forceinline__ bool in_gap(int y, int x, int gaps) {
-    if (!gaps) return false;
-    if (y >= 195 && ((y - 195) % 212) < 17) return true;
-    if (x >= 487 && ((x - 487) % 494) < 7) return true;
-    return false;
-}
+// module gaps: 17-row bands every 212 rows from row 195, 7-column bands every 494 columns from column 487
+__device__ __forceinline__ bool gap_row(int y, int gaps) { return gaps && y >= 195 && ((y - 195) % 212) < 17; }
+__device__ __forceinline__ bool gap_col(int x, int gaps) { return gaps && x >= 487 && ((x - 487) % 494) < 7; }
+__device__ __forceinline__ bool in_gap(int y, int x, int gaps) { return gap_row(y, gaps) || gap_col(x, gaps); }
 
 // Poisson draw of mean lam from one uniform u (inversion for small means, rounded normal approximation above 40,
 // with a second uniform from the same hash)
@@ -58,24 +56,30 @@ __device__ __forceinline__ uint32_t poisson_draw(float lam, uint64_t h) {
     return v <= 0.0f ? 0u : (v >= 4294967040.0f ? 0xFFFFFF00u : (uint32_t)v);
 }
 
-// background counts of every pixel of the wedge (flat level with a radial ramp), gaps flagged
+// background counts of every pixel of the wedge (flat level with a radial ramp), gaps flagged: CTAs stride over
+// (detector row, frame), threads over the row's pixels, so that every index is 32-bit arithmetic (the hash key is the
+// same 64-bit sum of frame and pixel index as a flat index would give)
 __global__ void k_background_counts(uint32_t* __restrict__ out, int first_frame, int n_frames, int ny, int nx,
                                     XiSynthBackground bg, uint64_t seed, int gaps) {
-    const size_t P = (size_t)ny * nx;
-    const size_t total = P * n_frames;
     const float ox = (float)bg.orgx, oy = (float)bg.orgy, lev = (float)bg.level, k = (float)(bg.ramp / bg.rmax);
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const size_t p = i % P;
-        const int f = first_frame + (int)(i / P);
-        const int y = (int)(p / nx), x = (int)(p % nx);
-        uint32_t c;
-        if (in_gap(y, x, gaps)) {
-            c = 0xFFFFFFFFu;
-        } else {
-            const float r = hypotf((float)x + 1.0f - ox, (float)y + 1.0f - oy);
-            c = poisson_draw(lev * (1.0f + k * r), mix64(seed * 0x9E3779B97F4A7C15ull + ((uint64_t)f << 40) + p));
+    for (int f = blockIdx.y; f < n_frames; f += gridDim.y) {
+        uint32_t* F = out + (size_t)f * ny * nx;
+        const uint64_t fkey = seed * 0x9E3779B97F4A7C15ull + ((uint64_t)(first_frame + f) << 40);
+        for (int y = blockIdx.x; y < ny; y += gridDim.x) {
+            const size_t row = (size_t)y * nx;
+            const bool gy = gap_row(y, gaps);
+            const float dy = (float)y + 1.0f - oy;
+            for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+                uint32_t c;
+                if (gy || gap_col(x, gaps)) {
+                    c = 0xFFFFFFFFu;
+                } else {
+                    const float r = hypotf((float)x + 1.0f - ox, dy);
+                    c = poisson_draw(lev * (1.0f + k * r), mix64(fkey + row + (size_t)x));
+                }
+                F[row + x] = c;
+            }
         }
-        out[i] = c;
     }
 }
 
@@ -144,7 +148,7 @@ int xi_synth_frames(const XiSynthSpots* spots, const XiSynthBackground* bg, int 
     }
     if (n_frames == 0) return XI_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    const int grid = 148 * 16;
+    const dim3 grid((unsigned)(ny < 296 ? ny : 296), (unsigned)(n_frames < 32 ? n_frames : 32));
     k_background_counts<<<grid, 256, 0, s>>>(out, first_frame, n_frames, ny, nx, *bg, seed, gaps);
     if (spots->n > 0) k_spot_counts<<<spots->n, 128, 0, s>>>(out, first_frame, n_frames, ny, nx, *spots, seed, gaps);
     cudaError_t e = cudaGetLastError();
