@@ -185,7 +185,8 @@ def workload_config(name, spec, edges, n_frames, plan, world):
             "phi_blocks": len(edges) - 1, "detector": [spec.nx, spec.ny],
             "voxels_per_step": int((plan.Dz * plan.bx.astype(np.int64) ** 2).sum()),
             "l2": f"inputs larger than L2 (frame stack {4 * P * n_frames / 1e9:.3g} GB of uint32)",
-            "parallelism": f"replicas x{world} (one sweep per rank)"}
+            "parallelism": f"replicas x{world} (one sweep per rank)",
+            "device_buffers": "kept between integrate() calls (xpg_b200.keep_buffers)"}
 
 
 def alg_bytes(spec, n_frames, plan):
@@ -409,6 +410,7 @@ def run(args):
         build.build()
     clocks = Clocks(local)
     clocks.start()                # before the set-up: nvidia-smi's start-up load stays out of the timed steps
+    D.keep_buffers(True)          # sweep after sweep: the pooled device buffers are kept between integrate() calls
     wl = Workload(args.workload, seed_offset=rank)
     src = wl.source()
     res = None

@@ -4,6 +4,7 @@ sm_100a CUDA kernels in libxpgi.so (C ABI: include/xpgi.h); `output` holds the s
 `xpg_integrated.npz` / `INTEGRATE.HKL` writers."""
 __version__ = "0.1.0"
 
+from .device import keep_buffers  # noqa: F401
 from .integrate import IntegrationResult, estimate_sigmas, integrate  # noqa: F401
 from .kernels import make_kernels  # noqa: F401
 from .plan import IntegrationModel  # noqa: F401

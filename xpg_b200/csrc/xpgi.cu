@@ -1684,7 +1684,7 @@ constexpr size_t kStageBudget = 190 * 1024;
 // Launch tuning (xi_tune): the largest shoebox each pass stages in shared memory, and the fit-list capacity of
 // pass 2. Larger staging overlaps the box read with the set-up but costs resident CTAs per SM.
 size_t g_stage_max[2] = {48 * 1024, 48 * 1024};
-int g_list_cap = 2048;
+int g_list_cap[2] = {2048, 8192};   // boxes up to XI_PASS2_LARGE_VOXELS voxels, larger boxes
 int g_wide_nt = 256;          // threads per CTA of the pass kernels for boxes over 200 pixels (128 or 256)
 
 // Pass 1 stages boxes of up to g_stage_max[0] bytes when they fit beside the per-pixel tables.
@@ -1696,7 +1696,9 @@ bool pass1_staged(size_t P, int max_dz) {
 // Pass 2's shared-memory plan for boxes up to max_bx pixels a side and max_dz bins with K neighbour columns: whether the box is
 // staged, and the fit list's capacity. The largest boxes (up to 97 px, 65 frames) take what the device allows a CTA
 // beyond the kernel's static arrays and the neighbour tables, not the default budget. The fit list holds up to every
-// voxel of small boxes and g_list_cap fitted voxels of large ones (less when shared memory is short; rows whose list
+// voxel of small boxes and g_list_cap fitted voxels of large ones (the second capacity for launches whose largest box
+// exceeds XI_PASS2_LARGE_VOXELS: deep boxes fit more voxels, whose rows would otherwise overflow a short list and
+// fit from the box in each later pass; fewer CTAs per SM pay less there; less when shared memory is short; rows whose list
 // overflows fit from the box); the box is staged only when small (it is read once: staging buys the copy's overlap
 // with the set-up, not re-reads).
 int pass2_plan(int max_bx, int max_dz, int K, const char* who, bool* staged, int* cap_out) {
@@ -1718,7 +1720,8 @@ int pass2_plan(int max_bx, int max_dz, int K, const char* who, bool* staged, int
             return fail(XI_E_LIMIT, "pass 2: box too large (per-pixel tables exceed shared memory)");
     }
     const size_t fit = (budget - pass2_pix_bytes((int)P, max_dz)) / 8 / 4 * 4;
-    size_t capz = V < (size_t)g_list_cap ? V : (size_t)g_list_cap;
+    const size_t want = (size_t)g_list_cap[V > (size_t)XI_PASS2_LARGE_VOXELS ? 1 : 0];
+    size_t capz = V < want ? V : want;
     if (capz > fit) capz = fit;
     *cap_out = (int)capz;
     const size_t base = pass2_stage_offset((int)P, max_dz, *cap_out);
@@ -1749,9 +1752,9 @@ int xi_tune(int key, long long value) {
         g_wide_nt = (int)value;
         return XI_OK;
     }
-    if (key == XI_TUNE_PASS2_LIST_CAP) {
+    if (key == XI_TUNE_PASS2_LIST_CAP || key == XI_TUNE_PASS2_LIST_CAP_LARGE) {
         if (value < 0 || value > 16384) return fail(XI_E_LIMIT, "xi_tune: list capacity");
-        g_list_cap = (int)value;
+        g_list_cap[key == XI_TUNE_PASS2_LIST_CAP ? 0 : 1] = (int)value;
         return XI_OK;
     }
     return fail(XI_E_ARG, "xi_tune: unknown key");

@@ -127,6 +127,7 @@ class BufferPool:
 
     def __init__(self):
         self.free = {}                 # (device index, dtype) -> [tensor]
+        self.persist = False           # kept buffers outlive a run (keep_buffers)
 
     def take(self, n, dtype, device):
         dev = torch.device(device)
@@ -163,6 +164,17 @@ class BufferPool:
 
 
 POOL = BufferPool()
+
+
+def keep_buffers(on=True):
+    """Keeps the pooled device buffers (shoebox arenas, pass-1 tables, frame wedges; tens of GB) from one
+    integration to the next, for callers that integrate sweep after sweep on a device of their own: the next run
+    takes them instead of allocating anew. Off by default: a run then gives its buffers and the allocator's cached
+    memory back to the device when it returns. `keep_buffers(False)` also releases what is kept."""
+    POOL.persist = bool(on)
+    if not on:
+        POOL.clear()
+        torch.cuda.empty_cache()
 
 
 def h2d(a, dtype=None, device="cuda"):

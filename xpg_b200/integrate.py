@@ -658,8 +658,9 @@ class SweepRun:
         if self.src is not None and getattr(self.src, "_buf", None) is not None:
             D.POOL.give(self.src._buf)
             self.src._buf = None
-        D.POOL.clear()                        # the kept arenas go back to the allocator between runs
-        torch.cuda.empty_cache()              # and to the device: the next run's small buffers must not split them
+        if not D.POOL.persist:
+            D.POOL.clear()                    # the kept arenas go back to the allocator between runs
+            torch.cuda.empty_cache()          # and to the device: the next run's small buffers must not split them
 
 
 ADAPT_KEYS = ("isum", "vsum", "n_over", "frac_rec", "m_d")

@@ -159,6 +159,7 @@ class XiHklRows(C.Structure):
 
 
 XI_TUNE_PASS1_STAGE_BYTES, XI_TUNE_PASS2_STAGE_BYTES, XI_TUNE_PASS2_LIST_CAP, XI_TUNE_WIDE_THREADS = 1, 2, 3, 4
+XI_TUNE_PASS2_LIST_CAP_LARGE, XI_PASS2_LARGE_VOXELS = 5, 49152
 XI_PACK_ESCAPE, XI_PACK_FLAGGED = 254, 255
 
 EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_status_copy", "xi_tune", "xi_gather", "xi_decode_bins",
@@ -251,7 +252,8 @@ def _apply_tuned(lib):
     if not shape:
         return
     keys = {"wide_threads": XI_TUNE_WIDE_THREADS, "pass1_stage_bytes": XI_TUNE_PASS1_STAGE_BYTES,
-            "pass2_stage_bytes": XI_TUNE_PASS2_STAGE_BYTES, "pass2_list_cap": XI_TUNE_PASS2_LIST_CAP}
+            "pass2_stage_bytes": XI_TUNE_PASS2_STAGE_BYTES, "pass2_list_cap": XI_TUNE_PASS2_LIST_CAP,
+            "pass2_list_cap_large": XI_TUNE_PASS2_LIST_CAP_LARGE}
     for k, v in shape.items():
         if k in keys:
             lib.xi_tune(keys[k], int(v))
@@ -283,9 +285,12 @@ def require_cuda():
     load()
 
 
-def tune(pass1_stage_bytes=None, pass2_stage_bytes=None, pass2_list_cap=None, wide_threads=None):
+def tune(pass1_stage_bytes=None, pass2_stage_bytes=None, pass2_list_cap=None, wide_threads=None,
+         pass2_list_cap_large=None):
     """Launch tuning of the pass kernels (results are independent of it)."""
     lib = load()
+    if pass2_list_cap_large is not None:
+        check(lib.xi_tune(XI_TUNE_PASS2_LIST_CAP_LARGE, int(pass2_list_cap_large)), "xi_tune")
     if wide_threads is not None:
         check(lib.xi_tune(XI_TUNE_WIDE_THREADS, int(wide_threads)), "xi_tune")
     if pass1_stage_bytes is not None:

@@ -56,6 +56,13 @@ SHAPES = ({"wide_threads": 256, "pass1_stage_bytes": 48 * 1024}, {"wide_threads"
 
 
 LIST_CAPS = (2048, 4096, 8192, 12288, 16384)
+CAP_DEFAULTS = {"pass2_list_cap": 2048, "pass2_list_cap_large": 8192}
+
+
+def _apply(shape):
+    """Sets a launch shape, the list capacities it does not name at their defaults."""
+    from . import native as N
+    N.tune(**dict(CAP_DEFAULTS, **shape))
 
 
 def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES, caps=LIST_CAPS):
@@ -76,18 +83,20 @@ def tune_round(picks, max_bins=4, reps=3, device="cuda", shapes=SHAPES, caps=LIS
     out = []
     base = candidates(sides, 1)[0]
     for shape in shapes:                 # launch shape first, on one bin of all sides
-        N.tune(**shape)
+        _apply(shape)
         launches = D.batched_items(groups, base, device)
         out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base, shape))
     best_shape = dict(min(out, key=lambda r: r[0])[2])
-    N.tune(**best_shape)
-    for cap in caps:                     # pass 2's fit-list capacity (rows whose list overflows fit from the box)
-        shape = dict(best_shape, pass2_list_cap=cap)
-        N.tune(**shape)
-        launches = D.batched_items(groups, base, device)
-        out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base, shape))
-    best_shape = dict(min(out, key=lambda r: r[0])[2])
-    N.tune(**best_shape)
+    _apply(best_shape)
+    for key in ("pass2_list_cap", "pass2_list_cap_large"):   # pass 2's fit-list capacities (small, large boxes)
+        for cap in caps:
+            shape = dict(best_shape, **{key: cap})
+            _apply(shape)
+            launches = D.batched_items(groups, base, device)
+            out.append((_time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps), base,
+                        shape))
+        best_shape = dict(min(out, key=lambda r: r[0])[2])
+        _apply(best_shape)
     for bins in candidates(sides, max_bins)[1:]:
         launches = D.batched_items(groups, bins, device)
         t = _time(lambda: (D.pass1_batched(t1, launches), D.pass2_batched(t2, launches)), reps)
