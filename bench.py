@@ -474,6 +474,7 @@ def run(args):
     # end to end: frames from pinned host memory, uploaded inside every step; results read back by the API
     e2e = None
     if not args.no_e2e:
+        src = None                # the resident source holds the HBM copy of the packed frames
         wl.drop_resident()
         hsrc = wl.host_source()
         res = wl.integrate(hsrc)

@@ -154,14 +154,15 @@ int xi_status_copy(int *host_dst, void *stream);
 
 /* Launch tuning (process-wide; no counterpart in XPG, whose torch kernels have no launch shape): the largest
  * shoebox (bytes) pass 1 / pass 2 stage in shared memory, pass 2's fit-list capacity (voxels) for launches whose
- * largest box is up to XI_PASS2_LARGE_VOXELS voxels and for larger ones, and the CTA width of large boxes. Results
- * do not depend on these. */
+ * largest box is up to XI_PASS2_LARGE_VOXELS voxels and XI_PASS2_LARGE_DEPTH bins deep and for larger ones, and the
+ * CTA width of large boxes. Results do not depend on these. */
 #define XI_TUNE_PASS1_STAGE_BYTES 1
 #define XI_TUNE_PASS2_STAGE_BYTES 2
 #define XI_TUNE_PASS2_LIST_CAP 3
 #define XI_TUNE_WIDE_THREADS 4      /* threads per CTA of the pass kernels for boxes over 200 pixels: 128 or 256 */
 #define XI_TUNE_PASS2_LIST_CAP_LARGE 5
 #define XI_PASS2_LARGE_VOXELS 49152
+#define XI_PASS2_LARGE_DEPTH 33
 int xi_tune(int key, long long value);
 
 /* Frame gather (xpg/integrate.py:704-787 with the preparation of :667-699 and the encoding of

@@ -27,3 +27,17 @@ def test_pool_reuses_buffers_of_about_the_size_asked():
     assert e._base is not base and not pool.free[(None, torch.float32)]
     pool.clear()
     assert not pool.free
+
+
+def test_pool_retains_only_buffers_a_run_can_take():
+    pool = BufferPool()
+    a = pool.take(100_000, torch.float32, "cpu")
+    b = pool.take(10_000, torch.float32, "cpu")
+    c = pool.take(5_000, torch.uint8, "cpu")
+    pool.give(a)
+    pool.give(b)
+    pool.give(c)
+    pool.retain({torch.float32: [95_000]})            # the next run's arenas: about a's size; no uint8 request
+    kept = pool.free[(None, torch.float32)]
+    assert len(kept) == 1 and kept[0] is a._base
+    assert not pool.free[(None, torch.uint8)]

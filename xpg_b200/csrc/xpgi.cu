@@ -339,7 +339,10 @@ constexpr int kGatherBatch = 8;     // frames of a box pixel read together by th
 __host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * P + 15) / 16 * 16; }
 
 // resident CTAs per SM the pass kernels are compiled for (registers per thread <= 65536 / (NT * blocks))
-template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 6 : 8); }
+#ifndef XI_MIN_CTAS_256
+#define XI_MIN_CTAS_256 3
+#endif
+template <int NT> constexpr int min_ctas() { return NT == 256 ? XI_MIN_CTAS_256 : (NT == 128 ? 6 : 8); }
 
 // Pass 1 of one row, by the whole CTA. `bar`: the CTA's bulk-copy barrier (initialised once per CTA), `phase`: its
 // next phase (advanced here when the row is staged by a bulk copy). The caller separates consecutive rows of a CTA
@@ -1697,7 +1700,8 @@ bool pass1_staged(size_t P, int max_dz) {
 // staged, and the fit list's capacity. The largest boxes (up to 97 px, 65 frames) take what the device allows a CTA
 // beyond the kernel's static arrays and the neighbour tables, not the default budget. The fit list holds up to every
 // voxel of small boxes and g_list_cap fitted voxels of large ones (the second capacity for launches whose largest box
-// exceeds XI_PASS2_LARGE_VOXELS: deep boxes fit more voxels, whose rows would otherwise overflow a short list and
+// exceeds XI_PASS2_LARGE_VOXELS voxels or XI_PASS2_LARGE_DEPTH bins: such boxes fit more voxels (a deep rocking curve
+// keeps many frames above the profile threshold), whose rows would otherwise overflow a short list and
 // fit from the box in each later pass; fewer CTAs per SM pay less there; less when shared memory is short; rows whose list
 // overflows fit from the box); the box is staged only when small (it is read once: staging buys the copy's overlap
 // with the set-up, not re-reads).
@@ -1720,7 +1724,8 @@ int pass2_plan(int max_bx, int max_dz, int K, const char* who, bool* staged, int
             return fail(XI_E_LIMIT, "pass 2: box too large (per-pixel tables exceed shared memory)");
     }
     const size_t fit = (budget - pass2_pix_bytes((int)P, max_dz)) / 8 / 4 * 4;
-    const size_t want = (size_t)g_list_cap[V > (size_t)XI_PASS2_LARGE_VOXELS ? 1 : 0];
+    const bool large = V > (size_t)XI_PASS2_LARGE_VOXELS || max_dz > XI_PASS2_LARGE_DEPTH;
+    const size_t want = (size_t)g_list_cap[large ? 1 : 0];
     size_t capz = V < want ? V : want;
     if (capz > fit) capz = fit;
     *cap_out = (int)capz;

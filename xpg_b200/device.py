@@ -148,6 +148,19 @@ class BufferPool:
             torch.cuda.empty_cache()
             return torch.empty(n, dtype=dtype, device=dev)
 
+    def retain(self, wanted):
+        """Keeps only the kept buffers that one of the requests `wanted` ({dtype: [element counts]}) would take; the
+        others go back to the device (a run whose buffers differ in size from the last run's)."""
+        dropped = False
+        for (_, dt), pool in self.free.items():
+            sizes = wanted.get(dt, ())
+            keep = [t for t in pool if any(n <= t.numel() <= self.FIT * n + 4096 for n in sizes)]
+            if len(keep) != len(pool):
+                pool[:] = keep
+                dropped = True
+        if dropped:
+            torch.cuda.empty_cache()
+
     def give(self, t):
         if t is None:
             return
