@@ -105,3 +105,15 @@ def test_served_slots_plan_each_sweep_in_its_share():
     for c, a, b in zip(cases, alone, res):
         assert b.memory["parts"] == a.memory["parts"] and "passes" not in b.memory
         _same(a, b, c)
+
+
+def test_concurrent_results_equal_alone():
+    """Sweeps integrated on three host threads at once (each the plain path on streams of its own, sharing the
+    device and the buffer pool): the same bits as each sweep integrated alone."""
+    from xpg_b200.batch import integrate_concurrent
+    jobs = [_job(c) for c in CASES]
+    alone = [_alone(j) for j in jobs]
+    res, stats = integrate_concurrent(jobs, workers=3)
+    assert len(stats["admitted_at"]) == len(jobs)
+    for c, a, b in zip(CASES, alone, res):
+        _same(a, b, c)

@@ -243,6 +243,59 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
     return results, stats
 
 
+def integrate_concurrent(jobs, budget_bytes=None, workers=3, device="cuda"):
+    """Integrates every job (all frames available) on `workers` host threads, each running the plain path of one
+    sweep at a time (`integrate.drive`) on streams of its own: one sweep's host stages (planning, adaptation,
+    result assembly) and waits for its own device work overlap the other sweeps' device work. Each sweep is planned
+    for the whole budget, exactly as `integrate(..., mem_budget=budget_bytes)` plans it, and starts once its planned
+    peak fits beside the running sweeps' (the largest runs alone), so every result is the same bits as the sweep
+    integrated alone under that budget. Returns (results in job order, stats)."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .integrate import drive
+    budget = budget_bytes if budget_bytes is not None else memplan.budget(device)
+    cond = threading.Condition()
+    state = dict(used=0, running=0, peak=0)
+    results = [None] * len(jobs)
+    t0 = time.perf_counter()
+    stats = dict(admitted_at={}, peak_bytes=0, workers=workers)
+
+    def work(i):
+        job = jobs[i]
+        dev = torch.device(device)
+        with torch.cuda.device(dev if dev.index is not None else torch.cuda.current_device()):
+            stream = torch.cuda.Stream()
+            with torch.cuda.stream(stream):
+                run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, verbose=False,
+                               device=device, mem_budget=budget, overlap=True, **job.kwargs)
+                need = int(run.mem["peak"])
+                try:
+                    with cond:
+                        while state["running"] and state["used"] + need > budget:
+                            cond.wait()
+                        state["used"] += need
+                        state["running"] += 1
+                        stats["peak_bytes"] = max(stats["peak_bytes"], state["used"])
+                        stats["admitted_at"][i] = time.perf_counter() - t0
+                    try:
+                        results[i] = drive(run)
+                    finally:
+                        with cond:
+                            state["used"] -= need
+                            state["running"] -= 1
+                            cond.notify_all()
+                finally:
+                    run.close()
+            stream.synchronize()
+
+    with ThreadPoolExecutor(max_workers=max(int(workers), 1)) as ex:
+        for f in [ex.submit(work, i) for i in range(len(jobs))]:
+            f.result()
+    stats["seconds"] = time.perf_counter() - t0
+    return results, stats
+
+
 def integrate_batch(jobs, budget_bytes=None, bins=None, device="cuda"):
     """Integrates every job (all frames available) with batched rounds; results in job order."""
     res, stats = run_jobs(jobs, budget_bytes, bins, device)

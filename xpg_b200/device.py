@@ -118,8 +118,10 @@ class BufferPool:
     block; here a request takes the smallest kept buffer that holds it (a view of its first elements) if that is at
     most FIT times the request (a small block holding a large buffer would leave the next large block to allocate
     anew, beyond what the memory plan counts), else a new one allocated SLACK larger than asked (so that later blocks
-    of about the same size fit), and `give` returns it. A buffer is given back only once no queued work uses it any
-    more, or when the next user writes it on the same stream (stream order)."""
+    of about the same size fit), and `give` returns it. A buffer is given back once every kernel that uses it is
+    queued: `give` records an event on the giver's stream, the next taker's stream waits for it, and the taker's
+    stream is recorded on the buffer (so that the allocator keeps it until that stream's work is done when it is
+    freed), which keeps reuse safe across the streams of several host threads."""
 
     SLACK = 1.05
     FIT = 1.3
@@ -128,8 +130,14 @@ class BufferPool:
     def __init__(self):
         self.free = {}                 # (device index, dtype) -> [tensor]
         self.persist = False           # kept buffers outlive a run (keep_buffers)
+        self.lock = threading.RLock()  # sweeps integrated on several host threads share the pool
+        self.ready = {}                # id(buffer) -> event recorded when it was given back
 
     def take(self, n, dtype, device):
+        with self.lock:
+            return self._take(n, dtype, device)
+
+    def _take(self, n, dtype, device):
         dev = torch.device(device)
         if dev.type == "cuda" and dev.index is None:
             dev = torch.device("cuda", torch.cuda.current_device())
@@ -138,12 +146,24 @@ class BufferPool:
         fits = [i for i, t in enumerate(pool) if n <= t.numel() <= self.FIT * n + 4096]
         if fits:
             i = min(fits, key=lambda j: pool[j].numel())
-            return pool.pop(i)[:n]
-        pool[:] = [t for t in pool if t.numel() > n]     # kept buffers too small for this request: memory back first
+            base = pool.pop(i)
+            ev = self.ready.pop(id(base), None)
+            if base.is_cuda:
+                st = torch.cuda.current_stream(base.device)
+                if ev is not None:
+                    st.wait_event(ev)
+                base.record_stream(st)
+            return base[:n]
+        for t in pool:                                    # kept buffers too small for this request: memory back first
+            if t.numel() <= n:
+                self.ready.pop(id(t), None)
+        pool[:] = [t for t in pool if t.numel() > n]
         size = max(int(n * self.SLACK), 1)
         try:
             return torch.empty(size, dtype=dtype, device=dev)[:n]
         except torch.OutOfMemoryError:
+            for t in pool:
+                self.ready.pop(id(t), None)
             pool.clear()                # the kept buffers: let the allocator have their memory
             torch.cuda.empty_cache()
             return torch.empty(n, dtype=dtype, device=dev)
@@ -151,10 +171,17 @@ class BufferPool:
     def retain(self, wanted):
         """Keeps only the kept buffers that one of the requests `wanted` ({dtype: [element counts]}) would take; the
         others go back to the device (a run whose buffers differ in size from the last run's)."""
+        with self.lock:
+            self._retain(wanted)
+
+    def _retain(self, wanted):
         dropped = False
         for (_, dt), pool in self.free.items():
             sizes = wanted.get(dt, ())
             keep = [t for t in pool if any(n <= t.numel() <= self.FIT * n + 4096 for n in sizes)]
+            for t in pool:
+                if not any(t is k for k in keep):
+                    self.ready.pop(id(t), None)
             if len(keep) != len(pool):
                 pool[:] = keep
                 dropped = True
@@ -164,16 +191,28 @@ class BufferPool:
     def give(self, t):
         if t is None:
             return
+        with self.lock:
+            self._give(t)
+
+    def _give(self, t):
         base = t._base if t._base is not None else t
         key = (base.device.index, base.dtype)
         pool = self.free.setdefault(key, [])
         if not any(x is base for x in pool):
             pool.append(base)
+            if base.is_cuda:
+                ev = torch.cuda.Event()
+                ev.record(torch.cuda.current_stream(base.device))
+                self.ready[id(base)] = ev
         pool.sort(key=lambda x: -x.numel())
+        for x in pool[self.KEEP:]:
+            self.ready.pop(id(x), None)
         del pool[self.KEEP:]
 
     def clear(self):
-        self.free.clear()
+        with self.lock:
+            self.free.clear()
+            self.ready.clear()
 
 
 POOL = BufferPool()

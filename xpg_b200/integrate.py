@@ -157,27 +157,34 @@ def integrate(images, exp_blocks, block_edges, model: IntegrationModel, dmin, dm
                    bkg_template, foreign_spots, n_foreign, moments_only, wedge_frames=wedge_frames, device=device,
                    allowed=allowed, graphs=graphs, mem_budget=mem_budget, overlap=overlap)
     try:
-        ahead = LOOKAHEAD if run.gs is not None else 0
-        done = []                                    # (block, wedge that completed it), in processing order
-        for w in range(len(run.wedges)):
-            done += [(b, w) for b in run.feed(w)]
-            while done and w - done[0][1] >= ahead:  # later wedges' gathers are queued before a block's passes
-                run.process(done.pop(0)[0])
-            run.early_pass1(w)
-        for b, _ in done:
-            run.process(b)
-        for b in run.remaining():
-            run.process(b)
-        for k in range(1, run.n_passes):             # blocks that did not fit in one pass over the frames
-            run.start_pass(k)
-            for w in range(len(run.wedges)):
-                for b in run.feed(w):
-                    run.process(b)
-            for b in run.remaining():
-                run.process(b)
-        return run.result()
+        return drive(run)
     finally:
         run.close()
+
+
+def drive(run):
+    """Runs a planned sweep (`SweepRun`) through its frame loop and returns its result: wedges fed in order, each
+    completed block processed once the gathers of LOOKAHEAD later wedges are queued (overlap mode), then the blocks
+    left open, then further passes over the frames when the memory plan asks for them."""
+    ahead = LOOKAHEAD if run.gs is not None else 0
+    done = []                                        # (block, wedge that completed it), in processing order
+    for w in range(len(run.wedges)):
+        done += [(b, w) for b in run.feed(w)]
+        while done and w - done[0][1] >= ahead:      # later wedges' gathers are queued before a block's passes
+            run.process(done.pop(0)[0])
+        run.early_pass1(w)
+    for b, _ in done:
+        run.process(b)
+    for b in run.remaining():
+        run.process(b)
+    for k in range(1, run.n_passes):                 # blocks that did not fit in one pass over the frames
+        run.start_pass(k)
+        for w in range(len(run.wedges)):
+            for b in run.feed(w):
+                run.process(b)
+        for b in run.remaining():
+            run.process(b)
+    return run.result()
 
 
 class SweepRun:
