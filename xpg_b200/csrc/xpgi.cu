@@ -339,10 +339,10 @@ constexpr int kGatherBatch = 8;     // frames of a box pixel read together by th
 __host__ __device__ inline size_t pass1_pix_bytes(int P) { return ((size_t)18 * P + 15) / 16 * 16; }
 
 // resident CTAs per SM the pass kernels are compiled for (registers per thread <= 65536 / (NT * blocks))
-#ifndef XI_MIN_CTAS_256
-#define XI_MIN_CTAS_256 3
-#endif
-template <int NT> constexpr int min_ctas() { return NT == 256 ? XI_MIN_CTAS_256 : (NT == 128 ? 6 : 8); }
+// Pass 1 takes four 256-thread CTAs per SM (64 registers; measured 9% faster than three at 80 on the config-2 block
+// and on deep config-4 boxes), pass 2 three (four makes it 5% slower: its spills cost more than the occupancy buys).
+template <int NT> constexpr int min_ctas() { return NT == 256 ? 3 : (NT == 128 ? 6 : 8); }
+template <int NT> constexpr int min_ctas_pass1() { return NT == 256 ? 4 : min_ctas<NT>(); }
 
 // Pass 1 of one row, by the whole CTA. `bar`: the CTA's bulk-copy barrier (initialised once per CTA), `phase`: its
 // next phase (advanced here when the row is staged by a bulk copy). The caller separates consecutive rows of a CTA
@@ -816,7 +816,7 @@ __device__ __forceinline__ void pass1_row(const XiDetector& det_g, const XiRows&
 
 // Pass 1, one CTA per row of `order` (one shoebox shape group per launch).
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1(XiDetector det_g, XiRows R, XiBlock B,
+__global__ void __launch_bounds__(NT, min_ctas_pass1<NT>()) k_pass1(XiDetector det_g, XiRows R, XiBlock B,
                                                               const float* __restrict__ arena, XiPass1Out O,
                                                               const int32_t* __restrict__ order, int max_bx,
                                                               int max_dz, int* status) {
@@ -841,7 +841,7 @@ __device__ __forceinline__ void load_set(const XiRowSet* __restrict__ sets, int 
 // Pass 1 over a queue of (set, row) items: resident CTAs take items in queue order until it is empty, so rows of
 // any blocks and sweeps (of one size bin) share one launch with no tail between shape groups.
 template <int NT, bool STAGED>
-__global__ void __launch_bounds__(NT, min_ctas<NT>()) k_pass1_q(const XiRowSet* __restrict__ sets,
+__global__ void __launch_bounds__(NT, min_ctas_pass1<NT>()) k_pass1_q(const XiRowSet* __restrict__ sets,
                                                                 const int64_t* __restrict__ items, int n_items,
                                                                 int max_bx, int max_dz, int max_k, int* queue,
                                                                 int* status) {
