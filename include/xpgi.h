@@ -189,6 +189,12 @@ int xi_gather_step(const XiGatherStep *step, const XiGatherRows *rows, float *ar
  * given), once each, after their last frame has been gathered. */
 int xi_decode_bins(const XiGatherRows *rows, float *arena, const int32_t *cnt, void *stream);
 
+/* Zeroes the arena slots (Dz * bx^2 floats, rounded up to 4; 0 = unrecorded) of the rows (of rows->order when
+ * given): the rows a block's gathers do not write in full (binned rows, which accumulate; rows whose frames reach
+ * beyond the integrated range). XPG allocates its buffers zeroed (xpg/integrate.py:372-398); here the other rows'
+ * slots are written whole by the gathers, so only these need clearing. `arena` on 16 bytes. */
+int xi_zero_rows(const XiGatherRows *rows, float *arena, void *stream);
+
 /* Pass 1 (xpg/integrate_kernels.py:287-365): pixel geometry, masks, robust background, summation, centroids,
  * moments and the projected 2D spot of every row. */
 int xi_pass1(const XiDetector *det, const XiRows *rows, const XiBlock *blk, const float *arena, XiPass1Out *out,

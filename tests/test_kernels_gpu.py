@@ -296,3 +296,29 @@ def test_batched_passes_match_per_shape_launches():
                 assert same(a1.t[k], b1.t[k]), (n, bins, k)
             for k in a2.t:
                 assert same(a2.t[k], b2.t[k]), (n, bins, k)
+
+
+def test_zero_rows_clears_only_the_listed_slots():
+    """xi_zero_rows: the listed rows' slots (Dz * bx^2 floats rounded up to 4) read 0, every other float keeps its
+    value."""
+    import ctypes as C
+
+    import torch
+    from xpg_b200 import native as N
+    Dz = np.array([2, 3, 1, 4], np.int32)
+    bx = np.array([3, 2, 5, 1], np.int32)
+    slot = (Dz.astype(np.int64) * bx * bx + 3) // 4 * 4
+    off = np.concatenate([[0], np.cumsum(slot)[:-1]]).astype(np.int64)
+    arena = torch.full((int(slot.sum()) + 4,), 7.0, dtype=torch.float32, device="cuda")
+    t = {k: torch.from_numpy(v).cuda() for k, v in dict(Dz=Dz, bx=bx, sb_off=off).items()}
+    order = torch.tensor([1, 3], dtype=torch.int32, device="cuda")
+    g = N.XiGatherRows()
+    g.n = 4
+    g.Dz, g.bx, g.sb_off = N.ptr(t["Dz"]), N.ptr(t["bx"]), N.ptr(t["sb_off"])
+    g.order, g.n_order = N.ptr(order), 2
+    N.check(N.load().xi_zero_rows(C.byref(g), N.ptr(arena), N.stream_handle()), "xi_zero_rows")
+    a = arena.cpu().numpy()
+    want = np.full(a.size, 7.0, np.float32)
+    for r in (1, 3):
+        want[off[r]:off[r] + slot[r]] = 0.0
+    np.testing.assert_array_equal(a, want)

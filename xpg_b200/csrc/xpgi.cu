@@ -1496,6 +1496,17 @@ __global__ void k_decode_bins(XiGatherRows G, float* __restrict__ arena, const i
     }
 }
 
+// zero the arena slots of the listed rows (rows the gather does not write in full: binned rows accumulate, rows whose
+// frames reach beyond the run's). A row's slot is Dz * bx^2 floats rounded up to 4 and starts on 16 bytes.
+__global__ void k_zero_rows(XiGatherRows G, float* __restrict__ arena) {
+    const int row = G.order ? G.order[blockIdx.x] : blockIdx.x;
+    const int64_t v = (int64_t)G.Dz[row] * G.bx[row] * G.bx[row];
+    const int64_t n4 = (v + 3) / 4;
+    float4* a = reinterpret_cast<float4*>(arena + G.sb_off[row]);
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int64_t i = threadIdx.x; i < n4; i += blockDim.x) a[i] = z;
+}
+
 // ==================================================================================================================
 // profile accumulation and finalisation
 // ==================================================================================================================
@@ -1906,6 +1917,15 @@ int xi_decode_bins(const XiGatherRows* G, float* arena, const int32_t* cnt, void
     if (nblk <= 0) return XI_OK;
     k_decode_bins<<<nblk, 256, 0, (cudaStream_t)stream>>>(*G, arena, cnt);
     return cuda_check("xi_decode_bins");
+}
+
+int xi_zero_rows(const XiGatherRows* G, float* arena, void* stream) {
+    if (!G || !arena) return fail(XI_E_ARG, "xi_zero_rows: null argument");
+    const int nblk = G->order ? G->n_order : G->n;
+    if (nblk <= 0) return XI_OK;
+    if (((uintptr_t)arena & 15) != 0) return fail(XI_E_ARG, "xi_zero_rows: arena not on 16 bytes");
+    k_zero_rows<<<nblk, 256, 0, (cudaStream_t)stream>>>(*G, arena);
+    return cuda_check("xi_zero_rows");
 }
 
 int xi_accumulate(const XiRows* R, const XiPass1Out* p1, const uint8_t* sel, int strong_test, int n_regions,

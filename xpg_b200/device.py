@@ -595,6 +595,11 @@ def decode_bins(grows: GatherRows, arena, cnt, stream=None, order=None):
         N.check(lib.xi_decode_bins(C.byref(g), N.ptr(arena), N.ptr(cnt), _stream(stream)), "xi_decode_bins")
 
 
+def zero_rows(grows: GatherRows, arena, order, stream=None):
+    """Zeroes the arena slots of the rows in the device int32 `order` (xi_zero_rows)."""
+    N.check(N.load().xi_zero_rows(C.byref(grows.view(order)), N.ptr(arena), _stream(stream)), "xi_zero_rows")
+
+
 def host_groups(rows: RowSet, idx):
     """Launch groups (as RowSet.groups: one shape each, largest first) of the local rows idx, as host int32 arrays."""
     idx = np.asarray(idx, np.int64)

@@ -92,9 +92,17 @@ class _Block:
         self.by_tile = np.argsort(tile, kind="stable").astype(np.int32)
         self.z_lo_t, self.z_hi_t = self.z_lo[self.by_tile], self.z_hi[self.by_tile]
 
-    def allocate(self, device):
-        """The zeroed shoebox arena (from the buffer pool) and bin counters: the block opens."""
-        self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device).zero_()
+    def allocate(self, device, f_lo, f_hi, zero_all):
+        """The shoebox arena (from the buffer pool) and bin counters: the block opens. A slot must read 0 wherever no
+        frame is gathered into it; the gathers write every slot of a plain row whose frames lie inside the integrated
+        range [f_lo, f_hi] (frame indices) in full, so only the others are cleared: binned rows (they accumulate) and
+        rows reaching beyond the range, or every row when frames are excluded."""
+        self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device)
+        need = self.grows.binned | (self.z_lo < f_lo) | (self.z_hi > f_hi)
+        if zero_all or need.all():
+            self.arena.zero_()
+        elif need.any():
+            D.zero_rows(self.grows, self.arena, D.h2d(np.flatnonzero(need).astype(np.int32), None, device))
         self.cnt = torch.zeros(max(self.grows.n_cnt, 1), dtype=torch.int32, device=device)
 
     def rows_in(self, fi_a, fi_b):
@@ -221,6 +229,8 @@ class SweepRun:
         W = (f_last - f_first + 1) if resident else max(int(wedge_frames), 1)    # resident: one wedge, one gather
         self.wedges = [(f, min(f + W - 1, f_last)) for f in range(f_first, f_last + 1, max(W, 1))]
         self.oks = [np.array([(g_ not in excl) for g_ in range(fa, fb + 1)], bool) for fa, fb in self.wedges]
+        self.f_range = (f_first - 1, f_last - 1)              # frame indices the run integrates
+        self.any_excluded = not all(ok.all() for ok in self.oks)
         self.src = src
         self.feeder = src.feeder(self.wedges, self.oks) if (hasattr(src, "feeder") and not resident) else None
         self.device, self.model, self.verbose, self.log = device, model, verbose, log
@@ -382,7 +392,7 @@ class SweepRun:
         while self.pending and p.need_lo[self.pending[0]] <= fi_b:
             b = self.pending.pop(0)
             blk = self.prepared.pop(b, None) or self._prepare(b)
-            blk.allocate(self.device)
+            blk.allocate(self.device, self.f_range[0], self.f_range[1], self.any_excluded)
             if self.early_rows and self.next_block(extra=b) == b:
                 self.block_pass1_consts(b, blk)
             self.opened[b] = blk

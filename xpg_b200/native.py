@@ -167,7 +167,8 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_status_copy", "xi_tun
            "xi_plan_boxes", "xi_knn", "xi_knn_noalloc", "xi_rocking_costs", "xi_rocking_gram",
            "xi_predict_workspace", "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8",
            "xi_upload", "xi_bslz4_lz4_stage", "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong",
-           "xi_spot_workspace", "xi_pass1_batched", "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames")
+           "xi_spot_workspace", "xi_pass1_batched", "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames",
+           "xi_zero_rows")
 
 _LIB = None
 
@@ -219,6 +220,7 @@ def load(path=None):
     lib.xi_tune.argtypes = [C.c_int, C.c_longlong]
     lib.xi_gather.argtypes = [C.POINTER(XiFrames), C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.xi_decode_bins.argtypes = [C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.xi_zero_rows.argtypes = [C.POINTER(XiGatherRows), C.c_void_p, C.c_void_p]
     lib.xi_pass1.argtypes = [C.POINTER(XiDetector), C.POINTER(XiRows), C.POINTER(XiBlock), C.c_void_p,
                              C.POINTER(XiPass1Out), C.c_void_p]
     lib.xi_accumulate.argtypes = [C.POINTER(XiRows), C.POINTER(XiPass1Out), C.c_void_p, C.c_int, C.c_int,
