@@ -287,7 +287,7 @@ class Workload:
 # DRAM bytes (read + write) per shoebox voxel of the pass kernels, from one ncu capture of a launch of the same
 # kernels on the config-2 geometry (a 20-frame block, `--workload config2-small`: the 2,597-reflection launch of
 # 31 x 31 x 33 boxes, 82.4 M voxels); the traffic of a launch here is that figure times its voxels
-DRAM_BYTES_PER_VOXEL = {"pass1": 4.554, "pass2": 4.439}
+DRAM_BYTES_PER_VOXEL = {"pass1": 5.060, "pass2": 4.432}
 
 
 def _parity(wl, res, n_min=500):
