@@ -1,7 +1,7 @@
 """Parity tolerances of the integration outputs.
 
-The north-star quantities (background, summation intensity and variance, profile-fitted intensity and variance)
-must agree within 1e-5 relative of the reference, with an absolute floor of 1e-5 of the quantity's natural scale
+The primary outputs (background, summation intensity and variance, profile-fitted intensity and variance) must
+agree within 1e-5 relative of the reference, with an absolute floor of 1e-5 of the quantity's natural scale
 where it can cancel to zero (an intensity near zero is judged against its sigma). Other floating outputs (moments,
 correlations, fractions) carry the reference's own float32 summation error and are held to 1e-4 of their scale.
 Integer outputs and masks are exact.

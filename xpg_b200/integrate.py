@@ -92,13 +92,15 @@ class _Block:
         self.by_tile = np.argsort(tile, kind="stable").astype(np.int32)
         self.z_lo_t, self.z_hi_t = self.z_lo[self.by_tile], self.z_hi[self.by_tile]
 
-    def allocate(self, device, f_lo, f_hi, zero_all):
+    def allocate(self, device, f_lo, eff_hi, zero_all):
         """The shoebox arena (from the buffer pool) and bin counters: the block opens. A slot must read 0 wherever no
-        frame is gathered into it; the gathers write every slot of a plain row whose frames lie inside the integrated
-        range [f_lo, f_hi] (frame indices) in full, so only the others are cleared: binned rows (they accumulate) and
-        rows reaching beyond the range, or every row when frames are excluded."""
+        frame is gathered into it. The block gathers every frame from f_lo (the first frame index of the run) or
+        its first row's, up to eff_hi (its last gathered frame), so the gathers write the whole slot of a plain row
+        whose box frames (all Dz of them, the depth bucket's padding included) lie in [f_lo, eff_hi]; only the
+        others are cleared: binned rows (they accumulate), rows starting before the run, rows whose padded depth
+        reaches past eff_hi, or every row when frames are excluded."""
         self.arena = D.POOL.take(max(self.rowset.n_vox, 1), torch.float32, device)
-        need = self.grows.binned | (self.z_lo < f_lo) | (self.z_hi > f_hi)
+        need = self.grows.binned | (self.z_lo < f_lo) | (self.z_hi > eff_hi)
         if zero_all or need.all():
             self.arena.zero_()
         elif need.any():
@@ -392,7 +394,7 @@ class SweepRun:
         while self.pending and p.need_lo[self.pending[0]] <= fi_b:
             b = self.pending.pop(0)
             blk = self.prepared.pop(b, None) or self._prepare(b)
-            blk.allocate(self.device, self.f_range[0], self.f_range[1], self.any_excluded)
+            blk.allocate(self.device, self.f_range[0], self.eff_hi[b], self.any_excluded)
             if self.early_rows and self.next_block(extra=b) == b:
                 self.block_pass1_consts(b, blk)
             self.opened[b] = blk
