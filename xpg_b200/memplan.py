@@ -109,6 +109,18 @@ class _ZOrders:
             c = np.concatenate([[0.0], np.cumsum(w_row[o], dtype=np.float64)])
             self.items.append((b, o, c, np.asarray(zstart)[o], np.asarray(zend)[o]))
 
+    def subset(self, keep):
+        """The same orders restricted to the rows where `keep` (a boolean per row) holds: no new sort."""
+        out = _ZOrders.__new__(_ZOrders)
+        out.items = []
+        for b, o, c, zs, ze in self.items:
+            m = keep[o]
+            if not m.any():
+                continue
+            step = np.diff(c)[m]
+            out.items.append((b, o[m], np.concatenate([[0.0], np.cumsum(step)]), zs[m], ze[m]))
+        return out
+
     def cut(self, k, out=None):
         """Every block in k parts of consecutive z with about equal bytes (XPG's `_split_blocks` rule: cuts where the
         cumulative bytes pass k equal shares; empty parts dropped)."""
@@ -175,8 +187,7 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
         # frames read once and no split by XPG's rule fits: a few rows far deeper in phi than a part (binned, near
         # the rotation axis) keep every part of their block open; those rows go in a part of their own
         wide = wide_rows(plan.blocks_refl, plan.zstart, plan.zend)
-        zn = _ZOrders(plan.blocks_refl, plan.refl["z"], w_row, plan.zstart, plan.zend, keep=~wide)
-        zw = _ZOrders(plan.blocks_refl, plan.refl["z"], w_row, plan.zstart, plan.zend, keep=wide)
+        zn, zw = zo.subset(~wide), zo.subset(wide)
         for k in range(2, BLOCK_PARTS_MAX + 1):
             cuts = _wide_cut(zn, zw, k)
             pk = cuts.peak(n_frames)
