@@ -837,6 +837,68 @@ def decode_bench(args):
     }), flush=True)
 
 
+def forward_bench(args):
+    """The forward-model likelihood passes (xi_fm_scatter, xi_fm_gather; XPG's forward integrator on crowded data) on
+    a window of 40 frames x a 1024 x 1024 tile holding 60,000 reflections of 9-frame, 13 x 13 px boxes with two
+    separable terms (profile and halo), seeded factors; one step = one scatter (mu) and one gather of each mode, the
+    passes of one Newton step of the intensity fit. One JSON line: voxel-terms per second and each pass's bandwidth
+    against the HBM peak (algorithmic bytes: per box voxel, scatter 8 B of read-modify-write of mu; gather 6 B (int16
+    counts, float32 mu) and, in mode 0, 4 B more; the factors once per reflection)."""
+    import torch
+    from xpg_b200 import forward as F
+    from xpg_b200.csrc import build
+    if build.stale():
+        build.build()
+
+    class Win:
+        f0, f1, y0, ny, x0, nx = 0, 40, 0, 1024, 0, 1024
+    n, T, Dz, b = 60000, 2, 9, 13
+    g = torch.Generator(device="cuda").manual_seed(3)
+    R = torch.rand((T, n, Dz), device="cuda", generator=g)
+    P = torch.rand((T, n, b, b), device="cuda", generator=g) * 0.01
+    iz0 = torch.randint(-4, 36, (n,), device="cuda", generator=g)
+    iy0 = torch.randint(-6, 1018, (n,), device="cuda", generator=g)
+    ix0 = torch.randint(-6, 1018, (n,), device="cuda", generator=g)
+    rows = torch.arange(n, device="cuda")
+    I = torch.rand(n, device="cuda", generator=g) * 100
+    nv = 40 * 1024 * 1024
+    M = torch.rand(nv, device="cuda", generator=g) + 0.1
+    A = torch.rand(nv, device="cuda", generator=g)
+    NS = torch.randint(-1, 8, (nv,), device="cuda", generator=g).to(torch.int16)
+    mu = torch.zeros(nv, device="cuda")
+    g0 = torch.zeros(n, device="cuda")
+    g1 = torch.zeros(n, device="cuda")
+    fd = torch.zeros(n, device="cuda")
+    passes = {"scatter": lambda: F.scatter(mu, R, P, I, None, iz0, iy0, ix0, Win),
+              "gather_ratio": lambda: F.gather(g0, None, R, P, rows, iz0, iy0, ix0, Win, A, M, NS, 0),
+              "gather_newton": lambda: F.gather(g1, fd, R, P, rows, iz0, iy0, ix0, Win, None, M, NS, 1)}
+    vox = n * Dz * b * b
+    factors = n * T * (Dz + b * b) * 4
+    alg = {"scatter": 8 * vox + factors, "gather_ratio": 10 * vox + factors, "gather_newton": 6 * vox + factors}
+    peak, peak_kind = _peaks()
+    out = {}
+    for name, fn in passes.items():
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3 / args.steps
+        out[name] = {"ms": round(t * 1e3, 3), "gbs": round(alg[name] / t / 1e9, 1),
+                     "hbm_frac": round(alg[name] / t / 1e9 / peak, 4)}
+    step = sum(v["ms"] for v in out.values()) * 1e-3
+    line = {"metric": "forward-model likelihood passes: box voxel-terms per second (one scatter + two gathers)",
+            "unit": "voxels/s", "value": round(3 * vox / step, 1), "steps": args.steps, "warmup": max(args.warmup, 3),
+            "passes": out, "peak_gbs": peak, "peak_kind": peak_kind,
+            "config": {"window": [40, 1024, 1024], "reflections": n, "box": [Dz, b, b], "terms": T},
+            "data": "synthetic seeded factors, counts and model", "dtype": "f32 (per-reflection sums f64)"}
+    print(json.dumps(line), flush=True)
+
+
 def spots_bench(args):
     """The strong-pixel classifier of spot finding (both passes) on 4148 x 4362 float32 frames (Poisson background 0.2,
     flagged columns, 3000 spots per frame), timed with CUDA events, one JSON line; cpu_baseline: the oracle's numpy
@@ -910,9 +972,12 @@ def main():
                                                           "device-time spans")
     ap.add_argument("--decode", action="store_true", help="time the bitshuffle-LZ4 frame decode instead")
     ap.add_argument("--spots", action="store_true", help="time the spot-finding classifier instead")
+    ap.add_argument("--forward", action="store_true", help="time the forward-model likelihood passes instead")
     args = ap.parse_args()
     if args.decode:
         decode_bench(args)
+    elif args.forward:
+        forward_bench(args)
     elif args.spots:
         spots_bench(args)
     elif args.workload == "config4" and args.impl != "reference":

@@ -491,6 +491,48 @@ int xi_format_integrate_hkl(const XiHklRows *rows, char *out, int64_t cap, int t
  * before any launch). No counterpart in XPG (its arrays stay on the host). */
 int xi_upload(const void *src, void *dst, int64_t bytes, void *stream);
 
+/* ---- Forward-model likelihood passes ---------------------------------------------------------------------------
+ * XPG's pixel-level forward integrator (xpg/forward/) models every pixel-frame of a window as a background plus
+ * sum_h I_h f_h, with each reflection's fraction separable per term: f(z, y, x) = sum_t R[t, row, z] P[t, row, y, x]
+ * over its box of Dz frames and b x b pixels at (iz0, iy0, ix0). Window voxels are indexed densely:
+ * ((iz0 + z - f0) * ny + (iy0 + y - y0)) * nx + (ix0 + x - x0), voxels outside the window dropped
+ * (WindowModel.vid, xpg/forward/model.py:381-392). These replace the Triton kernels of xpg/forward/kernels.py:34-134
+ * (`scatter`, `gather`) and the eager passes WindowModel.mu / grad_ratio / grad_newton (model.py:476-577).
+ * Device pointers; float32 factors and windows; int64 origins. */
+typedef struct {
+    int n;                          /* reflections of the chunk */
+    int n_terms;                    /* separable terms T: 1 (profile) or 2 (profile and halo); at most 4 */
+    int Dz, b;                      /* box frames and side */
+    const float *R;                 /* (T, n, Dz) rocking-curve factors */
+    const float *P;                 /* (T, n, b, b) detector-profile factors */
+    const int64_t *iz0, *iy0, *ix0; /* (n) box origins: frame index, row, column (super-pixel units) */
+} XiFmBoxes;
+
+typedef struct {
+    int64_t f0, nf;                 /* frames [f0, f0 + nf) (0-based frame indices) */
+    int64_t y0, ny, x0, nx;         /* detector tile: rows [y0, y0 + ny), columns [x0, x0 + nx) */
+} XiFmWindow;
+
+#define XI_FM_NS_I16 0              /* counts NS as int16 (XPG's store), int32 or float32; NS < 0: no term */
+#define XI_FM_NS_I32 1
+#define XI_FM_NS_F32 2
+
+/* Scatter (`kernels.scatter`, kernels.py:110-120; `WindowModel.mu`): mu[v] += I[row] * f + beta[row] over every
+ * in-window voxel of every box (float atomics: the sum's order is not fixed). I, beta: (n) of the chunk's rows;
+ * beta NULL: no flat term. */
+int xi_fm_scatter(const XiFmBoxes *boxes, const XiFmWindow *win, const float *I, const float *beta, float *mu,
+                  void *stream);
+
+/* Gather (`kernels.gather`, kernels.py:123-134; `WindowModel.grad_ratio` / `grad_newton`) over the in-window voxels
+ * with NS >= 0: mode 0: g[rows[row]] += sum f A / M; mode 1: g[rows[row]] += sum f (1 - max(NS, 0) / M) and
+ * fd[rows[row]] += sum f^2 / max(M, 1e-6). rows: (n) output index of each reflection (NULL: row itself). Each
+ * reflection's sums are accumulated in float64 and added once. */
+int xi_fm_gather(const XiFmBoxes *boxes, const XiFmWindow *win, const int64_t *rows, const float *A, const float *M,
+                 const void *NS, int ns_type, int mode, float *g, float *fd, void *stream);
+
+/* Last error message of the forward-model passes on this thread. */
+const char *xi_fm_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

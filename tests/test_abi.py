@@ -33,7 +33,7 @@ def test_struct_layouts_match_header(tmp_path):
                "XiPass2In": N.XiPass2In, "XiPass2Out": N.XiPass2Out, "XiGatherRows": N.XiGatherRows,
                "XiFrames": N.XiFrames, "XiPlanDetector": N.XiPlanDetector, "XiPredict": N.XiPredict,
                "XiPredictOut": N.XiPredictOut, "XiBoxRules": N.XiBoxRules, "XiBoxOut": N.XiBoxOut, "XiKnn": N.XiKnn,
-               "XiRocking": N.XiRocking}
+               "XiRocking": N.XiRocking, "XiFmBoxes": N.XiFmBoxes, "XiFmWindow": N.XiFmWindow}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "xpgi.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')

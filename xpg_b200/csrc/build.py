@@ -18,7 +18,7 @@ ROOT = HERE.parent.parent
 LIB_DIR = HERE.parent / "_lib"
 LIB = LIB_DIR / "libxpgi.so"
 SOURCES = [HERE / "xpgi.cu", HERE / "xpgi_plan.cu", HERE / "xpgi_adapt.cu", HERE / "xpgi_synth.cu",
-           HERE / "xpgi_frames.cu", HERE / "xpgi_spot.cu", HERE / "xpgi_pack.cpp"]
+           HERE / "xpgi_forward.cu", HERE / "xpgi_frames.cu", HERE / "xpgi_spot.cu", HERE / "xpgi_pack.cpp"]
 DEPS = SOURCES + [HERE / "xpgi_device.cuh", HERE / "xpgi_internal.h", HERE / "xpgi_synth.h", ROOT / "include" / "xpgi.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

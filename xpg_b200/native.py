@@ -76,6 +76,16 @@ class XiSynthBackground(C.Structure):
                 ("rmax", C.c_double)]
 
 
+class XiFmBoxes(C.Structure):
+    _fields_ = [("n", C.c_int), ("n_terms", C.c_int), ("Dz", C.c_int), ("b", C.c_int), ("R", C.c_void_p),
+                ("P", C.c_void_p), ("iz0", C.c_void_p), ("iy0", C.c_void_p), ("ix0", C.c_void_p)]
+
+
+class XiFmWindow(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("f0", "nf", "y0", "ny", "x0", "nx")]
+
+
+XI_FM_NS_I16, XI_FM_NS_I32, XI_FM_NS_F32 = 0, 1, 2
 XI_PANEL_F64 = 28
 XI_PANELS_INLINE = 4
 XI_KNN_MAX = 16
@@ -168,7 +178,7 @@ EXPORTS = ("xi_last_error", "xi_version", "xi_status", "xi_status_copy", "xi_tun
            "xi_predict_workspace", "xi_knn_workspace", "xi_rocking_gram_workspace", "xi_pack_u8", "xi_unpack_u8",
            "xi_upload", "xi_bslz4_lz4_stage", "xi_bitunshuffle", "xi_format_integrate_hkl", "xi_spot_strong",
            "xi_spot_workspace", "xi_pass1_batched", "xi_pass2_batched", "xi_gather_step", "xi_unpack_u8_frames",
-           "xi_zero_rows")
+           "xi_zero_rows", "xi_fm_scatter", "xi_fm_gather")
 
 _LIB = None
 
@@ -238,6 +248,11 @@ def load(path=None):
     lib.xi_synth_frames.argtypes = [C.POINTER(XiSynthSpots), C.POINTER(XiSynthBackground), C.c_int, C.c_int,
                                     C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p]
     lib.xi_synth_last_error.restype = C.c_char_p
+    lib.xi_fm_last_error.restype = C.c_char_p
+    lib.xi_fm_scatter.argtypes = [C.POINTER(XiFmBoxes), C.POINTER(XiFmWindow), C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]
+    lib.xi_fm_gather.argtypes = [C.POINTER(XiFmBoxes), C.POINTER(XiFmWindow), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     if path is None:
         _LIB = lib
         _apply_tuned(lib)
