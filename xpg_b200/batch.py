@@ -21,6 +21,7 @@ wedges arrive over time and reports the wedge-to-intensities latency of every we
 """
 from __future__ import annotations
 
+import contextlib
 import time
 from dataclasses import dataclass, field
 
@@ -243,6 +244,17 @@ def run_jobs(jobs, budget_bytes=None, bins=None, device="cuda", served=False, cl
     return results, stats
 
 
+@contextlib.contextmanager
+def _own_stream(device):
+    """The calling thread's device work on a CUDA stream of its own (made current), waited for on exit."""
+    dev = torch.device(device)
+    with torch.cuda.device(dev if dev.index is not None else torch.cuda.current_device()):
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            yield stream
+        stream.synchronize()
+
+
 def integrate_concurrent(jobs, budget_bytes=None, workers=3, device="cuda"):
     """Integrates every job (all frames available) on `workers` host threads, each running the plain path of one
     sweep at a time (`integrate.drive`) on streams of its own: one sweep's host stages (planning, adaptation,
@@ -263,31 +275,27 @@ def integrate_concurrent(jobs, budget_bytes=None, workers=3, device="cuda"):
 
     def work(i):
         job = jobs[i]
-        dev = torch.device(device)
-        with torch.cuda.device(dev if dev.index is not None else torch.cuda.current_device()):
-            stream = torch.cuda.Stream()
-            with torch.cuda.stream(stream):
-                run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, verbose=False,
-                               device=device, mem_budget=budget, overlap=True, **job.kwargs)
-                need = int(run.mem["peak"])
+        with _own_stream(device):
+            run = SweepRun(job.images, job.exp_blocks, job.block_edges, job.model, job.dmin, verbose=False,
+                           device=device, mem_budget=budget, overlap=True, **job.kwargs)
+            need = int(run.mem["peak"])
+            try:
+                with cond:
+                    while state["running"] and state["used"] + need > budget:
+                        cond.wait()
+                    state["used"] += need
+                    state["running"] += 1
+                    stats["peak_bytes"] = max(stats["peak_bytes"], state["used"])
+                    stats["admitted_at"][i] = time.perf_counter() - t0
                 try:
-                    with cond:
-                        while state["running"] and state["used"] + need > budget:
-                            cond.wait()
-                        state["used"] += need
-                        state["running"] += 1
-                        stats["peak_bytes"] = max(stats["peak_bytes"], state["used"])
-                        stats["admitted_at"][i] = time.perf_counter() - t0
-                    try:
-                        results[i] = drive(run)
-                    finally:
-                        with cond:
-                            state["used"] -= need
-                            state["running"] -= 1
-                            cond.notify_all()
+                    results[i] = drive(run)
                 finally:
-                    run.close()
-            stream.synchronize()
+                    with cond:
+                        state["used"] -= need
+                        state["running"] -= 1
+                        cond.notify_all()
+            finally:
+                run.close()
 
     with ThreadPoolExecutor(max_workers=max(int(workers), 1)) as ex:
         for f in [ex.submit(work, i) for i in range(len(jobs))]:
