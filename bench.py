@@ -185,8 +185,7 @@ def workload_config(name, spec, edges, n_frames, plan, world):
             "phi_blocks": len(edges) - 1, "detector": [spec.nx, spec.ny],
             "voxels_per_step": int((plan.Dz * plan.bx.astype(np.int64) ** 2).sum()),
             "l2": f"inputs larger than L2 (frame stack {4 * P * n_frames / 1e9:.3g} GB of uint32)",
-            "parallelism": f"replicas x{world} (one sweep per rank)",
-            "device_buffers": "kept between integrate() calls (xpg_b200.keep_buffers)"}
+            "parallelism": f"replicas x{world} (one sweep per rank)"}
 
 
 def alg_bytes(spec, n_frames, plan):
@@ -520,6 +519,7 @@ def run(args):
                            "open_buffers_gb": round(res_timed.memory["peak"] / 1e9, 1),
                            "budget_gb": round(res_timed.memory["budget"] / 1e9, 1)},
                 "host_s_last_step": {k: round(v, 3) for k, v in res_timed.timing.get("host_s", {}).items()},
+                "device_buffers": "kept between integrate() calls (xpg_b200.keep_buffers)",
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "parity": parity}
         print(json.dumps(line), flush=True)
