@@ -50,3 +50,30 @@ def test_cases_reach_every_edge():
                      (g["iy0"] + b > y0 + ny).any(), (g["ix0"] < x0).any(), (g["ix0"] + b > x0 + nx).any()]
         assert edge.all()
         assert (c["NS"] < 0).any()
+
+
+def test_oracle_fraction_terms_match_xpg():
+    """The separable factors (`fraction_terms`, xpg/forward/model.py:206-280) against XPG's own on rows of the
+    config-1 fixture (tests/golden/forward_terms.npz): parametric and learnt profiles, the rocking-curve mixture, the
+    halo's second term; within 1e-6 of each reflection's largest factor."""
+    import golden_io as G
+    from oracle import kernels as OK
+    z = np.load(Path(__file__).resolve().parent / "golden" / "forward_terms.npz")
+    spec = G.case_inputs("config1")[0]
+    det = OK.detector_consts(spec.geometry(), None)
+    Dz, b = int(z["Dz"]), int(z["b"])
+    worst = 0.0
+    for v in ("gauss", "learnt", "learnt_rcw", "gauss_halo"):
+        terms = OF.fraction_terms(det, z["S"], z["phi"], z["ix0"], z["iy0"], z["iz0"], Dz, b, z["s0"], z["axis"],
+                                  float(z["frames_phi0"]), float(z["osc"]), float(z["sd"]), float(z["sm"]),
+                                  prof=z["prof"] if v.startswith("learnt") else None, region=z["region"],
+                                  umax=float(z["umax"]), halo=tuple(z["halo"]) if v.endswith("halo") else None,
+                                  rcw=z["rcw"] if v == "learnt_rcw" else None)
+        assert len(terms) == int(z[f"{v}_n_terms"])
+        for k, (R, P) in enumerate(terms):
+            for ours, xpg in ((R, z[f"{v}_R{k}"]), (P, z[f"{v}_P{k}"])):
+                scale = np.abs(xpg).max(axis=tuple(range(1, xpg.ndim)), keepdims=True)
+                err = np.abs(ours.astype(np.float64) - xpg) / np.maximum(scale, 1e-30)
+                worst = max(worst, float(err.max()))
+                assert err.max() <= 1e-6, (v, k, float(err.max()))      # float32 rounding (measured 4e-7)
+    assert worst < 1e-6
