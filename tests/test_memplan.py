@@ -121,3 +121,18 @@ def test_passes_by_lattice_first():
     passes, pk = M.split_passes(nbytes, lo, hi, [0, 0, 0, 1, 1, 1], 300, 0.3 * one)
     assert len(passes) == 4 and sorted(sum(passes, [])) == list(range(6))
     assert all(len({b // 3 for b in q}) == 1 for q in passes)           # each pass holds one lattice
+
+
+def test_row_bytes_table_matches_the_formula():
+    """The table lookup of row_bytes gives the formula's bytes for every bucket combination, and the formula itself
+    answers values beyond the table."""
+    from types import SimpleNamespace
+    rng = np.random.default_rng(9)
+    n = 20000
+    Dz = rng.choice([3, 5, 9, 17, 33, 65], n).astype(np.int32)
+    bx = rng.choice([9, 13, 17, 23, 31, 41, 55, 73, 97], n).astype(np.int32)
+    fb = np.where(rng.random(n) < 0.1, rng.integers(2, 9, n), 1).astype(np.int32)
+    p = SimpleNamespace(Dz=Dz, bx=bx, fb=fb)
+    np.testing.assert_array_equal(M.row_bytes(p), M._bytes_of(Dz, bx, fb > 1))
+    q = SimpleNamespace(Dz=np.array([130, 5]), bx=np.array([9, 200]), fb=np.array([1, 3]))
+    np.testing.assert_array_equal(M.row_bytes(q), M._bytes_of(q.Dz, q.bx, q.fb > 1))

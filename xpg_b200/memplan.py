@@ -20,14 +20,32 @@ DEVICE_FRACTION = 0.95       # share of the device memory free at the start that
 WIDE_SPANS = 4.0             # rows deeper in phi than this many median spans: a part of their own (frames read once)
 
 
+def _bytes_of(Dz, bx, binned):
+    Dz = np.asarray(Dz, np.int64)
+    bx = np.asarray(bx, np.int64)
+    arena = 4 * ((Dz * bx * bx + 3) & ~3)
+    return arena + arena // 20 + np.where(binned, 4 * Dz, 0) + 17 * bx * bx + 4 * Dz + 400     # + the pool's 5%
+
+
+_TABLE = _bytes_of(*np.meshgrid(np.arange(128), np.arange(128), np.arange(2), indexing="ij")).reshape(-1)
+
+
 def row_bytes(plan):
     """Device bytes of every row while its block is open: the shoebox (value + 3 floats, rows on 16 bytes, and the
     buffer pool's 5% slack), bin counters of binned rows, the per-pixel pass-1 tables (img2, J, u1, u2,
-    all_valid2), per-frame fz, per-row scalars of both passes."""
-    Dz = plan.Dz.astype(np.int64)
-    bx = plan.bx.astype(np.int64)
-    arena = 4 * ((Dz * bx * bx + 3) & ~3)
-    return (arena + arena // 20 + np.where(plan.fb > 1, 4 * Dz, 0) + 17 * bx * bx + 4 * Dz + 400)   # + the pool's 5%
+    all_valid2), per-frame fz, per-row scalars of both passes. Depths and sides come from short bucket lists, so a
+    table over (depth, side, binned) below 128 answers every row with one gather (millions of rows per plan)."""
+    Dz = np.asarray(plan.Dz).astype(np.int32, copy=False)
+    bx = np.asarray(plan.bx).astype(np.int32, copy=False)
+    binned = np.asarray(plan.fb) > 1
+    if Dz.size:
+        code = Dz << 8
+        code |= bx << 1
+        lo, hi = int(code.min()), int(code.max())
+        if 0 <= lo and hi < (128 << 8) and 0 <= int(bx.min()) and int(bx.max()) < 128:
+            code |= binned
+            return _TABLE[code]
+    return _bytes_of(Dz, bx, binned)
 
 
 def budget(device="cuda"):
@@ -60,6 +78,14 @@ def peak_bytes(blocks_refl, need_lo, need_hi, w_row, n_frames):
             d[int(np.clip(need_hi[b] + 1, 0, n_frames + 1))] -= w
             big = max(big, w)
     return float(np.cumsum(d).max()), big
+
+
+def _rows_sum(w, rows):
+    """w summed over a block's rows (sorted, distinct plan rows: a slice when they are a range)."""
+    if not rows.size:
+        return 0.0
+    a, e = int(rows[0]), int(rows[-1]) + 1
+    return float(w[a:e].sum() if e - a == rows.size else w[rows].sum())
 
 
 def peak_of(nbytes, lo, hi, n_frames):
@@ -153,7 +179,7 @@ def fit(plan, exp_blocks, n_frames, wedge_bytes, limit, allow_passes=True):
     ["wide_apart"]). Returns (plan, exp_blocks, info); info["passes"]: the block lists of the passes when there are
     several; info["parts"]: parts per block of the consecutive-phi split."""
     w_row = row_bytes(plan)
-    nb = [float(w_row[r].sum()) if r.size else 0.0 for r in plan.blocks_refl]
+    nb = [_rows_sum(w_row, r) for r in plan.blocks_refl]
     one = peak_of(nb, plan.need_lo, plan.need_hi, n_frames)
     info = dict(peak=one + wedge_bytes, one=one + wedge_bytes, parts=1, budget=limit)
     if limit is None or one + wedge_bytes <= limit:
