@@ -249,9 +249,11 @@ class SweepRun:
         self.exp_blocks = exp_blocks
         self.refl = p.refl
         n = p.n
-        if D.POOL.persist:                # buffers kept from the last run: only those this run's blocks can take
-            vox = [int((p.Dz[r].astype(np.int64) * p.bx[r].astype(np.int64) ** 2).sum()) for r in p.blocks_refl]
-            pix = [17 * int((p.bx[r].astype(np.int64) ** 2).sum()) for r in p.blocks_refl]
+        if D.POOL.persist and D.POOL.free:    # buffers kept from the last run: only those this run's blocks can take
+            b2 = p.bx.astype(np.int64) ** 2
+            vox_row = b2 * p.Dz
+            vox = [int(memplan._rows_sum(vox_row, r)) for r in p.blocks_refl]
+            pix = [17 * int(memplan._rows_sum(b2, r)) for r in p.blocks_refl]
             D.POOL.retain({torch.float32: vox, torch.uint8: pix, torch.int32: [W * src.ny * src.nx]})
         if verbose and (self.mem["parts"] > 1 or "passes" in self.mem):
             log(f"  INTEGRATE: open shoebox buffers ~{self.mem['one'] / 2 ** 30:.1f} GB > the device budget "
